@@ -1,0 +1,142 @@
+/*
+ * pfsht_b200.h -- C ABI of libpfsht_b200, a B200 (sm_100a) backend for PartialFSHT.jl's
+ * partial-sky spherical harmonic synthesis and its exact adjoint.
+ *
+ * The entry points are what a PartialFSHT.jl device extension would ccall in place of the
+ * reference's Julia leaf (see INTEGRATION.md for the binding). Plain pointers and sizes only.
+ *
+ * Layouts are the reference's, column-major:
+ *   alm : (lmax+1) x (2lmax+1) x ntrans complex double, FastSphericalHarmonics sph_mode
+ *         packing (src/Layout.jl:13-20): 0-based column 2m for m >= 0, 2|m|-1 for m < 0,
+ *         row l-|m|. Padding slots are ignored on input and written as zero by the adjoint.
+ *   f   : npts x ntrans complex double, points in the caller's order.
+ *   G   : nrings x (2lmax+1) x ntrans complex double, column m+lmax (src/Legendre.jl:306).
+ * Complex numbers are interleaved (re, im) pairs of doubles.
+ *
+ * Every function returns a pfsht_status; a non-zero status leaves a message readable with
+ * pfsht_last_error (thread-local). Validation happens before any launch.
+ */
+#ifndef PFSHT_B200_H
+#define PFSHT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    PFSHT_OK = 0,
+    PFSHT_ERR_ARGUMENT = 1,       /* Julia ArgumentError (src/Plan.jl:98-102) */
+    PFSHT_ERR_DIMENSION = 2,      /* Julia DimensionMismatch (src/Layout.jl:251-272) */
+    PFSHT_ERR_REFUSED = 3,        /* degenerate stretch geometry (src/Windows.jl:66-75) */
+    PFSHT_ERR_CUDA = 4,           /* a CUDA or cuFFT call failed */
+    PFSHT_ERR_OUT_OF_MEMORY = 5,  /* device allocation failed, or a budget was exceeded */
+    PFSHT_ERR_TIMEOUT = 6,        /* a bounded device-side wait gave up */
+    PFSHT_ERR_UNSUPPORTED = 7     /* option not built into this library */
+} pfsht_status;
+
+typedef enum { PFSHT_METHOD_AUTO = 0, PFSHT_METHOD_STRETCH = 1, PFSHT_METHOD_DIRECT = 2 } pfsht_method;
+
+typedef enum {
+    PFSHT_PRECISION_FP64 = 0,   /* plain form: FP64 everywhere */
+    PFSHT_PRECISION_MIXED = 1   /* FP64 recurrence + exponents; FP32 compensated ring sums and FP32 NUFFT */
+} pfsht_precision;
+
+typedef enum { PFSHT_KIND_POLE = 0, PFSHT_KIND_INTERIOR = 1, PFSHT_KIND_FULL = 2, PFSHT_KIND_DIRECT = 3 } pfsht_kind;
+
+/* Plan options: the keyword arguments of Plan(...) (src/Plan.jl:84-97) that change the
+ * apply, plus the device knobs. Fill with pfsht_opts_default first. */
+typedef struct pfsht_opts {
+    int32_t method;             /* pfsht_method */
+    int32_t points_on_device;   /* theta/phi are device pointers */
+    int32_t device;             /* CUDA device ordinal; -1 = current */
+    int32_t ring_rings_per_lane;/* ring-pass tile shape: rings per lane (1, 2 or 4; 0 = auto) */
+    int32_t nufft_bin_rows;     /* NUFFT spreading bin height in fine cells (0 = auto) */
+    int32_t nufft_bin_cols;     /* NUFFT spreading bin width in fine cells (0 = auto) */
+    double oversample_theta;    /* src/Plan.jl:95 */
+    double oversample_phi;      /* src/Plan.jl:96 */
+    double eps_apo_max;         /* src/Plan.jl:97 */
+    int32_t reserved[8];
+} pfsht_opts;
+
+typedef struct pfsht_plan pfsht_plan;
+
+/* Geometry and sizes of a plan (the fields of StretchLeaf, src/Stretch.jl:94-127). */
+typedef struct pfsht_plan_info {
+    int32_t kind;        /* pfsht_kind */
+    int32_t flip;        /* south periodisation reflected to the north */
+    int32_t lmax, ntrans, precision;
+    int32_t nth_half, nth, nph, mmax, nrings;
+    int64_t npts, K, ring_work;
+    double tol, beta, h, theta_lo, theta_hi, eps_apo, Theta1, sigma, ThetaT;
+    /* NUFFT */
+    int32_t nufft_w, nf1, nf2, row0, nrows, ncols;
+    double nufft_beta;
+    int64_t device_bytes; /* device memory the plan holds */
+} pfsht_plan_info;
+
+/* Fill defaults (method AUTO, host points, current device, oversampling 1, eps_apo_max 1). */
+pfsht_status pfsht_opts_default(pfsht_opts* opts);
+
+/* Plan(theta, phi; lmax, tol, ntrans) (src/Plan.jl:84-116). Geometry on the host; the
+ * point transform, the NUFFT bin sort and the recurrence tables on the device. */
+pfsht_status pfsht_plan_create(const double* theta, const double* phi, int64_t npts,
+                               int32_t lmax, int32_t ntrans, double tol, int32_t precision,
+                               const pfsht_opts* opts, pfsht_plan** out);
+pfsht_status pfsht_plan_destroy(pfsht_plan* plan);
+
+/* mul!(f, plan, alm) (src/Plan.jl:137-141): device pointers, enqueued on `stream`
+ * (a cudaStream_t; NULL = legacy default stream). */
+pfsht_status pfsht_forward(pfsht_plan* plan, const void* alm, void* f, void* stream);
+/* mul!(alm, plan', f) (src/Plan.jl:143-148): overwrites alm, padding zeroed. */
+pfsht_status pfsht_adjoint(pfsht_plan* plan, const void* f, void* alm, void* stream);
+
+/* The same two applies on host buffers: copies in, apply, copies out, synchronous.
+ * The plan keeps staging buffers for this (src/Stretch.jl:393-410 role). */
+pfsht_status pfsht_forward_host(pfsht_plan* plan, const void* alm, void* f);
+pfsht_status pfsht_adjoint_host(pfsht_plan* plan, const void* f, void* alm);
+
+/* rings_from_alm! / alm_from_rings! (src/Legendre.jl:310-341) on the plan's ring set:
+ * G is nrings x (2lmax+1) x ntrans on the device. For parity tests of the ring pass. */
+pfsht_status pfsht_ring_forward(pfsht_plan* plan, const void* alm, void* G, void* stream);
+pfsht_status pfsht_ring_adjoint(pfsht_plan* plan, const void* G, void* alm, void* stream);
+
+/* Queries: ring_work (src/Plan.jl:44), sizes (src/Stretch.jl:94-127). */
+int64_t pfsht_ring_work(const pfsht_plan* plan);
+pfsht_status pfsht_plan_get_info(const pfsht_plan* plan, pfsht_plan_info* info);
+int64_t pfsht_workspace_bytes(const pfsht_plan* plan);
+
+/* Host-only plan geometry, no device touched: what pfsht_plan_create would choose for
+ * these points (kind, sizes, ring_work). Points are host pointers. */
+pfsht_status pfsht_plan_geometry(const double* theta, const double* phi, int64_t npts,
+                                 int32_t lmax, int32_t ntrans, double tol,
+                                 const pfsht_opts* opts, pfsht_plan_info* info);
+
+/* dfs_double! / dfs_fold! (src/DFS.jl:13-56) on device arrays, column-major
+ * F: Nth x Nph x B, Ft: 2Nth x Nph x B. */
+pfsht_status pfsht_dfs_double(const void* F, void* Ft, int32_t Nth, int32_t Nph, int32_t B,
+                              int32_t spin, void* stream);
+pfsht_status pfsht_dfs_fold(void* F, const void* Ft, int32_t Nth, int32_t Nph, int32_t B,
+                            int32_t spin, void* stream);
+
+/* The NUFFT seam (src/NUFFT.jl:17-25, _nufft_makeplan/_nufft_exec!): a 2-D type-1/type-2
+ * NUFFT with modes n1 x n2 in FFT order (modeord = 1), points x, y (host pointers, any
+ * real values; taken modulo 2 pi). type 2: modes -> M values; type 1: M values -> modes. */
+typedef struct pfsht_nufft pfsht_nufft;
+pfsht_status pfsht_nufft_create(int32_t type, int32_t n1, int32_t n2, int32_t iflag,
+                                int32_t ntrans, double tol, const double* x, const double* y,
+                                int64_t M, pfsht_nufft** out);
+pfsht_status pfsht_nufft_exec(pfsht_nufft* p, const void* in, void* out, void* stream);
+pfsht_status pfsht_nufft_destroy(pfsht_nufft* p);
+
+/* Thread-local message of the last failing call; returns its length. */
+size_t pfsht_last_error(char* buf, size_t len);
+/* Library version string. */
+const char* pfsht_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PFSHT_B200_H */

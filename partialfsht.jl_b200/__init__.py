@@ -1,0 +1,371 @@
+"""pfsht_b200: PartialFSHT.jl's partial-sky SHT apply on one B200, behind the reference's API.
+
+Mirrors the reference's public operator (src/Plan.jl):
+
+    plan = Plan(theta, phi, lmax=L, tol=1e-8)     # Plan(θ, φ; lmax, tol)
+    mul(f, plan, alm)                              # mul!(f, plan, alm)
+    mul(alm, plan.H, f)                            # mul!(alm, plan', f)
+    f = plan * alm;  alm = plan.H * f              # Base.:* (src/Plan.jl:190-199)
+
+Arrays keep the reference's column-major layout. A coefficient array has Julia shape
+(lmax+1, 2lmax+1[, ntrans]) with sph_mode packing (src/Layout.jl:13-20); a field has shape
+(npts[, ntrans]). On the device these are torch complex128 CUDA tensors with Fortran strides
+(``zeros_alm`` / ``zeros_field`` make them); host numpy arrays (Fortran order) go through
+the library's host-buffer entry points. All compute is the CUDA library libpfsht_b200.so:
+there is no CPU fallback and the package refuses to import without it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import DimensionMismatch, PFSHTError, RefusedGeometry  # noqa: F401
+
+__all__ = ["Plan", "AdjointPlan", "mul", "coeff_size", "sph_mode", "zeros_alm", "zeros_field",
+           "plan_geometry", "ring_forward", "ring_adjoint", "NUFFT", "DimensionMismatch",
+           "RefusedGeometry", "PFSHTError", "version"]
+
+_lib.load()
+
+
+def version() -> str:
+    return _lib.load().pfsht_version().decode()
+
+
+# ---------------------------------------------------------------------------------------
+# layout (src/Layout.jl)
+# ---------------------------------------------------------------------------------------
+def coeff_size(lmax: int):
+    """(lmax+1, 2lmax+1) (src/Layout.jl:13)."""
+    return (int(lmax) + 1, 2 * int(lmax) + 1)
+
+
+def sph_mode(l: int, m: int):
+    """0-based (row, column) of degree l, order m (src/Layout.jl:20)."""
+    am = abs(int(m))
+    return (int(l) - am, 2 * am if m >= 0 else 2 * am - 1)
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def zeros_alm(lmax: int, ntrans: int = 1, device="cuda"):
+    """Zero coefficient array, Julia shape (lmax+1, 2lmax+1[, ntrans]), column-major."""
+    nr, nc = coeff_size(lmax)
+    if device in (None, "cpu", "host"):
+        shape = (nr, nc) if ntrans == 1 else (nr, nc, ntrans)
+        return np.zeros(shape, dtype=np.complex128, order="F")
+    torch = _torch()
+    t = torch.zeros((ntrans, nc, nr), dtype=torch.complex128, device=device).permute(2, 1, 0)
+    return t[:, :, 0] if ntrans == 1 else t
+
+
+def zeros_field(npts: int, ntrans: int = 1, device="cuda"):
+    """Zero field, Julia shape (npts[, ntrans]), column-major."""
+    if device in (None, "cpu", "host"):
+        shape = (npts,) if ntrans == 1 else (npts, ntrans)
+        return np.zeros(shape, dtype=np.complex128, order="F")
+    torch = _torch()
+    t = torch.zeros((ntrans, npts), dtype=torch.complex128, device=device).permute(1, 0)
+    return t[:, 0] if ntrans == 1 else t
+
+
+def _is_torch(a) -> bool:
+    return type(a).__module__.startswith("torch")
+
+
+def _colmajor_ok(a, shape) -> bool:
+    """True when `a` holds `shape` (Julia order) in column-major memory."""
+    if tuple(a.shape) != tuple(shape):
+        return False
+    if _is_torch(a):
+        strides = a.stride()
+        item = 1
+    else:
+        strides = a.strides
+        item = a.itemsize
+    expect = item
+    for n, s in zip(shape, strides):
+        if n > 1 and s != expect:
+            return False
+        expect *= n
+    return True
+
+
+def _check_array(a, shapes, what):
+    if _is_torch(a):
+        torch = _torch()
+        if a.dtype != torch.complex128:
+            raise TypeError(f"{what} must be complex128, got {a.dtype}")
+    else:
+        if not isinstance(a, np.ndarray) or a.dtype != np.complex128:
+            raise TypeError(f"{what} must be a complex128 numpy array or torch tensor")
+    for shp in shapes:
+        if tuple(a.shape) == tuple(shp):
+            if not _colmajor_ok(a, shp):
+                raise ValueError(f"{what} must be column-major (Fortran order), as in Julia")
+            return
+    raise DimensionMismatch(f"{what} is {tuple(a.shape)}, expected {' or '.join(map(str, shapes))}")
+
+
+def _coeff_shapes(lmax, B):
+    nr, nc = coeff_size(lmax)
+    return [(nr, nc), (nr, nc, 1)] if B == 1 else [(nr, nc, B)]
+
+
+def _field_shapes(npts, B):
+    return [(npts,), (npts, 1)] if B == 1 else [(npts, B)]
+
+
+def _ptr(a) -> int:
+    return a.data_ptr() if _is_torch(a) else a.ctypes.data
+
+
+def _stream_of(a, stream):
+    if stream is not None:
+        return int(getattr(stream, "cuda_stream", stream))
+    torch = _torch()
+    return torch.cuda.current_stream(a.device).cuda_stream
+
+
+# ---------------------------------------------------------------------------------------
+# Plan (src/Plan.jl)
+# ---------------------------------------------------------------------------------------
+class Plan:
+    """Plan(theta, phi; lmax, tol=1e-10, ntrans=1, method="auto") (src/Plan.jl:84-116).
+
+    ``method`` is "auto" (stretched leaf, or the direct leaf where the stretched geometry is
+    refused, src/Cost.jl:121-122), "stretch" (refusal raises RefusedGeometry) or "direct".
+    ``precision`` is "fp64" (plain form) or "mixed". Points may be host arrays or CUDA
+    tensors (float64). ``rings_per_lane`` / ``bin_rows`` / ``bin_cols`` are device tile
+    shapes (0 = defaults).
+    """
+
+    def __init__(self, theta, phi, *, lmax, tol=1e-10, ntrans=1, method="auto",
+                 precision="fp64", oversample_theta=1.0, oversample_phi=1.0, eps_apo_max=1.0,
+                 device=None, rings_per_lane=0, bin_rows=0, bin_cols=0):
+        self._h = None
+        if len(theta) != len(phi):
+            raise DimensionMismatch("θ and φ must have the same length")
+        if lmax < 0:
+            raise ValueError("lmax must be nonnegative")
+        if ntrans < 1:
+            raise ValueError("ntrans must be ≥ 1")
+        if method not in _lib.METHODS:
+            raise ValueError(f"unknown method {method!r}")
+        if precision not in _lib.PRECISIONS:
+            raise ValueError(f"unknown precision {precision!r}")
+        o = _lib.default_opts()
+        o.method = _lib.METHODS[method]
+        o.oversample_theta = float(oversample_theta)
+        o.oversample_phi = float(oversample_phi)
+        o.eps_apo_max = float(eps_apo_max)
+        o.ring_rings_per_lane = int(rings_per_lane)
+        o.nufft_bin_rows = int(bin_rows)
+        o.nufft_bin_cols = int(bin_cols)
+        if _is_torch(theta):
+            torch = _torch()
+            th = theta.to(torch.float64).contiguous()
+            ph = phi.to(dtype=torch.float64, device=th.device).contiguous()
+            if th.is_cuda:
+                # the plan is built on the library's own stream: finish torch's writes first
+                torch.cuda.current_stream(th.device).synchronize()
+                o.points_on_device = 1
+                o.device = th.device.index if device is None else int(device)
+            else:
+                o.device = -1 if device is None else int(device)
+            keep = (th, ph)
+            pth, pph = th.data_ptr(), ph.data_ptr()
+        else:
+            th = np.ascontiguousarray(theta, dtype=np.float64)
+            ph = np.ascontiguousarray(phi, dtype=np.float64)
+            o.device = -1 if device is None else int(device)
+            keep = (th, ph)
+            pth, pph = th.ctypes.data, ph.ctypes.data
+        h = C.c_void_p()
+        _lib.check(_lib.load().pfsht_plan_create(pth, pph, len(th), int(lmax), int(ntrans),
+                                                 float(tol), _lib.PRECISIONS[precision],
+                                                 C.byref(o), C.byref(h)), "Plan")
+        del keep
+        self._h = h
+        self.lmax = int(lmax)
+        self.ntrans = int(ntrans)
+        self.tol = float(tol)
+        self.npts = len(theta)
+        self.precision = precision
+        inf = _lib.PlanInfo()
+        _lib.check(_lib.load().pfsht_plan_get_info(self._h, C.byref(inf)))
+        self.info = {k: getattr(inf, k) for k, _ in _lib.PlanInfo._fields_}
+        self.info["kind"] = _lib.KINDS[inf.kind]
+        self.device = o.device
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _lib is not None and _lib._lib is not None:
+            _lib._lib.pfsht_plan_destroy(h)
+        self._h = None
+
+    def close(self):
+        self.__del__()
+
+    # -- reference queries --------------------------------------------------------------
+    @property
+    def algorithm(self) -> str:
+        """algorithm(plan) (src/Plan.jl:36)."""
+        return "DirectAlgorithm" if self.info["kind"] == "direct" else "StretchAlgorithm"
+
+    def ring_work(self) -> int:
+        """ring_work(plan) (src/Plan.jl:44): retained (l, m, ring) triples per apply."""
+        return int(_lib.load().pfsht_ring_work(self._h))
+
+    def workspace_bytes(self) -> int:
+        return int(_lib.load().pfsht_workspace_bytes(self._h))
+
+    def __repr__(self):
+        return (f"PartialFSHT.Plan(lmax={self.lmax}, npts={self.npts}, ntrans={self.ntrans}, "
+                f"spin=0, algorithm={self.algorithm})")
+
+    @property
+    def H(self) -> "AdjointPlan":
+        """plan' (src/Plan.jl:22)."""
+        return AdjointPlan(self)
+
+    adjoint = H
+
+    # -- applies ------------------------------------------------------------------------
+    def mul(self, f, alm, stream=None):
+        """mul!(f, plan, alm) (src/Plan.jl:137-141)."""
+        _check_array(alm, _coeff_shapes(self.lmax, self.ntrans), "coefficient array")
+        _check_array(f, _field_shapes(self.npts, self.ntrans), "field")
+        lib = _lib.load()
+        if _is_torch(alm) and alm.is_cuda:
+            if not (_is_torch(f) and f.is_cuda):
+                raise ValueError("alm and f must both be CUDA tensors or both host arrays")
+            _lib.check(lib.pfsht_forward(self._h, _ptr(alm), _ptr(f), _stream_of(alm, stream)), "mul!")
+        else:
+            if _is_torch(f) and f.is_cuda:
+                raise ValueError("alm and f must both be CUDA tensors or both host arrays")
+            _lib.check(lib.pfsht_forward_host(self._h, _ptr(alm), _ptr(f)), "mul!")
+        return f
+
+    def mul_adjoint(self, alm, f, stream=None):
+        """mul!(alm, plan', f) (src/Plan.jl:143-148); overwrites alm."""
+        _check_array(alm, _coeff_shapes(self.lmax, self.ntrans), "coefficient array")
+        _check_array(f, _field_shapes(self.npts, self.ntrans), "field")
+        lib = _lib.load()
+        if _is_torch(f) and f.is_cuda:
+            if not (_is_torch(alm) and alm.is_cuda):
+                raise ValueError("alm and f must both be CUDA tensors or both host arrays")
+            _lib.check(lib.pfsht_adjoint(self._h, _ptr(f), _ptr(alm), _stream_of(f, stream)), "mul!")
+        else:
+            if _is_torch(alm) and alm.is_cuda:
+                raise ValueError("alm and f must both be CUDA tensors or both host arrays")
+            _lib.check(lib.pfsht_adjoint_host(self._h, _ptr(f), _ptr(alm)), "mul!")
+        return alm
+
+    def __mul__(self, alm):
+        """plan * alm (src/Plan.jl:190-193)."""
+        dev = alm.device if (_is_torch(alm) and alm.is_cuda) else "cpu"
+        f = zeros_field(self.npts, self.ntrans, device=dev)
+        return self.mul(f, alm)
+
+    __matmul__ = __mul__
+
+
+class AdjointPlan:
+    """plan' (src/Plan.jl:18-23)."""
+
+    def __init__(self, parent: Plan):
+        self.parent = parent
+
+    @property
+    def H(self) -> Plan:
+        return self.parent
+
+    def mul(self, alm, f, stream=None):
+        return self.parent.mul_adjoint(alm, f, stream)
+
+    def __mul__(self, f):
+        """plan' * f (src/Plan.jl:195-199)."""
+        dev = f.device if (_is_torch(f) and f.is_cuda) else "cpu"
+        alm = zeros_alm(self.parent.lmax, self.parent.ntrans, device=dev)
+        return self.parent.mul_adjoint(alm, f)
+
+    __matmul__ = __mul__
+
+
+def mul(out, op, x, stream=None):
+    """mul!(out, op, x): forward for a Plan, adjoint for an AdjointPlan."""
+    if isinstance(op, Plan):
+        return op.mul(out, x, stream)
+    if isinstance(op, AdjointPlan):
+        return op.mul(out, x, stream)
+    raise TypeError("op must be a Plan or an AdjointPlan")
+
+
+# ---------------------------------------------------------------------------------------
+# lower seams used by parity tests
+# ---------------------------------------------------------------------------------------
+def ring_forward(plan: Plan, alm, G, stream=None):
+    """rings_from_alm! on the plan's ring set (src/Legendre.jl:310-323); G is a CUDA tensor
+    of Julia shape (nrings, 2lmax+1[, ntrans])."""
+    _lib.check(_lib.load().pfsht_ring_forward(plan._h, _ptr(alm), _ptr(G), _stream_of(alm, stream)),
+               "rings_from_alm!")
+    return G
+
+
+def ring_adjoint(plan: Plan, G, alm, stream=None):
+    """alm_from_rings! (src/Legendre.jl:332-341)."""
+    _lib.check(_lib.load().pfsht_ring_adjoint(plan._h, _ptr(G), _ptr(alm), _stream_of(G, stream)),
+               "alm_from_rings!")
+    return alm
+
+
+def plan_geometry(theta, phi, *, lmax, tol=1e-10, ntrans=1, method="auto",
+                  oversample_theta=1.0, oversample_phi=1.0, eps_apo_max=1.0) -> dict:
+    """Host-only: the geometry and sizes pfsht_plan_create would choose (no device used)."""
+    th = np.ascontiguousarray(theta, dtype=np.float64)
+    ph = np.ascontiguousarray(phi, dtype=np.float64)
+    o = _lib.default_opts()
+    o.method = _lib.METHODS[method]
+    o.oversample_theta = float(oversample_theta)
+    o.oversample_phi = float(oversample_phi)
+    o.eps_apo_max = float(eps_apo_max)
+    inf = _lib.PlanInfo()
+    _lib.check(_lib.load().pfsht_plan_geometry(th.ctypes.data, ph.ctypes.data, len(th), int(lmax),
+                                               int(ntrans), float(tol), C.byref(o), C.byref(inf)),
+               "plan_geometry")
+    d = {k: getattr(inf, k) for k, _ in _lib.PlanInfo._fields_}
+    d["kind"] = _lib.KINDS[inf.kind]
+    return d
+
+
+class NUFFT:
+    """The NUFFT seam (src/NUFFT.jl:17-25): 2-D type-1/2 NUFFT, modes (n1, n2) in FFT order,
+    host points; exec on CUDA tensors."""
+
+    def __init__(self, type, n1, n2, iflag, x, y, tol, ntrans=1):
+        xx = np.ascontiguousarray(x, dtype=np.float64)
+        yy = np.ascontiguousarray(y, dtype=np.float64)
+        h = C.c_void_p()
+        _lib.check(_lib.load().pfsht_nufft_create(int(type), int(n1), int(n2), int(iflag),
+                                                  int(ntrans), float(tol), xx.ctypes.data,
+                                                  yy.ctypes.data, len(xx), C.byref(h)),
+                   "_nufft_makeplan")
+        self._h = h
+        self.type, self.n1, self.n2, self.ntrans, self.M = int(type), int(n1), int(n2), int(ntrans), len(xx)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _lib is not None and _lib._lib is not None:
+            _lib._lib.pfsht_nufft_destroy(h)
+        self._h = None
+
+    def exec(self, inp, out, stream=None):
+        _lib.check(_lib.load().pfsht_nufft_exec(self._h, _ptr(inp), _ptr(out), _stream_of(inp, stream)),
+                   "_nufft_exec!")
+        return out

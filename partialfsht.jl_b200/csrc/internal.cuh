@@ -1,0 +1,158 @@
+// Internal declarations shared by the CUDA sources of libpfsht_b200.
+#pragma once
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "geometry.hpp"
+
+namespace pf {
+
+// ---------------------------------------------------------------------------------------
+// error plumbing (thread-local last error; C ABI returns codes)
+// ---------------------------------------------------------------------------------------
+void set_error(const std::string& msg);
+const std::string& get_error();
+
+struct Status {
+    int code = 0;
+    static Status ok() { return Status{}; }
+};
+
+#define PF_CUDA(call)                                                                   \
+    do {                                                                                \
+        cudaError_t _e = (call);                                                        \
+        if (_e != cudaSuccess) {                                                        \
+            ::pf::set_error(std::string(#call) + ": " + cudaGetErrorString(_e));       \
+            return _e == cudaErrorMemoryAllocation ? 5 : 4;                             \
+        }                                                                               \
+    } while (0)
+
+#define PF_CUFFT(call)                                                                  \
+    do {                                                                                \
+        cufftResult _r = (call);                                                        \
+        if (_r != CUFFT_SUCCESS) {                                                      \
+            ::pf::set_error(std::string(#call) + ": cuFFT error " + std::to_string((int)_r)); \
+            return _r == CUFFT_ALLOC_FAILED ? 5 : 4;                                    \
+        }                                                                               \
+    } while (0)
+
+#define PF_TRY(call)                                                                    \
+    do {                                                                                \
+        int _s = (call);                                                                \
+        if (_s != 0) return _s;                                                         \
+    } while (0)
+
+// device allocation owned by a plan; freed in the destructor
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    ~DevBuf();
+    int alloc(size_t n);
+    template <class T> T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+// ---------------------------------------------------------------------------------------
+// ring pass (ring.cu)
+// ---------------------------------------------------------------------------------------
+// One work item: order m, rings [j0, j0 + n) with n <= 32 * R.
+struct RingItem {
+    int m, j0, n, pad;
+};
+
+struct RingTables {
+    const double* cos_t = nullptr;    // nrings, reflection sign folded in
+    const double* log2sin = nullptr;  // nrings
+    const double* log2c = nullptr;    // lmax + 1
+    const double* w = nullptr;        // nrings window, or null for 1
+    const double2* ab = nullptr;      // recurrence coefficients, per m from l = m + 2
+    const int64_t* aboff = nullptr;   // lmax + 1 offsets into ab
+    int lmax = 0;
+    int nrings = 0;
+};
+
+// Layout of the ring-side array: column-major (ld x ncols x B), column of order m at
+// col_off + m; reflect writes/reads the mirrored row nrows - 1 - j too (DFS rows).
+struct RingOut {
+    int64_t ld = 0;       // leading dimension (rows)
+    int64_t bstride = 0;  // elements between transforms
+    int col_off = 0;
+    int nrows = 0;
+    int reflect = 0;
+    double spin_sgn = 1.0;
+};
+
+int build_ab_table(int lmax, int mmax, DevBuf& ab, DevBuf& aboff, cudaStream_t s);
+// items over the retained (m, ring) set, tiles of up to 32*R rings, heaviest first
+std::vector<RingItem> make_ring_items(const std::vector<int>& jlo, const std::vector<int>& jhi,
+                                      int lmax, int mmax, int R);
+// launchers: B transforms, alm complex (lmax+1, 2lmax+1, B)
+int ring_forward(const RingTables& t, const RingOut& o, const RingItem* d_items, int nitems,
+                 int R, const double2* alm, double2* out, int B, cudaStream_t s);
+int ring_adjoint(const RingTables& t, const RingOut& o, const RingItem* d_items, int nitems,
+                 int R, const double2* in, double2* alm, int B, cudaStream_t s);
+
+// ---------------------------------------------------------------------------------------
+// NUFFT stages (nufft.cu)
+// ---------------------------------------------------------------------------------------
+struct NufftGrid {
+    int w = 9;
+    double beta = 0;
+    int nf1 = 0, nf2 = 0;
+    int row0 = 0, nrows = 0;   // fine-grid rows [row0, row0 + nrows) (mod nf1) are kept
+    int row_wrap = 0;          // 1 when all nf1 rows are kept and taps wrap
+    int n1 = 0;                // modes along dim 1 (FFT order)
+    int ncols = 0;             // mode columns
+    int bin_rows = 16, bin_cols = 16, nbr = 0, nbc = 0;
+    int64_t M = 0;
+};
+
+struct NufftDev {
+    DevBuf pts;       // double2 (g1 - row0, g2) in bin order
+    DevBuf perm;      // int32 original index, bin order
+    DevBuf binstart;  // int32 nbins + 1
+    DevBuf colp2;     // int32 ncols: fine column of each mode column
+    DevBuf p2col;     // int32 nf2: mode column of each fine column or -1
+    DevBuf mult1;     // double2 n1: per-mode complex factor along dim 1 (deconv incl.)
+    DevBuf dec2;      // double ncols: deconvolution along dim 2
+    DevBuf pad;       // double2 nf1 x ncols x B
+    DevBuf U;         // double2 nrows x nf2 x B
+    cufftHandle f1 = 0, f2 = 0;
+    bool have_f1 = false, have_f2 = false;
+    ~NufftDev();
+};
+
+// transform points (x = stretched colatitude, y = longitude; both radians) into grid
+// coordinates, sort them into bins, fill pts/perm/binstart. x,y are device arrays.
+int nufft_setpts(NufftGrid& g, NufftDev& d, const double* x, const double* y, cudaStream_t s);
+// allocate pad/U and plan the fine-grid FFTs for B transforms
+int nufft_alloc(NufftGrid& g, NufftDev& d, int B);
+// type 2 from mode columns (n1 x ncols x B, FFT order along dim 1) to values f (M x B)
+int nufft_type2(const NufftGrid& g, NufftDev& d, const double2* modes, double2* f, int B,
+                int iflag, cudaStream_t s);
+// type 1 from values to mode columns
+int nufft_type1(const NufftGrid& g, NufftDev& d, const double2* f, double2* modes, int B,
+                int iflag, cudaStream_t s);
+
+// point transform of the leaf (src/Stretch.jl:202-213) on the device
+int leaf_points(const Geom& g, bool flip, const double* theta, const double* phi, int64_t M,
+                double* Theta, double* phi_out, cudaStream_t s);
+int minmax_device(const double* x, int64_t M, double* mn, double* mx, cudaStream_t s);
+
+// Direct leaf helpers (src/Direct.jl:279-336) on the device
+int direct_phase_sum(const double2* G, const double* phi, int64_t M, int lmax, int B,
+                     double2* f, cudaStream_t s);
+int direct_phase_spread(const double2* f, const double* phi, int64_t M, int lmax, int B,
+                        double2* G, cudaStream_t s);
+
+// DFS (src/DFS.jl:13-56)
+int dfs_double(const double2* F, double2* Ft, int Nth, int Nph, int B, int spin, cudaStream_t s);
+int dfs_fold(double2* F, const double2* Ft, int Nth, int Nph, int B, int spin, cudaStream_t s);
+
+// launch-error check after a kernel
+int check_launch(const char* what);
+
+}  // namespace pf

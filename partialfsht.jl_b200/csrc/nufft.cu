@@ -1,0 +1,654 @@
+// 2-D NUFFT of the stretched leaf and the NUFFT seam, on sm_100a: an exponential-of-
+// semicircle (ES) kernel NUFFT with upsampling 2 (the published FINUFFT algorithm that the
+// reference calls through ext/PartialFSHTFINUFFTExt.jl and ext/PartialFSHTcuFINUFFTExt.jl;
+// its exact semantics are DirectSum's, src/NUFFT.jl:155-199).
+//
+// Type 2 (modes -> values), per transform:
+//   pad   : mode columns (n1 x ncols, FFT order along dim 1) times the per-mode factors
+//           (deconvolution, and for the leaf the half-cell phase and 1/n_theta) into the
+//           zero-padded fine columns (nf1 x ncols)
+//   FFT   : along dim 1 (length nf1) on the ncols non-zero columns only
+//   rows  : the fine-grid rows that points can reach, [row0, row0 + nrows), transposed to
+//           row-major U (nrows x nf2) with the unused fine columns zero
+//   FFT   : along dim 2 (length nf2) on those rows only
+//   interp: w x w taps per point, points in bin order
+// Type 1 is the exact transpose (spread -> FFT -> rows^T -> FFT -> unpad).
+//
+// Points are transformed and bin-sorted on the device at plan time (radix sort on bin key).
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+
+#include "internal.cuh"
+
+namespace pf {
+
+DevBuf::~DevBuf() {
+    if (p) cudaFree(p);
+}
+
+int DevBuf::alloc(size_t n) {
+    if (p) {
+        cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    if (n == 0) n = 16;
+    cudaError_t e = cudaMalloc(&p, n);
+    if (e != cudaSuccess) {
+        p = nullptr;
+        set_error(std::string("cudaMalloc of ") + std::to_string(n) + " bytes: " +
+                  cudaGetErrorString(e));
+        return 5;
+    }
+    bytes = n;
+    return 0;
+}
+
+NufftDev::~NufftDev() {
+    if (have_f1) cufftDestroy(f1);
+    if (have_f2) cufftDestroy(f2);
+}
+
+int check_launch(const char* what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error(std::string(what) + ": " + cudaGetErrorString(e));
+        return 4;
+    }
+    return 0;
+}
+
+static inline unsigned nblk(int64_t n, int bs) {
+    int64_t b = (n + bs - 1) / bs;
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>(b, 1 << 20));
+}
+
+// ---------------------------------------------------------------------------------------
+// leaf point transform (src/Stretch.jl:202-213, src/Windows.jl:289-298)
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ double dev_jl_mod(double x, double y) {
+    double r = fmod(x, y);
+    if (r == 0.0) return copysign(r, y);
+    if ((r > 0) != (y > 0)) return r + y;
+    return r;
+}
+
+__global__ void leaf_points_kernel(int kind, int north, double thmax, double lo_ext,
+                                   double period, int flip, const double* __restrict__ theta,
+                                   const double* __restrict__ phi, int64_t M,
+                                   double* __restrict__ Th, double* __restrict__ ph) {
+    const double pi = 3.141592653589793;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < M;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        double t = theta[i];
+        if (flip) t = pi - t;
+        double T;
+        if (kind == kFull) {
+            T = t;
+        } else if (kind == kPole) {
+            const double d = north ? t : pi - t;
+            T = pi * d / thmax;
+        } else {
+            T = 2 * pi * (t - lo_ext) / period;
+        }
+        Th[i] = T;
+        ph[i] = dev_jl_mod(phi[i], 2 * pi);
+    }
+}
+
+int leaf_points(const Geom& g, bool flip, const double* theta, const double* phi, int64_t M,
+                double* Th, double* ph, cudaStream_t s) {
+    const double thmax = g.h * (1 + g.eps_apo);
+    const int north = g.lo <= std::sqrt(2.220446049250313e-16) ? 1 : 0;
+    const double lo_ext = g.lo - g.h * g.eps_apo;
+    leaf_points_kernel<<<nblk(M, 256), 256, 0, s>>>(g.kind, north, thmax, lo_ext, g.period,
+                                                    flip ? 1 : 0, theta, phi, M, Th, ph);
+    return check_launch("leaf_points_kernel");
+}
+
+int minmax_device(const double* x, int64_t M, double* mn, double* mx, cudaStream_t s) {
+    DevBuf out, tmp;
+    PF_TRY(out.alloc(2 * sizeof(double)));
+    size_t tb = 0, tb2 = 0;
+    PF_CUDA(cub::DeviceReduce::Min(nullptr, tb, x, out.as<double>(), (int)M, s));
+    PF_CUDA(cub::DeviceReduce::Max(nullptr, tb2, x, out.as<double>() + 1, (int)M, s));
+    PF_TRY(tmp.alloc(std::max(tb, tb2)));
+    PF_CUDA(cub::DeviceReduce::Min(tmp.p, tb, x, out.as<double>(), (int)M, s));
+    PF_CUDA(cub::DeviceReduce::Max(tmp.p, tb2, x, out.as<double>() + 1, (int)M, s));
+    double h[2];
+    PF_CUDA(cudaMemcpyAsync(h, out.p, sizeof(h), cudaMemcpyDeviceToHost, s));
+    PF_CUDA(cudaStreamSynchronize(s));
+    *mn = h[0];
+    *mx = h[1];
+    return 0;
+}
+
+// ---------------------------------------------------------------------------------------
+// plan-time: grid coordinates, bin keys, sort
+// ---------------------------------------------------------------------------------------
+__global__ void bin_keys_kernel(const double* __restrict__ x, const double* __restrict__ y,
+                                int64_t M, double s1, double s2, int row0, int row_wrap,
+                                int nf1, int nf2, int bin_rows, int bin_cols, int nbr, int nbc,
+                                double2* __restrict__ g, int* __restrict__ key,
+                                int* __restrict__ idx, int* __restrict__ counts) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < M;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        double g1 = x[i] * s1;
+        double g2 = y[i] * s2;
+        if (row_wrap) {
+            g1 = dev_jl_mod(g1, (double)nf1);
+            if (g1 >= nf1) g1 -= nf1;
+        } else {
+            g1 = g1 - (double)row0;
+        }
+        g2 = dev_jl_mod(g2, (double)nf2);
+        if (g2 >= nf2) g2 -= nf2;
+        int br = (int)floor(g1 / bin_rows);
+        int bc = (int)floor(g2 / bin_cols);
+        br = min(max(br, 0), nbr - 1);
+        bc = min(max(bc, 0), nbc - 1);
+        const int k = br * nbc + bc;
+        g[i] = make_double2(g1, g2);
+        key[i] = k;
+        idx[i] = (int)i;
+        atomicAdd(counts + k, 1);
+    }
+}
+
+__global__ void gather_points_kernel(const double2* __restrict__ g, const int* __restrict__ sidx,
+                                     int64_t M, double2* __restrict__ pts, int* __restrict__ perm) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < M;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int j = sidx[i];
+        pts[i] = g[j];
+        perm[i] = j;
+    }
+}
+
+int nufft_setpts(NufftGrid& g, NufftDev& d, const double* x, const double* y, cudaStream_t s) {
+    const int64_t M = g.M;
+    if (M > INT32_MAX) {
+        set_error("more than 2^31-1 points in one plan");
+        return 1;
+    }
+    g.nbr = std::max(1, (g.nrows + g.bin_rows - 1) / g.bin_rows);
+    g.nbc = std::max(1, (g.nf2 + g.bin_cols - 1) / g.bin_cols);
+    const int nbins = g.nbr * g.nbc;
+    DevBuf gg, key, key2, idx, idx2, counts, tmp;
+    PF_TRY(gg.alloc(sizeof(double2) * M));
+    PF_TRY(key.alloc(sizeof(int) * M));
+    PF_TRY(key2.alloc(sizeof(int) * M));
+    PF_TRY(idx.alloc(sizeof(int) * M));
+    PF_TRY(idx2.alloc(sizeof(int) * M));
+    PF_TRY(counts.alloc(sizeof(int) * (nbins + 1)));
+    PF_TRY(d.binstart.alloc(sizeof(int) * (nbins + 1)));
+    PF_TRY(d.pts.alloc(sizeof(double2) * M));
+    PF_TRY(d.perm.alloc(sizeof(int) * M));
+    PF_CUDA(cudaMemsetAsync(counts.p, 0, sizeof(int) * (nbins + 1), s));
+    const double s1 = (double)g.nf1 / (2 * M_PI), s2 = (double)g.nf2 / (2 * M_PI);
+    bin_keys_kernel<<<nblk(M, 256), 256, 0, s>>>(x, y, M, s1, s2, g.row0, g.row_wrap, g.nf1,
+                                                 g.nf2, g.bin_rows, g.bin_cols, g.nbr, g.nbc,
+                                                 gg.as<double2>(), key.as<int>(), idx.as<int>(),
+                                                 counts.as<int>());
+    PF_TRY(check_launch("bin_keys_kernel"));
+    int end_bit = 1;
+    while ((1 << end_bit) < nbins + 1 && end_bit < 31) ++end_bit;
+    size_t tb = 0, tb2 = 0;
+    PF_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, key.as<int>(), key2.as<int>(),
+                                            idx.as<int>(), idx2.as<int>(), (int)M, 0, end_bit, s));
+    PF_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb2, counts.as<int>(), d.binstart.as<int>(),
+                                          nbins + 1, s));
+    PF_TRY(tmp.alloc(std::max(tb, tb2)));
+    PF_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tb, key.as<int>(), key2.as<int>(),
+                                            idx.as<int>(), idx2.as<int>(), (int)M, 0, end_bit, s));
+    PF_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, tb2, counts.as<int>(), d.binstart.as<int>(),
+                                          nbins + 1, s));
+    gather_points_kernel<<<nblk(M, 256), 256, 0, s>>>(gg.as<double2>(), idx2.as<int>(), M,
+                                                      d.pts.as<double2>(), d.perm.as<int>());
+    PF_TRY(check_launch("gather_points_kernel"));
+    // temporaries are freed when this returns, so finish using them first
+    PF_CUDA(cudaStreamSynchronize(s));
+    return 0;
+}
+
+int nufft_alloc(NufftGrid& g, NufftDev& d, int B) {
+    PF_TRY(d.pad.alloc(sizeof(double2) * (size_t)g.nf1 * g.ncols * B));
+    PF_TRY(d.U.alloc(sizeof(double2) * (size_t)g.nrows * g.nf2 * B));
+    int n1[1] = {g.nf1};
+    PF_CUFFT(cufftPlanMany(&d.f1, 1, n1, n1, 1, g.nf1, n1, 1, g.nf1, CUFFT_Z2Z, g.ncols * B));
+    d.have_f1 = true;
+    int n2[1] = {g.nf2};
+    PF_CUFFT(cufftPlanMany(&d.f2, 1, n2, n2, 1, g.nf2, n2, 1, g.nf2, CUFFT_Z2Z, g.nrows * B));
+    d.have_f2 = true;
+    return 0;
+}
+
+// ---------------------------------------------------------------------------------------
+// pad / unpad along dim 1
+// ---------------------------------------------------------------------------------------
+__global__ void pad_kernel(const double2* __restrict__ in, int n1, int ncols, int nf1,
+                           const double2* __restrict__ mult1, const double* __restrict__ dec2,
+                           double2* __restrict__ pad) {
+    const int c = blockIdx.y, b = blockIdx.z;
+    const int pos = (n1 + 1) / 2, neg = n1 / 2;
+    const double2* ic = in + (int64_t)n1 * c + (int64_t)n1 * ncols * b;
+    double2* oc = pad + (int64_t)nf1 * c + (int64_t)nf1 * ncols * b;
+    const double d2 = dec2[c];
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < nf1; p += gridDim.x * blockDim.x) {
+        int i1 = -1;
+        if (p < pos) i1 = p;
+        else if (p >= nf1 - neg) i1 = n1 + (p - nf1);
+        double2 v = make_double2(0.0, 0.0);
+        if (i1 >= 0) {
+            const double2 a = ic[i1];
+            const double2 f = mult1[i1];
+            v.x = (a.x * f.x - a.y * f.y) * d2;
+            v.y = (a.x * f.y + a.y * f.x) * d2;
+        }
+        oc[p] = v;
+    }
+}
+
+__global__ void unpad_kernel(const double2* __restrict__ pad, int n1, int ncols, int nf1,
+                             const double2* __restrict__ mult1, const double* __restrict__ dec2,
+                             double2* __restrict__ out) {
+    const int c = blockIdx.y, b = blockIdx.z;
+    const double2* ic = pad + (int64_t)nf1 * c + (int64_t)nf1 * ncols * b;
+    double2* oc = out + (int64_t)n1 * c + (int64_t)n1 * ncols * b;
+    const double d2 = dec2[c];
+    for (int i1 = blockIdx.x * blockDim.x + threadIdx.x; i1 < n1; i1 += gridDim.x * blockDim.x) {
+        const int k1 = i1 < (n1 + 1) / 2 ? i1 : i1 - n1;
+        const int p = k1 >= 0 ? k1 : nf1 + k1;
+        const double2 a = ic[p];
+        const double2 f = mult1[i1];  // conj(f)
+        double2 v;
+        v.x = (a.x * f.x + a.y * f.y) * d2;
+        v.y = (a.y * f.x - a.x * f.y) * d2;
+        oc[i1] = v;
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// fine rows <-> fine columns (tile transpose through shared memory)
+// ---------------------------------------------------------------------------------------
+// U[r, p2] = pad[(row0 + r) mod nf1, p2col[p2]] (or 0)
+__global__ void rows_fwd_kernel(const double2* __restrict__ pad, int nf1, int ncols, int row0,
+                                int nrows, int nf2, const int* __restrict__ p2col,
+                                double2* __restrict__ U) {
+    __shared__ double2 tile[32][33];
+    const int b = blockIdx.z;
+    const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;  // c0 indexes p2
+    const double2* pb = pad + (int64_t)nf1 * ncols * b;
+    double2* ub = U + (int64_t)nrows * nf2 * b;
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int p2 = c0 + k;
+        const int r = r0 + threadIdx.x;
+        double2 v = make_double2(0.0, 0.0);
+        if (p2 < nf2 && r < nrows) {
+            const int c = p2col[p2];
+            if (c >= 0) {
+                int p1 = row0 + r;
+                p1 %= nf1;
+                if (p1 < 0) p1 += nf1;
+                v = pb[p1 + (int64_t)nf1 * c];
+            }
+        }
+        tile[k][threadIdx.x] = v;
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int r = r0 + k;
+        const int p2 = c0 + threadIdx.x;
+        if (r < nrows && p2 < nf2) ub[(int64_t)r * nf2 + p2] = tile[threadIdx.x][k];
+    }
+}
+
+// pad[p1, c] = U[(p1 - row0) mod nf1, colp2[c]] when that row is kept, else 0
+__global__ void rows_adj_kernel(const double2* __restrict__ U, int nf1, int ncols, int row0,
+                                int nrows, int nf2, const int* __restrict__ colp2,
+                                double2* __restrict__ pad) {
+    __shared__ double2 tile[32][33];
+    const int b = blockIdx.z;
+    const int p0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+    const double2* ub = U + (int64_t)nrows * nf2 * b;
+    double2* pb = pad + (int64_t)nf1 * ncols * b;
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int p1 = p0 + k;
+        const int c = c0 + threadIdx.x;
+        double2 v = make_double2(0.0, 0.0);
+        if (p1 < nf1 && c < ncols) {
+            int r = (p1 - row0) % nf1;
+            if (r < 0) r += nf1;
+            if (r < nrows) v = ub[(int64_t)r * nf2 + colp2[c]];
+        }
+        tile[k][threadIdx.x] = v;
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int c = c0 + k;
+        const int p1 = p0 + threadIdx.x;
+        if (c < ncols && p1 < nf1) pb[p1 + (int64_t)nf1 * c] = tile[threadIdx.x][k];
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// interpolation and spreading
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ double es_ker(double z, double beta) {
+    return fabs(z) >= 1.0 ? 0.0 : exp(beta * (sqrt(1.0 - z * z) - 1.0));
+}
+
+template <int W>
+__device__ __forceinline__ int taps(double g, double beta, double* k) {
+    constexpr double hw = 0.5 * W;
+    const int i0 = (int)ceil(g - hw);
+#pragma unroll
+    for (int a = 0; a < W; ++a) k[a] = es_ker(((double)(i0 + a) - g) / hw, beta);
+    return i0;
+}
+
+__device__ __forceinline__ int wrap(int i, int n) {
+    int r = i % n;
+    return r < 0 ? r + n : r;
+}
+
+template <int W>
+__global__ void __launch_bounds__(256)
+interp_kernel(const double2* __restrict__ pts, const int* __restrict__ perm, int64_t M,
+              const double2* __restrict__ U, int nrows, int nf2, int row_wrap, double beta,
+              int B, double2* __restrict__ f) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < M;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const double2 g = pts[i];
+        double k1[W], k2[W];
+        const int i10 = taps<W>(g.x, beta, k1);
+        const int i20 = taps<W>(g.y, beta, k2);
+        int col[W];
+#pragma unroll
+        for (int c = 0; c < W; ++c) col[c] = wrap(i20 + c, nf2);
+        const int j = perm[i];
+        for (int b = 0; b < B; ++b) {
+            const double2* ub = U + (int64_t)nrows * nf2 * b;
+            double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+            for (int a = 0; a < W; ++a) {
+                int r = i10 + a;
+                if (row_wrap) r = wrap(r, nrows);
+                if (r < 0 || r >= nrows) continue;
+                const double2* row = ub + (int64_t)r * nf2;
+                double2 s = make_double2(0.0, 0.0);
+#pragma unroll
+                for (int c = 0; c < W; ++c) {
+                    const double2 u = row[col[c]];
+                    s.x = fma(u.x, k2[c], s.x);
+                    s.y = fma(u.y, k2[c], s.y);
+                }
+                acc.x = fma(s.x, k1[a], acc.x);
+                acc.y = fma(s.y, k1[a], acc.y);
+            }
+            f[j + M * b] = acc;
+        }
+    }
+}
+
+// one CTA per bin: spread the bin's points into a shared tile, then add the tile to U
+template <int W>
+__global__ void __launch_bounds__(256)
+spread_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
+              const int* __restrict__ binstart, int nbc, int bin_rows, int bin_cols, int64_t M,
+              const double2* __restrict__ fin, int b, int nrows, int nf2, int row_wrap,
+              double beta, double2* __restrict__ U) {
+    extern __shared__ double2 tile[];
+    const int bin = blockIdx.x;
+    const int s = binstart[bin], e = binstart[bin + 1];
+    if (s == e) return;
+    const int br = bin / nbc, bc = bin % nbc;
+    constexpr int hc = (W + 1) / 2;
+    const int TR = bin_rows + W + 1, TC = bin_cols + W + 1;
+    const int tr0 = br * bin_rows - hc, tc0 = bc * bin_cols - hc;
+    for (int t = threadIdx.x; t < TR * TC; t += blockDim.x) tile[t] = make_double2(0.0, 0.0);
+    __syncthreads();
+    for (int p = s + threadIdx.x; p < e; p += blockDim.x) {
+        const double2 g = pts[p];
+        const double2 v = fin[perm[p] + M * b];
+        double k1[W], k2[W];
+        const int i10 = taps<W>(g.x, beta, k1) - tr0;
+        const int i20 = taps<W>(g.y, beta, k2) - tc0;
+#pragma unroll
+        for (int a = 0; a < W; ++a) {
+            const int rr = i10 + a;
+            if (rr < 0 || rr >= TR) continue;
+            const double vx = v.x * k1[a], vy = v.y * k1[a];
+#pragma unroll
+            for (int c = 0; c < W; ++c) {
+                const int cc = i20 + c;
+                if (cc < 0 || cc >= TC) continue;
+                double* q = reinterpret_cast<double*>(&tile[rr * TC + cc]);
+                atomicAdd(q, vx * k2[c]);
+                atomicAdd(q + 1, vy * k2[c]);
+            }
+        }
+    }
+    __syncthreads();
+    double2* ub = U + (int64_t)nrows * nf2 * b;
+    for (int t = threadIdx.x; t < TR * TC; t += blockDim.x) {
+        const double2 v = tile[t];
+        if (v.x == 0.0 && v.y == 0.0) continue;
+        int r = tr0 + t / TC;
+        if (row_wrap) r = wrap(r, nrows);
+        if (r < 0 || r >= nrows) continue;
+        const int c = wrap(tc0 + t % TC, nf2);
+        double* q = reinterpret_cast<double*>(ub + (int64_t)r * nf2 + c);
+        atomicAdd(q, v.x);
+        atomicAdd(q + 1, v.y);
+    }
+}
+
+template <int W>
+static int launch_interp(const NufftGrid& g, NufftDev& d, double2* f, int B, cudaStream_t s) {
+    interp_kernel<W><<<nblk(g.M, 256), 256, 0, s>>>(d.pts.as<double2>(), d.perm.as<int>(), g.M,
+                                                     d.U.as<double2>(), g.nrows, g.nf2,
+                                                     g.row_wrap, g.beta, B, f);
+    return check_launch("interp_kernel");
+}
+
+template <int W>
+static int launch_spread(const NufftGrid& g, NufftDev& d, const double2* f, int B, cudaStream_t s) {
+    const size_t smem = sizeof(double2) * (g.bin_rows + W + 1) * (g.bin_cols + W + 1);
+    if (smem > 48 * 1024)
+        PF_CUDA(cudaFuncSetAttribute(spread_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+    for (int b = 0; b < B; ++b) {
+        spread_kernel<W><<<g.nbr * g.nbc, 256, smem, s>>>(
+            d.pts.as<double2>(), d.perm.as<int>(), d.binstart.as<int>(), g.nbc, g.bin_rows,
+            g.bin_cols, g.M, f, b, g.nrows, g.nf2, g.row_wrap, g.beta, d.U.as<double2>());
+        PF_TRY(check_launch("spread_kernel"));
+    }
+    return 0;
+}
+
+static int interp_any(const NufftGrid& g, NufftDev& d, double2* f, int B, cudaStream_t s) {
+#define PF_CALL(WW) launch_interp<WW>(g, d, f, B, s)
+    switch (g.w) {
+        case 2: return PF_CALL(2); case 3: return PF_CALL(3); case 4: return PF_CALL(4);
+        case 5: return PF_CALL(5); case 6: return PF_CALL(6); case 7: return PF_CALL(7);
+        case 8: return PF_CALL(8); case 9: return PF_CALL(9); case 10: return PF_CALL(10);
+        case 11: return PF_CALL(11); case 12: return PF_CALL(12); case 13: return PF_CALL(13);
+        case 14: return PF_CALL(14); case 15: return PF_CALL(15); case 16: return PF_CALL(16);
+        default: set_error("unsupported NUFFT kernel width"); return 7;
+    }
+#undef PF_CALL
+}
+
+static int spread_any(const NufftGrid& g, NufftDev& d, const double2* f, int B, cudaStream_t s) {
+#define PF_CALL(WW) launch_spread<WW>(g, d, f, B, s)
+    switch (g.w) {
+        case 2: return PF_CALL(2); case 3: return PF_CALL(3); case 4: return PF_CALL(4);
+        case 5: return PF_CALL(5); case 6: return PF_CALL(6); case 7: return PF_CALL(7);
+        case 8: return PF_CALL(8); case 9: return PF_CALL(9); case 10: return PF_CALL(10);
+        case 11: return PF_CALL(11); case 12: return PF_CALL(12); case 13: return PF_CALL(13);
+        case 14: return PF_CALL(14); case 15: return PF_CALL(15); case 16: return PF_CALL(16);
+        default: set_error("unsupported NUFFT kernel width"); return 7;
+    }
+#undef PF_CALL
+}
+
+int nufft_type2(const NufftGrid& g, NufftDev& d, const double2* modes, double2* f, int B,
+                int iflag, cudaStream_t s) {
+    const int dir = iflag > 0 ? CUFFT_INVERSE : CUFFT_FORWARD;
+    {
+        dim3 grid(nblk(g.nf1, 256), g.ncols, B);
+        pad_kernel<<<grid, 256, 0, s>>>(modes, g.n1, g.ncols, g.nf1, d.mult1.as<double2>(),
+                                        d.dec2.as<double>(), d.pad.as<double2>());
+        PF_TRY(check_launch("pad_kernel"));
+    }
+    PF_CUFFT(cufftSetStream(d.f1, s));
+    PF_CUFFT(cufftExecZ2Z(d.f1, d.pad.as<cufftDoubleComplex>(), d.pad.as<cufftDoubleComplex>(), dir));
+    {
+        dim3 grid((g.nf2 + 31) / 32, (g.nrows + 31) / 32, B);
+        rows_fwd_kernel<<<grid, dim3(32, 8), 0, s>>>(d.pad.as<double2>(), g.nf1, g.ncols, g.row0,
+                                                     g.nrows, g.nf2, d.p2col.as<int>(),
+                                                     d.U.as<double2>());
+        PF_TRY(check_launch("rows_fwd_kernel"));
+    }
+    PF_CUFFT(cufftSetStream(d.f2, s));
+    PF_CUFFT(cufftExecZ2Z(d.f2, d.U.as<cufftDoubleComplex>(), d.U.as<cufftDoubleComplex>(), dir));
+    return interp_any(g, d, f, B, s);
+}
+
+int nufft_type1(const NufftGrid& g, NufftDev& d, const double2* f, double2* modes, int B,
+                int iflag, cudaStream_t s) {
+    const int dir = iflag > 0 ? CUFFT_INVERSE : CUFFT_FORWARD;
+    PF_CUDA(cudaMemsetAsync(d.U.p, 0, sizeof(double2) * (size_t)g.nrows * g.nf2 * B, s));
+    PF_TRY(spread_any(g, d, f, B, s));
+    PF_CUFFT(cufftSetStream(d.f2, s));
+    PF_CUFFT(cufftExecZ2Z(d.f2, d.U.as<cufftDoubleComplex>(), d.U.as<cufftDoubleComplex>(), dir));
+    {
+        dim3 grid((g.ncols + 31) / 32, (g.nf1 + 31) / 32, B);
+        rows_adj_kernel<<<grid, dim3(32, 8), 0, s>>>(d.U.as<double2>(), g.nf1, g.ncols, g.row0,
+                                                     g.nrows, g.nf2, d.colp2.as<int>(),
+                                                     d.pad.as<double2>());
+        PF_TRY(check_launch("rows_adj_kernel"));
+    }
+    PF_CUFFT(cufftSetStream(d.f1, s));
+    PF_CUFFT(cufftExecZ2Z(d.f1, d.pad.as<cufftDoubleComplex>(), d.pad.as<cufftDoubleComplex>(), dir));
+    {
+        dim3 grid(nblk(g.n1, 256), g.ncols, B);
+        unpad_kernel<<<grid, 256, 0, s>>>(d.pad.as<double2>(), g.n1, g.ncols, g.nf1,
+                                          d.mult1.as<double2>(), d.dec2.as<double>(), modes);
+        PF_TRY(check_launch("unpad_kernel"));
+    }
+    return 0;
+}
+
+// ---------------------------------------------------------------------------------------
+// Direct leaf phases (src/Direct.jl:287-333): exact cis(m phi) per (point, order)
+// ---------------------------------------------------------------------------------------
+__global__ void direct_sum_kernel(const double2* __restrict__ G, const double* __restrict__ phi,
+                                  int64_t M, int L, int B, double2* __restrict__ f) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < M;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const double ph = phi[i];
+        for (int b = 0; b < B; ++b) {
+            const double2* Gb = G + (int64_t)M * (2 * L + 1) * b;
+            double2 acc = Gb[i + M * (int64_t)L];
+            for (int m = 1; m <= L; ++m) {
+                double sn, cs;
+                sincos((double)m * ph, &sn, &cs);
+                const double2 gp = Gb[i + M * (int64_t)(L + m)];
+                const double2 gm = Gb[i + M * (int64_t)(L - m)];
+                acc.x += (gp.x * cs - gp.y * sn) + (gm.x * cs + gm.y * sn);
+                acc.y += (gp.x * sn + gp.y * cs) + (gm.y * cs - gm.x * sn);
+            }
+            f[i + M * b] = acc;
+        }
+    }
+}
+
+__global__ void direct_spread_kernel(const double2* __restrict__ f, const double* __restrict__ phi,
+                                     int64_t M, int L, int B, double2* __restrict__ G) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < M;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const double ph = phi[i];
+        for (int b = 0; b < B; ++b) {
+            double2* Gb = G + (int64_t)M * (2 * L + 1) * b;
+            const double2 v = f[i + M * b];
+            Gb[i + M * (int64_t)L] = v;
+            for (int m = 1; m <= L; ++m) {
+                double sn, cs;
+                sincos((double)m * ph, &sn, &cs);
+                Gb[i + M * (int64_t)(L + m)] = make_double2(v.x * cs + v.y * sn, v.y * cs - v.x * sn);
+                Gb[i + M * (int64_t)(L - m)] = make_double2(v.x * cs - v.y * sn, v.y * cs + v.x * sn);
+            }
+        }
+    }
+}
+
+int direct_phase_sum(const double2* G, const double* phi, int64_t M, int L, int B, double2* f,
+                     cudaStream_t s) {
+    direct_sum_kernel<<<nblk(M, 128), 128, 0, s>>>(G, phi, M, L, B, f);
+    return check_launch("direct_sum_kernel");
+}
+
+int direct_phase_spread(const double2* f, const double* phi, int64_t M, int L, int B, double2* G,
+                        cudaStream_t s) {
+    direct_spread_kernel<<<nblk(M, 128), 128, 0, s>>>(f, phi, M, L, B, G);
+    return check_launch("direct_spread_kernel");
+}
+
+// ---------------------------------------------------------------------------------------
+// DFS periodisation (src/DFS.jl:13-56)
+// ---------------------------------------------------------------------------------------
+__global__ void dfs_double_kernel(const double2* __restrict__ F, double2* __restrict__ Ft, int Nth,
+                                  int Nph, int B, double sgn) {
+    const int64_t n = (int64_t)2 * Nth * Nph * B;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(t % (2 * Nth));
+        const int64_t rest = t / (2 * Nth);
+        const int j = (int)(rest % Nph);
+        const int b = (int)(rest / Nph);
+        double2 v;
+        if (i < Nth) {
+            v = F[i + (int64_t)Nth * j + (int64_t)Nth * Nph * b];
+        } else {
+            const int ii = i - Nth;
+            const int js = (j + Nph / 2) % Nph;
+            const double2 u = F[(Nth - 1 - ii) + (int64_t)Nth * js + (int64_t)Nth * Nph * b];
+            v = make_double2(sgn * u.x, sgn * u.y);
+        }
+        Ft[t] = v;
+    }
+}
+
+__global__ void dfs_fold_kernel(double2* __restrict__ F, const double2* __restrict__ Ft, int Nth,
+                                int Nph, int B, double sgn) {
+    const int64_t n = (int64_t)Nth * Nph * B;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(t % Nth);
+        const int64_t rest = t / Nth;
+        const int j = (int)(rest % Nph);
+        const int b = (int)(rest / Nph);
+        const int js = ((j - Nph / 2) % Nph + Nph) % Nph;
+        const double2 a = Ft[i + (int64_t)2 * Nth * j + (int64_t)2 * Nth * Nph * b];
+        const double2 u = Ft[(2 * Nth - 1 - i) + (int64_t)2 * Nth * js + (int64_t)2 * Nth * Nph * b];
+        F[t] = make_double2(a.x + sgn * u.x, a.y + sgn * u.y);
+    }
+}
+
+int dfs_double(const double2* F, double2* Ft, int Nth, int Nph, int B, int spin, cudaStream_t s) {
+    const double sgn = (spin % 2 == 0) ? 1.0 : -1.0;
+    dfs_double_kernel<<<nblk((int64_t)2 * Nth * Nph * B, 256), 256, 0, s>>>(F, Ft, Nth, Nph, B, sgn);
+    return check_launch("dfs_double_kernel");
+}
+
+int dfs_fold(double2* F, const double2* Ft, int Nth, int Nph, int B, int spin, cudaStream_t s) {
+    const double sgn = (spin % 2 == 0) ? 1.0 : -1.0;
+    dfs_fold_kernel<<<nblk((int64_t)Nth * Nph * B, 256), 256, 0, s>>>(F, Ft, Nth, Nph, B, sgn);
+    return check_launch("dfs_fold_kernel");
+}
+
+}  // namespace pf

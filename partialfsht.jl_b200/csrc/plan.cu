@@ -1,0 +1,712 @@
+// libpfsht_b200: plan construction and the C ABI (include/pfsht_b200.h).
+//
+// A plan is PartialFSHT.jl's Plan + StretchLeaf (src/Plan.jl:84-116, src/Stretch.jl:129-248)
+// on one device: geometry and sizes on the host, the point transform, bin sort and
+// recurrence tables on the device, and an apply that runs
+//   forward : ring pass -> FFT along Theta -> NUFFT type 2         (src/Stretch.jl:262-277)
+//   adjoint : NUFFT type 1 -> inverse FFT along Theta -> ring pass (src/Stretch.jl:279-295)
+// The reference's pack / bfft-along-phi / window / DFS / 2-D FFT / phase sequence
+// (src/Stretch.jl:269-273) is applied in closed form: the phi shift by pi of the DFS
+// reflection is (-1)^m on order columns and fft_phi o bfft_phi = n_phi I on the packed
+// orders, so the whole sequence is, per retained order column, the window and the mirrored
+// DFS rows (written by the ring pass) followed by one FFT along Theta and the half-cell
+// phase / n_theta (folded into the NUFFT's per-mode factor).
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/pfsht_b200.h"
+#include "internal.cuh"
+
+namespace pf {
+
+static thread_local std::string g_err;
+void set_error(const std::string& msg) { g_err = msg; }
+const std::string& get_error() { return g_err; }
+
+}  // namespace pf
+
+using namespace pf;
+
+struct pfsht_plan {
+    int device = 0;
+    int precision = 0;
+    int kind = kPole;
+    int L = 0, B = 1;
+    int64_t M = 0;
+    double tol = 0;
+    int R = 4;
+    Leaf leaf;
+    int ncols = 0;
+    int nrings = 0;
+    // ring pass
+    DevBuf cos_t, log2sin, log2c, w, ab, aboff, items;
+    int nitems = 0;
+    RingTables rt;
+    RingOut ro_cols;  // the apply's column array H (or G for the direct leaf)
+    // column array: nth x ncols x B (stretch) or M x (2L+1) x B (direct)
+    DevBuf H;
+    cufftHandle fth = 0;
+    bool have_fth = false;
+    // NUFFT
+    NufftGrid ng;
+    NufftDev nd;
+    // direct leaf
+    DevBuf phi_pts;
+    // host-buffer staging
+    DevBuf st_alm, st_f;
+    cudaStream_t st_stream = nullptr;
+    pfsht_plan_info info{};
+    ~pfsht_plan() {
+        if (have_fth) cufftDestroy(fth);
+        if (st_stream) cudaStreamDestroy(st_stream);
+    }
+};
+
+struct pfsht_nufft {
+    int device = 0;
+    int type = 2, iflag = 1, B = 1;
+    int n1 = 0, n2 = 0;
+    int64_t M = 0;
+    NufftGrid g;
+    NufftDev d;
+};
+
+namespace {
+
+int fail(int code, const std::string& msg) {
+    set_error(msg);
+    return code;
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (dev >= 0 && dev != prev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+template <class T>
+int upload(DevBuf& d, const std::vector<T>& h, cudaStream_t s) {
+    PF_TRY(d.alloc(sizeof(T) * std::max<size_t>(h.size(), 1)));
+    if (!h.empty()) PF_CUDA(cudaMemcpyAsync(d.p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, s));
+    PF_CUDA(cudaStreamSynchronize(s));
+    return 0;
+}
+
+int mode_k(int i, int n) { return i < (n + 1) / 2 ? i : i - n; }
+
+// NUFFT grid and per-mode factors; n1 modes along dim 1, columns -> k2 via colk2
+int setup_nufft_grid(NufftGrid& g, NufftDev& d, int n1, int nmodes2, const std::vector<int>& colk2,
+                     const std::vector<double2>& phase1, double tol, int64_t M, double xmin,
+                     double xmax, bool full_rows, int bin_rows, int bin_cols, cudaStream_t s) {
+    g.w = es_width(tol);
+    g.beta = 2.30 * g.w;
+    g.nf1 = (int)next_smooth(std::max<int64_t>(2 * (int64_t)n1, 2 * g.w));
+    g.nf2 = (int)next_smooth(std::max<int64_t>(2 * (int64_t)nmodes2, 2 * g.w));
+    g.n1 = n1;
+    g.ncols = (int)colk2.size();
+    g.M = M;
+    g.bin_rows = bin_rows > 0 ? bin_rows : 16;
+    g.bin_cols = bin_cols > 0 ? bin_cols : 16;
+    if (full_rows) {
+        g.row0 = 0;
+        g.nrows = g.nf1;
+        g.row_wrap = 1;
+    } else {
+        const double s1 = (double)g.nf1 / (2 * M_PI);
+        const double g1lo = xmin * s1, g1hi = xmax * s1;
+        const int r0 = (int)std::floor(g1lo - 0.5 * g.w) - 2;
+        const int r1 = (int)std::ceil(g1hi + 0.5 * g.w) + 2;
+        if (r1 - r0 + 1 >= g.nf1) {
+            g.row0 = 0;
+            g.nrows = g.nf1;
+            g.row_wrap = 1;
+        } else {
+            g.row0 = r0;
+            g.nrows = r1 - r0 + 1;
+            g.row_wrap = 0;
+        }
+    }
+    std::vector<double2> mult1(n1);
+    for (int i = 0; i < n1; ++i) {
+        const double dec = es_deconv(mode_k(i, n1), g.nf1, g.w, g.beta);
+        mult1[i] = make_double2(phase1[i].x * dec, phase1[i].y * dec);
+    }
+    std::vector<double> dec2(g.ncols);
+    std::vector<int> colp2(g.ncols), p2col(g.nf2, -1);
+    for (int c = 0; c < g.ncols; ++c) {
+        const int k2 = colk2[c];
+        dec2[c] = es_deconv(k2, g.nf2, g.w, g.beta);
+        int p2 = k2 % g.nf2;
+        if (p2 < 0) p2 += g.nf2;
+        colp2[c] = p2;
+        p2col[p2] = c;
+    }
+    PF_TRY(upload(d.mult1, mult1, s));
+    PF_TRY(upload(d.dec2, dec2, s));
+    PF_TRY(upload(d.colp2, colp2, s));
+    PF_TRY(upload(d.p2col, p2col, s));
+    return 0;
+}
+
+int validate_common(int64_t npts, int lmax, int ntrans, double tol) {
+    if (npts < 1) return fail(PFSHT_ERR_ARGUMENT, "need at least one point");
+    if (lmax < 0) return fail(PFSHT_ERR_ARGUMENT, "lmax must be nonnegative");
+    if (ntrans < 1) return fail(PFSHT_ERR_ARGUMENT, "ntrans must be >= 1");
+    if (!(tol > 0) || !(tol < 1)) return fail(PFSHT_ERR_ARGUMENT, "tol must lie in (0, 1)");
+    return 0;
+}
+
+void fill_info(pfsht_plan* p) {
+    pfsht_plan_info& in = p->info;
+    in = pfsht_plan_info{};
+    in.kind = p->kind;
+    in.flip = p->leaf.flip ? 1 : 0;
+    in.lmax = p->L;
+    in.ntrans = p->B;
+    in.precision = p->precision;
+    in.npts = p->M;
+    in.tol = p->tol;
+    if (p->kind == kDirect) {
+        in.nrings = (int)p->M;
+        in.mmax = p->L;
+        in.ring_work = 0;
+    } else {
+        const Leaf& lf = p->leaf;
+        in.nth_half = lf.nth_half;
+        in.nth = lf.nth;
+        in.nph = lf.nph;
+        in.mmax = lf.mmax;
+        in.nrings = lf.nth_half;
+        in.K = lf.g.K;
+        in.ring_work = lf.ring_work;
+        in.beta = lf.g.beta;
+        in.h = lf.g.h;
+        in.theta_lo = lf.g.lo;
+        in.theta_hi = lf.g.hi;
+        in.eps_apo = lf.g.eps_apo;
+        in.Theta1 = lf.g.Theta1;
+        in.sigma = lf.g.sigma;
+        in.ThetaT = lf.g.ThetaT;
+        in.nufft_w = p->ng.w;
+        in.nufft_beta = p->ng.beta;
+        in.nf1 = p->ng.nf1;
+        in.nf2 = p->ng.nf2;
+        in.row0 = p->ng.row0;
+        in.nrows = p->ng.nrows;
+        in.ncols = p->ng.ncols;
+    }
+    int64_t bytes = 0;
+    for (const DevBuf* b : {&p->cos_t, &p->log2sin, &p->log2c, &p->w, &p->ab, &p->aboff, &p->items,
+                            &p->H, &p->phi_pts, &p->nd.pts, &p->nd.perm, &p->nd.binstart,
+                            &p->nd.colp2, &p->nd.p2col, &p->nd.mult1, &p->nd.dec2, &p->nd.pad,
+                            &p->nd.U, &p->st_alm, &p->st_f})
+        bytes += (int64_t)b->bytes;
+    in.device_bytes = bytes;
+}
+
+int build_stretch(pfsht_plan* p, const double* d_theta, const double* d_phi, const pfsht_opts& o,
+                  cudaStream_t s) {
+    Leaf& lf = p->leaf;
+    const int L = p->L, B = p->B;
+    p->kind = lf.g.kind;
+    p->nrings = lf.nth_half;
+    PF_TRY(upload(p->cos_t, lf.cos_t, s));
+    PF_TRY(upload(p->log2sin, lf.log2sin, s));
+    PF_TRY(upload(p->log2c, lf.log2c, s));
+    PF_TRY(upload(p->w, lf.w, s));
+    PF_TRY(build_ab_table(L, lf.mmax, p->ab, p->aboff, s));
+    std::vector<RingItem> items = make_ring_items(lf.jlo, lf.jhi, L, lf.mmax, p->R);
+    p->nitems = (int)items.size();
+    PF_TRY(upload(p->items, items, s));
+    p->rt.cos_t = p->cos_t.as<double>();
+    p->rt.log2sin = p->log2sin.as<double>();
+    p->rt.log2c = p->log2c.as<double>();
+    p->rt.w = p->w.as<double>();
+    p->rt.ab = p->ab.as<double2>();
+    p->rt.aboff = p->aboff.as<int64_t>();
+    p->rt.lmax = L;
+    p->rt.nrings = lf.nth_half;
+    p->ncols = 2 * lf.mmax + 1;
+    p->ro_cols.ld = lf.nth;
+    p->ro_cols.bstride = (int64_t)lf.nth * p->ncols;
+    p->ro_cols.col_off = lf.mmax;
+    p->ro_cols.nrows = lf.nth;
+    p->ro_cols.reflect = lf.g.kind == kInterior ? 0 : 1;
+    p->ro_cols.spin_sgn = 1.0;
+    PF_TRY(p->H.alloc(sizeof(double2) * (size_t)lf.nth * p->ncols * B));
+    int n[1] = {lf.nth};
+    PF_CUFFT(cufftPlanMany(&p->fth, 1, n, n, 1, lf.nth, n, 1, lf.nth, CUFFT_Z2Z, p->ncols * B));
+    p->have_fth = true;
+
+    // points: stretched colatitude and longitude on the device (src/Stretch.jl:202-213)
+    DevBuf Th, ph;
+    PF_TRY(Th.alloc(sizeof(double) * p->M));
+    PF_TRY(ph.alloc(sizeof(double) * p->M));
+    PF_TRY(leaf_points(lf.g, lf.flip, d_theta, d_phi, p->M, Th.as<double>(), ph.as<double>(), s));
+    double Tmin = 0, Tmax = 0;
+    PF_TRY(minmax_device(Th.as<double>(), p->M, &Tmin, &Tmax, s));
+
+    // half-cell phase and 1/n_theta per Theta mode (src/Stretch.jl:229-233 with the n_phi of
+    // the phi round trip cancelled)
+    const double shift = lf.g.kind == kInterior ? 0.0 : M_PI / lf.nth;
+    std::vector<double2> phase(lf.nth);
+    for (int i = 0; i < lf.nth; ++i) {
+        const double a = -(double)mode_k(i, lf.nth) * shift;
+        phase[i] = make_double2(std::cos(a) / lf.nth, std::sin(a) / lf.nth);
+    }
+    std::vector<int> colk2(p->ncols);
+    for (int c = 0; c < p->ncols; ++c) colk2[c] = c - lf.mmax;
+    PF_TRY(setup_nufft_grid(p->ng, p->nd, lf.nth, lf.nph, colk2, phase, p->tol, p->M, Tmin, Tmax,
+                            false, o.nufft_bin_rows, o.nufft_bin_cols, s));
+    PF_TRY(nufft_setpts(p->ng, p->nd, Th.as<double>(), ph.as<double>(), s));
+    PF_TRY(nufft_alloc(p->ng, p->nd, B));
+    return 0;
+}
+
+int build_direct(pfsht_plan* p, const double* h_theta, const double* h_phi, cudaStream_t s) {
+    const int L = p->L, B = p->B;
+    const int64_t M = p->M;
+    if (M > INT32_MAX) return fail(PFSHT_ERR_ARGUMENT, "too many points for the direct method");
+    p->kind = kDirect;
+    p->nrings = (int)M;
+    std::vector<double> cs(M), l2s(M), ph(M);
+    for (int64_t i = 0; i < M; ++i) {
+        const double sn = std::sin(h_theta[i]), c = std::cos(h_theta[i]);
+        const double as = std::fabs(sn);
+        cs[i] = c;
+        l2s[i] = as > 0 ? std::log2(as) : -INFINITY;
+        ph[i] = h_phi[i];
+    }
+    std::vector<double> l2c;
+    sectorial_log2c(L, l2c);
+    PF_TRY(upload(p->cos_t, cs, s));
+    PF_TRY(upload(p->log2sin, l2s, s));
+    PF_TRY(upload(p->log2c, l2c, s));
+    PF_TRY(upload(p->phi_pts, ph, s));
+    PF_TRY(build_ab_table(L, L, p->ab, p->aboff, s));
+    // eps = 0: every order on every point (src/Direct.jl:262-263)
+    std::vector<int> jlo(L + 1, 0), jhi(L + 1, (int)M - 1);
+    std::vector<RingItem> items = make_ring_items(jlo, jhi, L, L, p->R);
+    p->nitems = (int)items.size();
+    PF_TRY(upload(p->items, items, s));
+    p->rt.cos_t = p->cos_t.as<double>();
+    p->rt.log2sin = p->log2sin.as<double>();
+    p->rt.log2c = p->log2c.as<double>();
+    p->rt.w = nullptr;
+    p->rt.ab = p->ab.as<double2>();
+    p->rt.aboff = p->aboff.as<int64_t>();
+    p->rt.lmax = L;
+    p->rt.nrings = (int)M;
+    p->ncols = 2 * L + 1;
+    p->ro_cols.ld = M;
+    p->ro_cols.bstride = M * (2 * L + 1);
+    p->ro_cols.col_off = L;
+    p->ro_cols.nrows = (int)M;
+    p->ro_cols.reflect = 0;
+    p->ro_cols.spin_sgn = 1.0;
+    PF_TRY(p->H.alloc(sizeof(double2) * (size_t)M * (2 * L + 1) * B));
+    return 0;
+}
+
+int plan_create(const double* theta, const double* phi, int64_t npts, int lmax, int ntrans,
+                double tol, int precision, const pfsht_opts* opts_in, pfsht_plan** out) {
+    if (!out) return fail(PFSHT_ERR_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    if (!theta || !phi) return fail(PFSHT_ERR_ARGUMENT, "theta and phi must not be NULL");
+    PF_TRY(validate_common(npts, lmax, ntrans, tol));
+    if (precision != PFSHT_PRECISION_FP64 && precision != PFSHT_PRECISION_MIXED)
+        return fail(PFSHT_ERR_ARGUMENT, "unknown precision mode");
+    pfsht_opts o;
+    pfsht_opts_default(&o);
+    if (opts_in) o = *opts_in;
+    if (o.method < 0 || o.method > 2) return fail(PFSHT_ERR_ARGUMENT, "unknown method");
+    if (!(o.oversample_theta >= 1) || !(o.oversample_phi >= 1))
+        return fail(PFSHT_ERR_ARGUMENT, "oversampling factors must be >= 1");
+    if (!(o.eps_apo_max > 0)) return fail(PFSHT_ERR_ARGUMENT, "eps_apo_max must be positive");
+    DeviceGuard dg(o.device);
+    int dev = 0;
+    PF_CUDA(cudaGetDevice(&dev));
+
+    std::unique_ptr<pfsht_plan> p(new pfsht_plan());
+    p->device = dev;
+    p->precision = precision;
+    p->L = lmax;
+    p->B = ntrans;
+    p->M = npts;
+    p->tol = tol;
+    p->R = o.ring_rings_per_lane > 0 ? o.ring_rings_per_lane : 4;
+    PF_CUDA(cudaStreamCreateWithFlags(&p->st_stream, cudaStreamNonBlocking));
+    cudaStream_t s = p->st_stream;
+
+    // host and device copies of the points
+    std::vector<double> h_theta, h_phi;
+    DevBuf d_theta, d_phi;
+    const double* dth;
+    const double* dph;
+    double lo, hi;
+    if (o.points_on_device) {
+        dth = theta;
+        dph = phi;
+        PF_TRY(minmax_device(theta, npts, &lo, &hi, s));
+    } else {
+        PF_TRY(d_theta.alloc(sizeof(double) * npts));
+        PF_TRY(d_phi.alloc(sizeof(double) * npts));
+        PF_CUDA(cudaMemcpyAsync(d_theta.p, theta, sizeof(double) * npts, cudaMemcpyHostToDevice, s));
+        PF_CUDA(cudaMemcpyAsync(d_phi.p, phi, sizeof(double) * npts, cudaMemcpyHostToDevice, s));
+        dth = d_theta.as<double>();
+        dph = d_phi.as<double>();
+        lo = INFINITY;
+        hi = -INFINITY;
+        for (int64_t i = 0; i < npts; ++i) {
+            lo = std::fmin(lo, theta[i]);
+            hi = std::fmax(hi, theta[i]);
+        }
+    }
+    if (!(std::isfinite(lo) && std::isfinite(hi)))
+        return fail(PFSHT_ERR_ARGUMENT, "colatitudes must be finite");
+    // bounding_box colatitude extent (src/Box.jl:51-59)
+    lo = std::fmax(lo, 0.0);
+    hi = std::fmin(hi, M_PI);
+
+    bool direct = o.method == PFSHT_METHOD_DIRECT;
+    if (!direct) {
+        std::string err;
+        int r = build_leaf(lo, hi, lmax, ntrans, tol, o.eps_apo_max, o.oversample_theta,
+                           o.oversample_phi, &p->leaf, &err);
+        if (r == 2) return fail(PFSHT_ERR_ARGUMENT, err);
+        if (r == 1) {
+            if (o.method == PFSHT_METHOD_STRETCH) return fail(PFSHT_ERR_REFUSED, err);
+            direct = true;  // what the reference's AutoAlgorithm answers (src/Cost.jl:121-122,184-186)
+        }
+    }
+    if (direct) {
+        if (o.points_on_device) {
+            h_theta.resize(npts);
+            h_phi.resize(npts);
+            PF_CUDA(cudaMemcpyAsync(h_theta.data(), theta, sizeof(double) * npts, cudaMemcpyDeviceToHost, s));
+            PF_CUDA(cudaMemcpyAsync(h_phi.data(), phi, sizeof(double) * npts, cudaMemcpyDeviceToHost, s));
+            PF_CUDA(cudaStreamSynchronize(s));
+            PF_TRY(build_direct(p.get(), h_theta.data(), h_phi.data(), s));
+        } else {
+            PF_TRY(build_direct(p.get(), theta, phi, s));
+        }
+    } else {
+        PF_TRY(build_stretch(p.get(), dth, dph, o, s));
+    }
+    PF_CUDA(cudaStreamSynchronize(s));
+    fill_info(p.get());
+    *out = p.release();
+    return 0;
+}
+
+int apply_forward(pfsht_plan* p, const double2* alm, double2* f, cudaStream_t s) {
+    const int B = p->B;
+    PF_CUDA(cudaMemsetAsync(p->H.p, 0, p->H.bytes, s));
+    PF_TRY(ring_forward(p->rt, p->ro_cols, p->items.as<RingItem>(), p->nitems, p->R, alm,
+                        p->H.as<double2>(), B, s));
+    if (p->kind == kDirect)
+        return direct_phase_sum(p->H.as<double2>(), p->phi_pts.as<double>(), p->M, p->L, B, f, s);
+    PF_CUFFT(cufftSetStream(p->fth, s));
+    PF_CUFFT(cufftExecZ2Z(p->fth, p->H.as<cufftDoubleComplex>(), p->H.as<cufftDoubleComplex>(),
+                          CUFFT_FORWARD));
+    return nufft_type2(p->ng, p->nd, p->H.as<double2>(), f, B, +1, s);
+}
+
+int apply_adjoint(pfsht_plan* p, const double2* f, double2* alm, cudaStream_t s) {
+    const int B = p->B;
+    const size_t alm_bytes = sizeof(double2) * (size_t)(p->L + 1) * (2 * p->L + 1) * B;
+    if (p->kind == kDirect) {
+        PF_TRY(direct_phase_spread(f, p->phi_pts.as<double>(), p->M, p->L, B, p->H.as<double2>(), s));
+    } else {
+        PF_TRY(nufft_type1(p->ng, p->nd, f, p->H.as<double2>(), B, -1, s));
+        PF_CUFFT(cufftSetStream(p->fth, s));
+        PF_CUFFT(cufftExecZ2Z(p->fth, p->H.as<cufftDoubleComplex>(), p->H.as<cufftDoubleComplex>(),
+                              CUFFT_INVERSE));
+    }
+    PF_CUDA(cudaMemsetAsync(alm, 0, alm_bytes, s));
+    return ring_adjoint(p->rt, p->ro_cols, p->items.as<RingItem>(), p->nitems, p->R,
+                        p->H.as<double2>(), alm, B, s);
+}
+
+}  // namespace
+
+extern "C" {
+
+pfsht_status pfsht_opts_default(pfsht_opts* o) {
+    if (!o) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "opts is NULL");
+    std::memset(o, 0, sizeof(*o));
+    o->method = PFSHT_METHOD_AUTO;
+    o->points_on_device = 0;
+    o->device = -1;
+    o->ring_rings_per_lane = 0;
+    o->nufft_bin_rows = 0;
+    o->nufft_bin_cols = 0;
+    o->oversample_theta = 1.0;
+    o->oversample_phi = 1.0;
+    o->eps_apo_max = 1.0;
+    return PFSHT_OK;
+}
+
+pfsht_status pfsht_plan_create(const double* theta, const double* phi, int64_t npts, int32_t lmax,
+                               int32_t ntrans, double tol, int32_t precision,
+                               const pfsht_opts* opts, pfsht_plan** out) {
+    return (pfsht_status)plan_create(theta, phi, npts, lmax, ntrans, tol, precision, opts, out);
+}
+
+pfsht_status pfsht_plan_destroy(pfsht_plan* p) {
+    if (!p) return PFSHT_OK;
+    DeviceGuard dg(p->device);
+    delete p;
+    return PFSHT_OK;
+}
+
+pfsht_status pfsht_forward(pfsht_plan* p, const void* alm, void* f, void* stream) {
+    if (!p || !alm || !f) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "NULL argument");
+    DeviceGuard dg(p->device);
+    return (pfsht_status)apply_forward(p, (const double2*)alm, (double2*)f, (cudaStream_t)stream);
+}
+
+pfsht_status pfsht_adjoint(pfsht_plan* p, const void* f, void* alm, void* stream) {
+    if (!p || !alm || !f) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "NULL argument");
+    DeviceGuard dg(p->device);
+    return (pfsht_status)apply_adjoint(p, (const double2*)f, (double2*)alm, (cudaStream_t)stream);
+}
+
+static int host_apply(pfsht_plan* p, const void* in, void* out, bool fwd) {
+    DeviceGuard dg(p->device);
+    const size_t na = sizeof(double2) * (size_t)(p->L + 1) * (2 * p->L + 1) * p->B;
+    const size_t nf = sizeof(double2) * (size_t)p->M * p->B;
+    if (!p->st_alm.p) PF_TRY(p->st_alm.alloc(na));
+    if (!p->st_f.p) PF_TRY(p->st_f.alloc(nf));
+    cudaStream_t s = p->st_stream;
+    if (fwd) {
+        PF_CUDA(cudaMemcpyAsync(p->st_alm.p, in, na, cudaMemcpyHostToDevice, s));
+        PF_TRY(apply_forward(p, p->st_alm.as<double2>(), p->st_f.as<double2>(), s));
+        PF_CUDA(cudaMemcpyAsync(out, p->st_f.p, nf, cudaMemcpyDeviceToHost, s));
+    } else {
+        PF_CUDA(cudaMemcpyAsync(p->st_f.p, in, nf, cudaMemcpyHostToDevice, s));
+        PF_TRY(apply_adjoint(p, p->st_f.as<double2>(), p->st_alm.as<double2>(), s));
+        PF_CUDA(cudaMemcpyAsync(out, p->st_alm.p, na, cudaMemcpyDeviceToHost, s));
+    }
+    PF_CUDA(cudaStreamSynchronize(s));
+    return 0;
+}
+
+pfsht_status pfsht_forward_host(pfsht_plan* p, const void* alm, void* f) {
+    if (!p || !alm || !f) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "NULL argument");
+    return (pfsht_status)host_apply(p, alm, f, true);
+}
+
+pfsht_status pfsht_adjoint_host(pfsht_plan* p, const void* f, void* alm) {
+    if (!p || !alm || !f) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "NULL argument");
+    return (pfsht_status)host_apply(p, f, alm, false);
+}
+
+pfsht_status pfsht_ring_forward(pfsht_plan* p, const void* alm, void* G, void* stream) {
+    if (!p || !alm || !G) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "NULL argument");
+    if (p->kind == kDirect) return (pfsht_status)fail(PFSHT_ERR_UNSUPPORTED, "direct plan has no ring set");
+    DeviceGuard dg(p->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    RingTables t = p->rt;
+    t.w = nullptr;
+    RingOut o;
+    o.ld = p->nrings;
+    o.bstride = (int64_t)p->nrings * (2 * p->L + 1);
+    o.col_off = p->L;
+    o.nrows = p->nrings;
+    o.reflect = 0;
+    const size_t bytes = sizeof(double2) * (size_t)o.bstride * p->B;
+    cudaError_t e = cudaMemsetAsync(G, 0, bytes, s);
+    if (e != cudaSuccess) return (pfsht_status)fail(PFSHT_ERR_CUDA, cudaGetErrorString(e));
+    return (pfsht_status)ring_forward(t, o, p->items.as<RingItem>(), p->nitems, p->R,
+                                      (const double2*)alm, (double2*)G, p->B, s);
+}
+
+pfsht_status pfsht_ring_adjoint(pfsht_plan* p, const void* G, void* alm, void* stream) {
+    if (!p || !alm || !G) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "NULL argument");
+    if (p->kind == kDirect) return (pfsht_status)fail(PFSHT_ERR_UNSUPPORTED, "direct plan has no ring set");
+    DeviceGuard dg(p->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    RingTables t = p->rt;
+    t.w = nullptr;
+    RingOut o;
+    o.ld = p->nrings;
+    o.bstride = (int64_t)p->nrings * (2 * p->L + 1);
+    o.col_off = p->L;
+    o.nrows = p->nrings;
+    o.reflect = 0;
+    const size_t bytes = sizeof(double2) * (size_t)(p->L + 1) * (2 * p->L + 1) * p->B;
+    cudaError_t e = cudaMemsetAsync(alm, 0, bytes, s);
+    if (e != cudaSuccess) return (pfsht_status)fail(PFSHT_ERR_CUDA, cudaGetErrorString(e));
+    return (pfsht_status)ring_adjoint(t, o, p->items.as<RingItem>(), p->nitems, p->R,
+                                      (const double2*)G, (double2*)alm, p->B, s);
+}
+
+int64_t pfsht_ring_work(const pfsht_plan* p) { return p ? p->info.ring_work : -1; }
+
+pfsht_status pfsht_plan_get_info(const pfsht_plan* p, pfsht_plan_info* info) {
+    if (!p || !info) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "NULL argument");
+    *info = p->info;
+    return PFSHT_OK;
+}
+
+int64_t pfsht_workspace_bytes(const pfsht_plan* p) { return p ? p->info.device_bytes : -1; }
+
+pfsht_status pfsht_plan_geometry(const double* theta, const double* phi, int64_t npts, int32_t lmax,
+                                 int32_t ntrans, double tol, const pfsht_opts* opts_in,
+                                 pfsht_plan_info* info) {
+    if (!theta || !phi || !info) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "NULL argument");
+    int v = validate_common(npts, lmax, ntrans, tol);
+    if (v) return (pfsht_status)v;
+    pfsht_opts o;
+    pfsht_opts_default(&o);
+    if (opts_in) o = *opts_in;
+    double lo = INFINITY, hi = -INFINITY;
+    for (int64_t i = 0; i < npts; ++i) {
+        lo = std::fmin(lo, theta[i]);
+        hi = std::fmax(hi, theta[i]);
+    }
+    lo = std::fmax(lo, 0.0);
+    hi = std::fmin(hi, M_PI);
+    *info = pfsht_plan_info{};
+    info->lmax = lmax;
+    info->ntrans = ntrans;
+    info->npts = npts;
+    info->tol = tol;
+    if (o.method == PFSHT_METHOD_DIRECT) {
+        info->kind = kDirect;
+        info->mmax = lmax;
+        info->nrings = (int)npts;
+        return PFSHT_OK;
+    }
+    Leaf lf;
+    std::string err;
+    int r = build_leaf(lo, hi, lmax, ntrans, tol, o.eps_apo_max, o.oversample_theta,
+                       o.oversample_phi, &lf, &err);
+    if (r == 2) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, err);
+    if (r == 1) {
+        if (o.method == PFSHT_METHOD_STRETCH) return (pfsht_status)fail(PFSHT_ERR_REFUSED, err);
+        info->kind = kDirect;
+        info->mmax = lmax;
+        info->nrings = (int)npts;
+        return PFSHT_OK;
+    }
+    info->kind = lf.g.kind;
+    info->flip = lf.flip;
+    info->nth_half = lf.nth_half;
+    info->nth = lf.nth;
+    info->nph = lf.nph;
+    info->mmax = lf.mmax;
+    info->nrings = lf.nth_half;
+    info->K = lf.g.K;
+    info->ring_work = lf.ring_work;
+    info->beta = lf.g.beta;
+    info->h = lf.g.h;
+    info->theta_lo = lf.g.lo;
+    info->theta_hi = lf.g.hi;
+    info->eps_apo = lf.g.eps_apo;
+    info->Theta1 = lf.g.Theta1;
+    info->sigma = lf.g.sigma;
+    info->ThetaT = lf.g.ThetaT;
+    info->nufft_w = es_width(tol);
+    info->nufft_beta = 2.30 * info->nufft_w;
+    info->nf1 = (int)next_smooth(std::max<int64_t>(2 * (int64_t)lf.nth, 2 * info->nufft_w));
+    info->nf2 = (int)next_smooth(std::max<int64_t>(2 * (int64_t)lf.nph, 2 * info->nufft_w));
+    info->ncols = 2 * lf.mmax + 1;
+    return PFSHT_OK;
+}
+
+pfsht_status pfsht_dfs_double(const void* F, void* Ft, int32_t Nth, int32_t Nph, int32_t B,
+                              int32_t spin, void* stream) {
+    if (!F || !Ft || Nth < 1 || Nph < 1 || B < 1)
+        return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "bad DFS arguments");
+    return (pfsht_status)dfs_double((const double2*)F, (double2*)Ft, Nth, Nph, B, spin, (cudaStream_t)stream);
+}
+
+pfsht_status pfsht_dfs_fold(void* F, const void* Ft, int32_t Nth, int32_t Nph, int32_t B,
+                            int32_t spin, void* stream) {
+    if (!F || !Ft || Nth < 1 || Nph < 1 || B < 1)
+        return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "bad DFS arguments");
+    return (pfsht_status)dfs_fold((double2*)F, (const double2*)Ft, Nth, Nph, B, spin, (cudaStream_t)stream);
+}
+
+pfsht_status pfsht_nufft_create(int32_t type, int32_t n1, int32_t n2, int32_t iflag, int32_t ntrans,
+                                double tol, const double* x, const double* y, int64_t M,
+                                pfsht_nufft** out) {
+    if (!out) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    if (type != 1 && type != 2)
+        return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "NUFFT type must be 1 or 2");
+    if (n1 < 1 || n2 < 1 || ntrans < 1 || M < 1 || !x || !y)
+        return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "bad NUFFT arguments");
+    if (!(tol > 0) || !(tol < 1)) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "tol must lie in (0, 1)");
+    std::unique_ptr<pfsht_nufft> p(new pfsht_nufft());
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return (pfsht_status)fail(PFSHT_ERR_CUDA, cudaGetErrorString(e));
+    p->device = dev;
+    p->type = type;
+    p->iflag = iflag >= 0 ? 1 : -1;
+    p->B = ntrans;
+    p->n1 = n1;
+    p->n2 = n2;
+    p->M = M;
+    DevBuf dx, dy;
+    int r = dx.alloc(sizeof(double) * M);
+    if (!r) r = dy.alloc(sizeof(double) * M);
+    if (r) return (pfsht_status)r;
+    if (cudaMemcpy(dx.p, x, sizeof(double) * M, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(dy.p, y, sizeof(double) * M, cudaMemcpyHostToDevice) != cudaSuccess)
+        return (pfsht_status)fail(PFSHT_ERR_CUDA, "copying NUFFT points");
+    std::vector<int> colk2(n2);
+    for (int c = 0; c < n2; ++c) colk2[c] = mode_k(c, n2);
+    std::vector<double2> ones(n1, make_double2(1.0, 0.0));
+    r = setup_nufft_grid(p->g, p->d, n1, n2, colk2, ones, tol, M, 0.0, 0.0, true, 0, 0, nullptr);
+    if (!r) r = nufft_setpts(p->g, p->d, dx.as<double>(), dy.as<double>(), nullptr);
+    if (!r) r = nufft_alloc(p->g, p->d, ntrans);
+    if (r) return (pfsht_status)r;
+    *out = p.release();
+    return PFSHT_OK;
+}
+
+pfsht_status pfsht_nufft_exec(pfsht_nufft* p, const void* in, void* out, void* stream) {
+    if (!p || !in || !out) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "NULL argument");
+    DeviceGuard dg(p->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (p->type == 2)
+        return (pfsht_status)nufft_type2(p->g, p->d, (const double2*)in, (double2*)out, p->B, p->iflag, s);
+    return (pfsht_status)nufft_type1(p->g, p->d, (const double2*)in, (double2*)out, p->B, p->iflag, s);
+}
+
+pfsht_status pfsht_nufft_destroy(pfsht_nufft* p) {
+    if (!p) return PFSHT_OK;
+    DeviceGuard dg(p->device);
+    delete p;
+    return PFSHT_OK;
+}
+
+size_t pfsht_last_error(char* buf, size_t len) {
+    const std::string& e = get_error();
+    if (buf && len > 0) {
+        size_t n = std::min(len - 1, e.size());
+        std::memcpy(buf, e.data(), n);
+        buf[n] = 0;
+    }
+    return e.size();
+}
+
+const char* pfsht_version(void) { return "pfsht_b200 0.1.0 (sm_100a)"; }
+
+}  // extern "C"
