@@ -131,6 +131,15 @@ pfsht_status pfsht_nufft_create(int32_t type, int32_t n1, int32_t n2, int32_t if
 pfsht_status pfsht_nufft_exec(pfsht_nufft* p, const void* in, void* out, void* stream);
 pfsht_status pfsht_nufft_destroy(pfsht_nufft* p);
 
+/* FMA-throughput microbenchmark on the current device (no reference counterpart): runs a
+ * grid of independent FP64 (fp64 = 1) or FP32 FMA chains and reports FLOP/s (2 per FMA).
+ * These are the denominators of the ring-pass and NUFFT FLOP rooflines. */
+pfsht_status pfsht_fma_peak(int32_t fp64, int32_t iters, double* flops_per_s, double* ms);
+
+/* Number of this library's own kernel launches since load (diagnostics; cuFFT and CUB
+ * kernels are not counted). */
+int64_t pfsht_launch_count(void);
+
 /* Thread-local message of the last failing call; returns its length. */
 size_t pfsht_last_error(char* buf, size_t len);
 /* Library version string. */

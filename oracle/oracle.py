@@ -93,6 +93,8 @@ def lib():
         "orc_nufft_direct": (None, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp,
                                     C.c_int64, vp, vp]),
         "orc_esnufft_create": (vp, [C.c_int, C.c_int, C.c_int, C.c_double, _dp, _dp, C.c_int64]),
+        "orc_esnufft_create_k": (vp, [C.c_int, C.c_int, C.c_int, C.c_double, _dp, _dp, C.c_int64,
+                                      C.c_int]),
         "orc_esnufft_destroy": (None, [vp]),
         "orc_esnufft_params": (None, [vp, C.POINTER(C.c_int), C.POINTER(C.c_double),
                                       C.POINTER(C.c_int), C.POINTER(C.c_int)]),
@@ -435,12 +437,12 @@ def nufft_direct(typ, n1, n2, iflag, x, y, inp):
 class ESNufft:
     """CPU ES-kernel NUFFT (published FINUFFT algorithm)."""
 
-    def __init__(self, n1, n2, x, y, tol, ntrans=1):
+    def __init__(self, n1, n2, x, y, tol, ntrans=1, kernel="poly"):
         self.x = _f64(x)
         self.y = _f64(y)
         self.n1, self.n2, self.B = int(n1), int(n2), int(ntrans)
-        self._h = lib().orc_esnufft_create(self.n1, self.n2, self.B, float(tol), self.x,
-                                           self.y, len(self.x))
+        self._h = lib().orc_esnufft_create_k(self.n1, self.n2, self.B, float(tol), self.x,
+                                             self.y, len(self.x), 1 if kernel == "poly" else 0)
 
     def __del__(self):
         if getattr(self, "_h", None):
@@ -506,7 +508,9 @@ class RefusedGeometry(ValueError):
 
 
 class Stretch:
-    """StretchLeaf (src/Stretch.jl:94-295) with DirectSum (exact) or ES NUFFT."""
+    """StretchLeaf (src/Stretch.jl:94-295) with DirectSum (exact, nufft="direct"), the ES
+    NUFFT with FINUFFT's polynomial kernel evaluation (nufft="es") or with the exact kernel
+    (nufft="es_exact")."""
 
     def __init__(self, theta, phi, lmax, tol, ntrans=1, nufft="es", eps_apo_max=1.0,
                  oversample_theta=1.0, oversample_phi=1.0):
@@ -514,7 +518,7 @@ class Stretch:
         self.phi = _f64(phi)
         self.M = len(self.theta)
         st = C.c_int(0)
-        kind = 1 if nufft == "es" else 0
+        kind = {"direct": 0, "es": 1, "es_exact": 2}[nufft]
         self._h = lib().orc_stretch_create(self.theta, self.phi, self.M, int(lmax), int(ntrans),
                                            float(tol), kind, float(eps_apo_max),
                                            float(oversample_theta), float(oversample_phi),

@@ -918,7 +918,39 @@ struct orc_esnufft {
     int64_t M;
     double *x, *y;
     cplx* grid;
+    int kermode;  /* ORC_KER_EXACT or ORC_KER_POLY */
+    double* cheb; /* w x (w + 3) Chebyshev coefficients per tap */
 };
+
+/* Per-tap Chebyshev interpolant of the ES kernel (FINUFFT's default piecewise-polynomial
+ * kernel evaluation): tap a as a function of s = i0 - g + w/2 in [0, 1), interpolated at
+ * the w + 3 Chebyshev points of the first kind (degree w + 2). */
+static void es_cheb_fit(int w, double beta, double* cheb) {
+    const int n = w + 3;
+    double ys[32];
+    for (int a = 0; a < w; ++a) {
+        for (int i = 0; i < n; ++i) {
+            double t = cos(M_PI * (i + 0.5) / n);
+            double z = ((t + 1.0) / 2.0 + a - 0.5 * w) / (0.5 * w);
+            ys[i] = orc_es_kernel(z, beta);
+        }
+        for (int k = 0; k < n; ++k) {
+            double acc = 0.0;
+            for (int i = 0; i < n; ++i) acc += ys[i] * cos(k * M_PI * (i + 0.5) / n);
+            cheb[a * n + k] = (k == 0 ? 1.0 : 2.0) * acc / n;
+        }
+    }
+}
+
+static double es_cheb_eval(const double* c, int n, double t) {
+    double b1 = 0.0, b2 = 0.0;
+    for (int k = n - 1; k >= 1; --k) {
+        double b0 = c[k] + 2.0 * t * b1 - b2;
+        b2 = b1;
+        b1 = b0;
+    }
+    return c[0] + t * b1 - b2;
+}
 
 double orc_es_kernel(double z, double beta) {
     if (fabs(z) >= 1.0) return 0.0;
@@ -955,7 +987,13 @@ static int es_width(double tol) {
 
 orc_esnufft* orc_esnufft_create(int n1, int n2, int ntrans, double tol, const double* x,
                                 const double* y, int64_t M) {
+    return orc_esnufft_create_k(n1, n2, ntrans, tol, x, y, M, ORC_KER_POLY);
+}
+
+orc_esnufft* orc_esnufft_create_k(int n1, int n2, int ntrans, double tol, const double* x,
+                                  const double* y, int64_t M, int kermode) {
     orc_esnufft* p = (orc_esnufft*)calloc(1, sizeof(orc_esnufft));
+    p->kermode = kermode;
     p->n1 = n1;
     p->n2 = n2;
     p->B = ntrans;
@@ -976,12 +1014,14 @@ orc_esnufft* orc_esnufft_create(int n1, int n2, int ntrans, double tol, const do
     memcpy(p->x, x, sizeof(double) * M);
     memcpy(p->y, y, sizeof(double) * M);
     p->grid = (cplx*)malloc(sizeof(cplx) * (size_t)p->nf1 * p->nf2);
+    p->cheb = (double*)malloc(sizeof(double) * p->w * (p->w + 3));
+    es_cheb_fit(p->w, p->beta, p->cheb);
     return p;
 }
 
 void orc_esnufft_destroy(orc_esnufft* p) {
     if (!p) return;
-    free(p->dec1); free(p->dec2); free(p->x); free(p->y); free(p->grid);
+    free(p->dec1); free(p->dec2); free(p->x); free(p->y); free(p->grid); free(p->cheb);
     free(p);
 }
 
@@ -998,10 +1038,16 @@ static inline int wrapi(int64_t i, int n) {
 }
 
 /* kernel taps of one coordinate: first cell index and w weights */
-static inline int64_t es_taps(double xg, int w, double beta, double* ker) {
+static inline int64_t es_taps_p(const orc_esnufft* p, double xg, double* ker) {
+    const int w = p->w;
     double hw = 0.5 * w;
     int64_t i0 = (int64_t)ceil(xg - hw);
-    for (int a = 0; a < w; ++a) ker[a] = orc_es_kernel(((double)(i0 + a) - xg) / hw, beta);
+    if (p->kermode == ORC_KER_POLY) {
+        double v = ((double)i0 - xg) + (hw - 0.5);
+        for (int a = 0; a < w; ++a) ker[a] = es_cheb_eval(p->cheb + a * (w + 3), w + 3, 2.0 * v);
+    } else {
+        for (int a = 0; a < w; ++a) ker[a] = orc_es_kernel(((double)(i0 + a) - xg) / hw, p->beta);
+    }
     return i0;
 }
 
@@ -1033,8 +1079,8 @@ void orc_esnufft_exec(orc_esnufft* p, int type, int iflag, const double* in, dou
 #endif
             for (int64_t j = 0; j < M; ++j) {
                 double k1w[16], k2w[16];
-                int64_t i10 = es_taps(p->x[j] * s1, w, p->beta, k1w);
-                int64_t i20 = es_taps(p->y[j] * s2, w, p->beta, k2w);
+                int64_t i10 = es_taps_p(p, p->x[j] * s1, k1w);
+                int64_t i20 = es_taps_p(p, p->y[j] * s2, k2w);
                 cplx acc = {0, 0};
                 for (int bb = 0; bb < w; ++bb) {
                     int c2 = wrapi(i20 + bb, nf2);
@@ -1069,8 +1115,8 @@ void orc_esnufft_exec(orc_esnufft* p, int type, int iflag, const double* in, dou
                     }
                     if (!hit) continue;
                     double k1w[16], k2w[16];
-                    int64_t i10 = es_taps(p->x[j] * s1, w, p->beta, k1w);
-                    es_taps(g2, w, p->beta, k2w);
+                    int64_t i10 = es_taps_p(p, p->x[j] * s1, k1w);
+                    es_taps_p(p, g2, k2w);
                     for (int bb = 0; bb < w; ++bb) {
                         int c2 = wrapi(i20 + bb, nf2);
                         if (c2 < c0 || c2 >= c1) continue;
@@ -1305,7 +1351,9 @@ orc_stretch* orc_stretch_create(const double* theta, const double* phi, int64_t 
         s->phase[i].im = c.im / N;
     }
     s->nufft_kind = nufft_kind;
-    if (nufft_kind == ORC_NUFFT_ES) s->es = orc_esnufft_create(nth, nph, ntrans, tol, s->Thp, s->php, M);
+    if (nufft_kind == ORC_NUFFT_ES || nufft_kind == ORC_NUFFT_ES_EXACT)
+        s->es = orc_esnufft_create_k(nth, nph, ntrans, tol, s->Thp, s->php, M,
+                                     nufft_kind == ORC_NUFFT_ES ? ORC_KER_POLY : ORC_KER_EXACT);
     size_t B = ntrans;
     s->G = (cplx*)calloc((size_t)nth_half * (2 * lmax + 1) * B, sizeof(cplx));
     s->Fphi = (cplx*)calloc((size_t)nth_half * nph * B, sizeof(cplx));
@@ -1407,7 +1455,7 @@ void orc_stretch_forward(orc_stretch* s, const double* alm, double* f, int nthre
                 *v = c_mul(*v, s->phase[i]);
             }
     /* type-2 NUFFT, iflag +1 */
-    if (s->nufft_kind == ORC_NUFFT_ES) orc_esnufft_exec(s->es, 2, +1, (double*)s->Fhat, f, nthreads);
+    if (s->es) orc_esnufft_exec(s->es, 2, +1, (double*)s->Fhat, f, nthreads);
     else orc_nufft_direct(2, nth, nph, +1, B, s->Thp, s->php, M, (double*)s->Fhat, f);
 }
 
@@ -1416,7 +1464,7 @@ void orc_stretch_adjoint(orc_stretch* s, const double* f, double* alm, int nthre
     const int L = in->lmax, B = in->ntrans, nh = in->nth_half, nth = in->nth, nph = in->nph;
     const int64_t M = in->M;
     /* type-1 NUFFT, iflag -1 */
-    if (s->nufft_kind == ORC_NUFFT_ES) orc_esnufft_exec(s->es, 1, -1, f, (double*)s->Fhat, nthreads);
+    if (s->es) orc_esnufft_exec(s->es, 1, -1, f, (double*)s->Fhat, nthreads);
     else orc_nufft_direct(1, nth, nph, -1, B, s->Thp, s->php, M, f, (double*)s->Fhat);
     for (int b = 0; b < B; ++b)
         for (int j = 0; j < nph; ++j)

@@ -85,10 +85,14 @@ int orc_mode_k(int i0 /* 0-based */, int n, int modeord);
 void orc_nufft_direct(int type, int n1, int n2, int iflag, int ntrans, const double* x,
                       const double* y, int64_t M, const double* in, double* out);
 /* ES-kernel NUFFT (the published FINUFFT algorithm: exponential-of-semicircle kernel,
- * width w = ceil(log10(10/tol)), beta = 2.30 w, upsampling 2) */
+ * width w = ceil(log10(10/tol)), beta = 2.30 w, upsampling 2; the kernel evaluated exactly
+ * or, as FINUFFT does by default, by a per-tap polynomial of degree w + 2) */
 typedef struct orc_esnufft orc_esnufft;
+enum { ORC_KER_EXACT = 0, ORC_KER_POLY = 1 };
 orc_esnufft* orc_esnufft_create(int n1, int n2, int ntrans, double tol, const double* x,
-                                const double* y, int64_t M);
+                                const double* y, int64_t M);  /* polynomial kernel */
+orc_esnufft* orc_esnufft_create_k(int n1, int n2, int ntrans, double tol, const double* x,
+                                  const double* y, int64_t M, int kermode);
 void orc_esnufft_destroy(orc_esnufft*);
 void orc_esnufft_params(const orc_esnufft*, int* w, double* beta, int* nf1, int* nf2);
 void orc_esnufft_exec(orc_esnufft*, int type, int iflag, const double* in, double* out,
@@ -106,7 +110,7 @@ void orc_direct_forward(orc_direct*, const double* alm, double* f, int nthreads)
 void orc_direct_adjoint(orc_direct*, const double* f, double* alm, int nthreads);
 
 /* ---- stretched leaf (src/Stretch.jl) ---- */
-enum { ORC_NUFFT_DIRECT = 0, ORC_NUFFT_ES = 1 };
+enum { ORC_NUFFT_DIRECT = 0, ORC_NUFFT_ES = 1, ORC_NUFFT_ES_EXACT = 2 };
 typedef struct orc_stretch orc_stretch;
 typedef struct {
     int kind, flip, lmax, ntrans, nth_half, nth, nph, mmax, nrings;

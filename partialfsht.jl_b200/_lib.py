@@ -65,6 +65,8 @@ SIGNATURES = {
     "pfsht_nufft_destroy": (C.c_int, [_vp]),
     "pfsht_last_error": (C.c_size_t, [C.c_char_p, C.c_size_t]),
     "pfsht_version": (C.c_char_p, []),
+    "pfsht_fma_peak": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "pfsht_launch_count": (C.c_int64, []),
 }
 
 _lib = None

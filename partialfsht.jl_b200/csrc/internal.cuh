@@ -58,9 +58,10 @@ struct DevBuf {
 // ---------------------------------------------------------------------------------------
 // ring pass (ring.cu)
 // ---------------------------------------------------------------------------------------
-// One work item: order m, rings [j0, j0 + n) with n <= 32 * R.
+// One work item: order m, rings [j0, j0 + n).
+enum { kItemFirst = 1, kItemSole = 2 };  // first tile of its order / only tile of its order
 struct RingItem {
-    int m, j0, n, pad;
+    int m, j0, n, flags;
 };
 
 struct RingTables {
@@ -83,17 +84,36 @@ struct RingOut {
     int nrows = 0;
     int reflect = 0;
     double spin_sgn = 1.0;
+    int nrings_out = 0;   // rings of the ring set (rows 0..nrings_out-1 belong to rings)
+    int zero_rest = 0;    // forward writes zeros for the rings an order does not retain
+};
+
+// device view of one item list
+struct RingItems {
+    const RingItem* items = nullptr;
+    int nitems = 0;
+    int rmax = 4;                          // tile = 32 * rmax rings
+    const unsigned char* sole_m = nullptr; // lmax + 1: order covered by a single tile
+    const int* jlo = nullptr;              // lmax + 1 retained ring range
+    const int* jhi = nullptr;
+};
+
+struct RingItemsOwner {
+    DevBuf items, sole, jlo, jhi;
+    RingItems view;
 };
 
 int build_ab_table(int lmax, int mmax, DevBuf& ab, DevBuf& aboff, cudaStream_t s);
-// items over the retained (m, ring) set, tiles of up to 32*R rings, heaviest first
+// items over the retained (m, ring) set, tiles of `tile` rings, heaviest first
 std::vector<RingItem> make_ring_items(const std::vector<int>& jlo, const std::vector<int>& jhi,
-                                      int lmax, int mmax, int R);
-// launchers: B transforms, alm complex (lmax+1, 2lmax+1, B)
-int ring_forward(const RingTables& t, const RingOut& o, const RingItem* d_items, int nitems,
-                 int R, const double2* alm, double2* out, int B, cudaStream_t s);
-int ring_adjoint(const RingTables& t, const RingOut& o, const RingItem* d_items, int nitems,
-                 int R, const double2* in, double2* alm, int B, cudaStream_t s);
+                                      int lmax, int mmax, int tile);
+int build_ring_items(const std::vector<int>& jlo, const std::vector<int>& jhi, int lmax, int mmax,
+                     int rmax, RingItemsOwner& own, cudaStream_t s);
+// launchers: B transforms, alm complex (lmax+1, 2lmax+1, B); the adjoint writes all of alm
+int ring_forward(const RingTables& t, const RingOut& o, const RingItems& it, const double2* alm,
+                 double2* out, int B, cudaStream_t s);
+int ring_adjoint(const RingTables& t, const RingOut& o, const RingItems& it, const double2* in,
+                 double2* alm, int B, cudaStream_t s);
 
 // ---------------------------------------------------------------------------------------
 // NUFFT stages (nufft.cu)
@@ -152,7 +172,8 @@ int direct_phase_spread(const double2* f, const double* phi, int64_t M, int lmax
 int dfs_double(const double2* F, double2* Ft, int Nth, int Nph, int B, int spin, cudaStream_t s);
 int dfs_fold(double2* F, const double2* Ft, int Nth, int Nph, int B, int spin, cudaStream_t s);
 
-// launch-error check after a kernel
+// launch-error check after a kernel (also counts the launch)
 int check_launch(const char* what);
+long long launch_count();
 
 }  // namespace pf

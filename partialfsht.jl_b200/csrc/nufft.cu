@@ -18,8 +18,10 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 
+#include "es_horner_table.h"
 #include "internal.cuh"
 
 namespace pf {
@@ -51,7 +53,12 @@ NufftDev::~NufftDev() {
     if (have_f2) cufftDestroy(f2);
 }
 
+static std::atomic<long long> g_launches{0};
+long long launch_count() { return g_launches.load(); }
+
+// every launch of this library's kernels is followed by this check, which also counts it
 int check_launch(const char* what) {
+    g_launches.fetch_add(1, std::memory_order_relaxed);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         set_error(std::string(what) + ": " + cudaGetErrorString(e));
@@ -150,8 +157,11 @@ __global__ void bin_keys_kernel(const double* __restrict__ x, const double* __re
         br = min(max(br, 0), nbr - 1);
         bc = min(max(bc, 0), nbc - 1);
         const int k = br * nbc + bc;
+        // cell of the point inside its bin, so that a bin's points are in row-major cell order
+        const int cr = min(max((int)floor(g1) - br * bin_rows, 0), bin_rows - 1);
+        const int cc = min(max((int)floor(g2) - bc * bin_cols, 0), bin_cols - 1);
         g[i] = make_double2(g1, g2);
-        key[i] = k;
+        key[i] = (k * bin_rows + cr) * bin_cols + cc;
         idx[i] = (int)i;
         atomicAdd(counts + k, 1);
     }
@@ -193,8 +203,13 @@ int nufft_setpts(NufftGrid& g, NufftDev& d, const double* x, const double* y, cu
                                                  gg.as<double2>(), key.as<int>(), idx.as<int>(),
                                                  counts.as<int>());
     PF_TRY(check_launch("bin_keys_kernel"));
+    const int64_t nkeys = (int64_t)nbins * g.bin_rows * g.bin_cols;
+    if (nkeys > INT32_MAX) {
+        set_error("NUFFT fine grid too large for 32-bit bin keys");
+        return 1;
+    }
     int end_bit = 1;
-    while ((1 << end_bit) < nbins + 1 && end_bit < 31) ++end_bit;
+    while ((1ll << end_bit) < nkeys && end_bit < 31) ++end_bit;
     size_t tb = 0, tb2 = 0;
     PF_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, key.as<int>(), key2.as<int>(),
                                             idx.as<int>(), idx2.as<int>(), (int)M, 0, end_bit, s));
@@ -336,16 +351,21 @@ __global__ void rows_adj_kernel(const double2* __restrict__ U, int nf1, int ncol
 // ---------------------------------------------------------------------------------------
 // interpolation and spreading
 // ---------------------------------------------------------------------------------------
-__device__ __forceinline__ double es_ker(double z, double beta) {
-    return fabs(z) >= 1.0 ? 0.0 : exp(beta * (sqrt(1.0 - z * z) - 1.0));
-}
-
+// ES kernel taps of one coordinate: first cell index and w weights, from the per-tap Horner
+// polynomials in v = s - 1/2, s = i0 - g + w/2 (es_horner_table.h)
 template <int W>
-__device__ __forceinline__ int taps(double g, double beta, double* k) {
-    constexpr double hw = 0.5 * W;
-    const int i0 = (int)ceil(g - hw);
+__device__ __forceinline__ int es_taps(double g, double* k) {
+    constexpr int NC = EsHorner<W>::NC;
+    const double* c = EsHorner<W>::coef();
+    const int i0 = (int)ceil(g - 0.5 * W);
+    const double v = ((double)i0 - g) + (0.5 * W - 0.5);
 #pragma unroll
-    for (int a = 0; a < W; ++a) k[a] = es_ker(((double)(i0 + a) - g) / hw, beta);
+    for (int a = 0; a < W; ++a) {
+        double p = c[a * NC + NC - 1];
+#pragma unroll
+        for (int q = NC - 2; q >= 0; --q) p = fma(p, v, c[a * NC + q]);
+        k[a] = p;
+    }
     return i0;
 }
 
@@ -354,116 +374,160 @@ __device__ __forceinline__ int wrap(int i, int n) {
     return r < 0 ? r + n : r;
 }
 
+// bin geometry: rows [br*BR - hc, +TR) x cols [bc*BC - hc, +TC) of the kept fine grid
+struct TileGeom {
+    int tr0, tc0, TR, TC;
+};
 template <int W>
-__global__ void __launch_bounds__(256)
-interp_kernel(const double2* __restrict__ pts, const int* __restrict__ perm, int64_t M,
-              const double2* __restrict__ U, int nrows, int nf2, int row_wrap, double beta,
-              int B, double2* __restrict__ f) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < M;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        const double2 g = pts[i];
-        double k1[W], k2[W];
-        const int i10 = taps<W>(g.x, beta, k1);
-        const int i20 = taps<W>(g.y, beta, k2);
-        int col[W];
-#pragma unroll
-        for (int c = 0; c < W; ++c) col[c] = wrap(i20 + c, nf2);
-        const int j = perm[i];
-        for (int b = 0; b < B; ++b) {
-            const double2* ub = U + (int64_t)nrows * nf2 * b;
-            double2 acc = make_double2(0.0, 0.0);
-#pragma unroll
-            for (int a = 0; a < W; ++a) {
-                int r = i10 + a;
-                if (row_wrap) r = wrap(r, nrows);
-                if (r < 0 || r >= nrows) continue;
-                const double2* row = ub + (int64_t)r * nf2;
-                double2 s = make_double2(0.0, 0.0);
-#pragma unroll
-                for (int c = 0; c < W; ++c) {
-                    const double2 u = row[col[c]];
-                    s.x = fma(u.x, k2[c], s.x);
-                    s.y = fma(u.y, k2[c], s.y);
-                }
-                acc.x = fma(s.x, k1[a], acc.x);
-                acc.y = fma(s.y, k1[a], acc.y);
-            }
-            f[j + M * b] = acc;
-        }
-    }
+__device__ __forceinline__ TileGeom tile_geom(int bin, int nbc, int BR, int BC) {
+    constexpr int hc = (W + 1) / 2;
+    const int br = bin / nbc, bc = bin % nbc;
+    return TileGeom{br * BR - hc, bc * BC - hc, BR + W + 1, BC + W + 1};
 }
 
-// one CTA per bin: spread the bin's points into a shared tile, then add the tile to U
+// Type-2 interpolation: one CTA per bin copies the bin's tile of U into shared memory, then
+// each thread interpolates points of the bin from it.
 template <int W>
-__global__ void __launch_bounds__(256)
-spread_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
-              const int* __restrict__ binstart, int nbc, int bin_rows, int bin_cols, int64_t M,
-              const double2* __restrict__ fin, int b, int nrows, int nf2, int row_wrap,
-              double beta, double2* __restrict__ U) {
+__global__ void __launch_bounds__(128)
+interp_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
+              const int* __restrict__ binstart, int nbc, int BR, int BC, int64_t M,
+              const double2* __restrict__ U, int nrows, int nf2, int row_wrap, int B,
+              double2* __restrict__ f) {
     extern __shared__ double2 tile[];
     const int bin = blockIdx.x;
     const int s = binstart[bin], e = binstart[bin + 1];
     if (s == e) return;
-    const int br = bin / nbc, bc = bin % nbc;
-    constexpr int hc = (W + 1) / 2;
-    const int TR = bin_rows + W + 1, TC = bin_cols + W + 1;
-    const int tr0 = br * bin_rows - hc, tc0 = bc * bin_cols - hc;
-    for (int t = threadIdx.x; t < TR * TC; t += blockDim.x) tile[t] = make_double2(0.0, 0.0);
-    __syncthreads();
-    for (int p = s + threadIdx.x; p < e; p += blockDim.x) {
+    const TileGeom tg = tile_geom<W>(bin, nbc, BR, BC);
+    for (int b = 0; b < B; ++b) {
+        const double2* ub = U + (int64_t)nrows * nf2 * b;
+        for (int t = threadIdx.x; t < tg.TR * tg.TC; t += blockDim.x) {
+            int r = tg.tr0 + t / tg.TC;
+            if (row_wrap) r = wrap(r, nrows);
+            double2 v = make_double2(0.0, 0.0);
+            if (r >= 0 && r < nrows) v = ub[(int64_t)r * nf2 + wrap(tg.tc0 + t % tg.TC, nf2)];
+            tile[t] = v;
+        }
+        __syncthreads();
+        for (int p = s + threadIdx.x; p < e; p += blockDim.x) {
+            const double2 g = pts[p];
+            double k1[W], k2[W];
+            const int i10 = es_taps<W>(g.x, k1) - tg.tr0;
+            const int i20 = es_taps<W>(g.y, k2) - tg.tc0;
+            double2 acc = make_double2(0.0, 0.0);
+            if (i10 >= 0 && i10 + W <= tg.TR && i20 >= 0 && i20 + W <= tg.TC) {
+#pragma unroll
+                for (int a = 0; a < W; ++a) {
+                    const double2* row = tile + (i10 + a) * tg.TC + i20;
+                    double2 sr = make_double2(0.0, 0.0);
+#pragma unroll
+                    for (int c = 0; c < W; ++c) {
+                        const double2 u = row[c];
+                        sr.x = fma(u.x, k2[c], sr.x);
+                        sr.y = fma(u.y, k2[c], sr.y);
+                    }
+                    acc.x = fma(sr.x, k1[a], acc.x);
+                    acc.y = fma(sr.y, k1[a], acc.y);
+                }
+            }
+            f[perm[p] + M * b] = acc;
+        }
+        __syncthreads();
+    }
+}
+
+// Type-1 spreading: one warp per bin accumulates the bin's points into a tile of its own
+// in shared memory (no atomics), thread per point, then adds the tile to U. Lanes of one
+// round have distinct first rows, and the warp synchronises after every kernel row, so two
+// lanes never update one cell in the same row step.
+template <int W>
+__global__ void __launch_bounds__(128)
+spread_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
+              const int* __restrict__ binstart, int nbins, int nbc, int BR, int BC, int64_t M,
+              const double2* __restrict__ fin, int b, int nrows, int nf2, int row_wrap,
+              double2* __restrict__ U) {
+    extern __shared__ double2 smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int bin = blockIdx.x * (blockDim.x >> 5) + warp;
+    if (bin >= nbins) return;
+    const int s = binstart[bin], e = binstart[bin + 1];
+    if (s == e) return;
+    const TileGeom tg = tile_geom<W>(bin, nbc, BR, BC);
+    double2* tile = smem + warp * tg.TR * tg.TC;
+    for (int t = lane; t < tg.TR * tg.TC; t += 32) tile[t] = make_double2(0.0, 0.0);
+    __syncwarp();
+    const int n = e - s;
+    const int nb = (n + 31) >> 5;
+    for (int bt = 0; bt < nb; ++bt) {
+        // interleave: lane l takes sorted position l*nb + bt, so one batch spans the bin
+        const int pos = lane * nb + bt;
+        const bool act = pos < n;
+        const unsigned amask = __ballot_sync(0xffffffffu, act);
+        if (!act) continue;
+        const int p = s + pos;
         const double2 g = pts[p];
         const double2 v = fin[perm[p] + M * b];
         double k1[W], k2[W];
-        const int i10 = taps<W>(g.x, beta, k1) - tr0;
-        const int i20 = taps<W>(g.y, beta, k2) - tc0;
+        const int i10 = es_taps<W>(g.x, k1) - tg.tr0;
+        const int i20 = es_taps<W>(g.y, k2) - tg.tc0;
+        const bool inside = i10 >= 0 && i10 + W <= tg.TR && i20 >= 0 && i20 + W <= tg.TC;
+        const unsigned peers = __match_any_sync(amask, i10);
+        const int rank = __popc(peers & ((1u << lane) - 1u));
+        const int nround = __reduce_max_sync(amask, (unsigned)__popc(peers));
+        for (int rd = 0; rd < nround; ++rd) {
+            const bool mine = rank == rd && inside;
 #pragma unroll
-        for (int a = 0; a < W; ++a) {
-            const int rr = i10 + a;
-            if (rr < 0 || rr >= TR) continue;
-            const double vx = v.x * k1[a], vy = v.y * k1[a];
+            for (int a = 0; a < W; ++a) {
+                if (mine) {
+                    double2* row = tile + (i10 + a) * tg.TC + i20;
+                    const double vx = v.x * k1[a], vy = v.y * k1[a];
 #pragma unroll
-            for (int c = 0; c < W; ++c) {
-                const int cc = i20 + c;
-                if (cc < 0 || cc >= TC) continue;
-                double* q = reinterpret_cast<double*>(&tile[rr * TC + cc]);
-                atomicAdd(q, vx * k2[c]);
-                atomicAdd(q + 1, vy * k2[c]);
+                    for (int c = 0; c < W; ++c) {
+                        double2 u = row[c];
+                        u.x = fma(vx, k2[c], u.x);
+                        u.y = fma(vy, k2[c], u.y);
+                        row[c] = u;
+                    }
+                }
+                __syncwarp(amask);
             }
         }
     }
-    __syncthreads();
+    __syncwarp();
     double2* ub = U + (int64_t)nrows * nf2 * b;
-    for (int t = threadIdx.x; t < TR * TC; t += blockDim.x) {
-        const double2 v = tile[t];
-        if (v.x == 0.0 && v.y == 0.0) continue;
-        int r = tr0 + t / TC;
+    for (int t = lane; t < tg.TR * tg.TC; t += 32) {
+        const double2 val = tile[t];
+        if (val.x == 0.0 && val.y == 0.0) continue;
+        int r = tg.tr0 + t / tg.TC;
         if (row_wrap) r = wrap(r, nrows);
         if (r < 0 || r >= nrows) continue;
-        const int c = wrap(tc0 + t % TC, nf2);
-        double* q = reinterpret_cast<double*>(ub + (int64_t)r * nf2 + c);
-        atomicAdd(q, v.x);
-        atomicAdd(q + 1, v.y);
+        double* q = reinterpret_cast<double*>(ub + (int64_t)r * nf2 + wrap(tg.tc0 + t % tg.TC, nf2));
+        atomicAdd(q, val.x);
+        atomicAdd(q + 1, val.y);
     }
 }
 
 template <int W>
 static int launch_interp(const NufftGrid& g, NufftDev& d, double2* f, int B, cudaStream_t s) {
-    interp_kernel<W><<<nblk(g.M, 256), 256, 0, s>>>(d.pts.as<double2>(), d.perm.as<int>(), g.M,
-                                                     d.U.as<double2>(), g.nrows, g.nf2,
-                                                     g.row_wrap, g.beta, B, f);
+    const size_t smem = sizeof(double2) * (g.bin_rows + W + 1) * (g.bin_cols + W + 1);
+    if (smem > 48 * 1024)
+        PF_CUDA(cudaFuncSetAttribute(interp_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    interp_kernel<W><<<g.nbr * g.nbc, 128, smem, s>>>(
+        d.pts.as<double2>(), d.perm.as<int>(), d.binstart.as<int>(), g.nbc, g.bin_rows,
+        g.bin_cols, g.M, d.U.as<double2>(), g.nrows, g.nf2, g.row_wrap, B, f);
     return check_launch("interp_kernel");
 }
 
 template <int W>
 static int launch_spread(const NufftGrid& g, NufftDev& d, const double2* f, int B, cudaStream_t s) {
-    const size_t smem = sizeof(double2) * (g.bin_rows + W + 1) * (g.bin_cols + W + 1);
+    constexpr int kWarps = 4;
+    const size_t smem = kWarps * sizeof(double2) * (g.bin_rows + W + 1) * (g.bin_cols + W + 1);
     if (smem > 48 * 1024)
-        PF_CUDA(cudaFuncSetAttribute(spread_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem));
+        PF_CUDA(cudaFuncSetAttribute(spread_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int nbins = g.nbr * g.nbc;
     for (int b = 0; b < B; ++b) {
-        spread_kernel<W><<<g.nbr * g.nbc, 256, smem, s>>>(
-            d.pts.as<double2>(), d.perm.as<int>(), d.binstart.as<int>(), g.nbc, g.bin_rows,
-            g.bin_cols, g.M, f, b, g.nrows, g.nf2, g.row_wrap, g.beta, d.U.as<double2>());
+        spread_kernel<W><<<(nbins + kWarps - 1) / kWarps, 32 * kWarps, smem, s>>>(
+            d.pts.as<double2>(), d.perm.as<int>(), d.binstart.as<int>(), nbins, g.nbc,
+            g.bin_rows, g.bin_cols, g.M, f, b, g.nrows, g.nf2, g.row_wrap, d.U.as<double2>());
         PF_TRY(check_launch("spread_kernel"));
     }
     return 0;

@@ -41,13 +41,13 @@ struct pfsht_plan {
     int L = 0, B = 1;
     int64_t M = 0;
     double tol = 0;
-    int R = 4;
+    int R = 0;  // ring tile rings-per-lane override (0 = defaults)
     Leaf leaf;
     int ncols = 0;
     int nrings = 0;
     // ring pass
-    DevBuf cos_t, log2sin, log2c, w, ab, aboff, items;
-    int nitems = 0;
+    DevBuf cos_t, log2sin, log2c, w, ab, aboff;
+    RingItemsOwner fwd_items, adj_items;
     RingTables rt;
     RingOut ro_cols;  // the apply's column array H (or G for the direct leaf)
     // column array: nth x ncols x B (stretch) or M x (2L+1) x B (direct)
@@ -117,8 +117,8 @@ int setup_nufft_grid(NufftGrid& g, NufftDev& d, int n1, int nmodes2, const std::
     g.n1 = n1;
     g.ncols = (int)colk2.size();
     g.M = M;
-    g.bin_rows = bin_rows > 0 ? bin_rows : 16;
-    g.bin_cols = bin_cols > 0 ? bin_cols : 16;
+    g.bin_rows = bin_rows > 0 ? bin_rows : 32;
+    g.bin_cols = bin_cols > 0 ? bin_cols : 8;
     if (full_rows) {
         g.row0 = 0;
         g.nrows = g.nf1;
@@ -208,7 +208,7 @@ void fill_info(pfsht_plan* p) {
         in.ncols = p->ng.ncols;
     }
     int64_t bytes = 0;
-    for (const DevBuf* b : {&p->cos_t, &p->log2sin, &p->log2c, &p->w, &p->ab, &p->aboff, &p->items,
+    for (const DevBuf* b : {&p->cos_t, &p->log2sin, &p->log2c, &p->w, &p->ab, &p->aboff, &p->fwd_items.items, &p->adj_items.items,
                             &p->H, &p->phi_pts, &p->nd.pts, &p->nd.perm, &p->nd.binstart,
                             &p->nd.colp2, &p->nd.p2col, &p->nd.mult1, &p->nd.dec2, &p->nd.pad,
                             &p->nd.U, &p->st_alm, &p->st_f})
@@ -227,9 +227,9 @@ int build_stretch(pfsht_plan* p, const double* d_theta, const double* d_phi, con
     PF_TRY(upload(p->log2c, lf.log2c, s));
     PF_TRY(upload(p->w, lf.w, s));
     PF_TRY(build_ab_table(L, lf.mmax, p->ab, p->aboff, s));
-    std::vector<RingItem> items = make_ring_items(lf.jlo, lf.jhi, L, lf.mmax, p->R);
-    p->nitems = (int)items.size();
-    PF_TRY(upload(p->items, items, s));
+    // forward tiles of 64 rings (more warps), adjoint tiles of 128 (amortises its reduction)
+    PF_TRY(build_ring_items(lf.jlo, lf.jhi, L, lf.mmax, p->R > 0 ? p->R : 2, p->fwd_items, s));
+    PF_TRY(build_ring_items(lf.jlo, lf.jhi, L, lf.mmax, p->R > 0 ? p->R : 4, p->adj_items, s));
     p->rt.cos_t = p->cos_t.as<double>();
     p->rt.log2sin = p->log2sin.as<double>();
     p->rt.log2c = p->log2c.as<double>();
@@ -245,6 +245,8 @@ int build_stretch(pfsht_plan* p, const double* d_theta, const double* d_phi, con
     p->ro_cols.nrows = lf.nth;
     p->ro_cols.reflect = lf.g.kind == kInterior ? 0 : 1;
     p->ro_cols.spin_sgn = 1.0;
+    p->ro_cols.nrings_out = lf.nth_half;
+    p->ro_cols.zero_rest = 1;
     PF_TRY(p->H.alloc(sizeof(double2) * (size_t)lf.nth * p->ncols * B));
     int n[1] = {lf.nth};
     PF_CUFFT(cufftPlanMany(&p->fth, 1, n, n, 1, lf.nth, n, 1, lf.nth, CUFFT_Z2Z, p->ncols * B));
@@ -298,9 +300,8 @@ int build_direct(pfsht_plan* p, const double* h_theta, const double* h_phi, cuda
     PF_TRY(build_ab_table(L, L, p->ab, p->aboff, s));
     // eps = 0: every order on every point (src/Direct.jl:262-263)
     std::vector<int> jlo(L + 1, 0), jhi(L + 1, (int)M - 1);
-    std::vector<RingItem> items = make_ring_items(jlo, jhi, L, L, p->R);
-    p->nitems = (int)items.size();
-    PF_TRY(upload(p->items, items, s));
+    PF_TRY(build_ring_items(jlo, jhi, L, L, p->R > 0 ? p->R : 2, p->fwd_items, s));
+    PF_TRY(build_ring_items(jlo, jhi, L, L, p->R > 0 ? p->R : 4, p->adj_items, s));
     p->rt.cos_t = p->cos_t.as<double>();
     p->rt.log2sin = p->log2sin.as<double>();
     p->rt.log2c = p->log2c.as<double>();
@@ -316,6 +317,8 @@ int build_direct(pfsht_plan* p, const double* h_theta, const double* h_phi, cuda
     p->ro_cols.nrows = (int)M;
     p->ro_cols.reflect = 0;
     p->ro_cols.spin_sgn = 1.0;
+    p->ro_cols.nrings_out = (int)M;
+    p->ro_cols.zero_rest = 0;  // every point keeps every order
     PF_TRY(p->H.alloc(sizeof(double2) * (size_t)M * (2 * L + 1) * B));
     return 0;
 }
@@ -346,7 +349,7 @@ int plan_create(const double* theta, const double* phi, int64_t npts, int lmax, 
     p->B = ntrans;
     p->M = npts;
     p->tol = tol;
-    p->R = o.ring_rings_per_lane > 0 ? o.ring_rings_per_lane : 4;
+    p->R = o.ring_rings_per_lane == 2 || o.ring_rings_per_lane == 4 ? o.ring_rings_per_lane : 0;
     PF_CUDA(cudaStreamCreateWithFlags(&p->st_stream, cudaStreamNonBlocking));
     cudaStream_t s = p->st_stream;
 
@@ -413,8 +416,7 @@ int plan_create(const double* theta, const double* phi, int64_t npts, int lmax, 
 
 int apply_forward(pfsht_plan* p, const double2* alm, double2* f, cudaStream_t s) {
     const int B = p->B;
-    PF_CUDA(cudaMemsetAsync(p->H.p, 0, p->H.bytes, s));
-    PF_TRY(ring_forward(p->rt, p->ro_cols, p->items.as<RingItem>(), p->nitems, p->R, alm,
+    PF_TRY(ring_forward(p->rt, p->ro_cols, p->fwd_items.view, alm,
                         p->H.as<double2>(), B, s));
     if (p->kind == kDirect)
         return direct_phase_sum(p->H.as<double2>(), p->phi_pts.as<double>(), p->M, p->L, B, f, s);
@@ -426,7 +428,6 @@ int apply_forward(pfsht_plan* p, const double2* alm, double2* f, cudaStream_t s)
 
 int apply_adjoint(pfsht_plan* p, const double2* f, double2* alm, cudaStream_t s) {
     const int B = p->B;
-    const size_t alm_bytes = sizeof(double2) * (size_t)(p->L + 1) * (2 * p->L + 1) * B;
     if (p->kind == kDirect) {
         PF_TRY(direct_phase_spread(f, p->phi_pts.as<double>(), p->M, p->L, B, p->H.as<double2>(), s));
     } else {
@@ -435,8 +436,7 @@ int apply_adjoint(pfsht_plan* p, const double2* f, double2* alm, cudaStream_t s)
         PF_CUFFT(cufftExecZ2Z(p->fth, p->H.as<cufftDoubleComplex>(), p->H.as<cufftDoubleComplex>(),
                               CUFFT_INVERSE));
     }
-    PF_CUDA(cudaMemsetAsync(alm, 0, alm_bytes, s));
-    return ring_adjoint(p->rt, p->ro_cols, p->items.as<RingItem>(), p->nitems, p->R,
+    return ring_adjoint(p->rt, p->ro_cols, p->adj_items.view,
                         p->H.as<double2>(), alm, B, s);
 }
 
@@ -527,10 +527,12 @@ pfsht_status pfsht_ring_forward(pfsht_plan* p, const void* alm, void* G, void* s
     o.col_off = p->L;
     o.nrows = p->nrings;
     o.reflect = 0;
+    o.nrings_out = p->nrings;
+    o.zero_rest = 0;  // the whole G is cleared first: orders above mmax have no item
     const size_t bytes = sizeof(double2) * (size_t)o.bstride * p->B;
     cudaError_t e = cudaMemsetAsync(G, 0, bytes, s);
     if (e != cudaSuccess) return (pfsht_status)fail(PFSHT_ERR_CUDA, cudaGetErrorString(e));
-    return (pfsht_status)ring_forward(t, o, p->items.as<RingItem>(), p->nitems, p->R,
+    return (pfsht_status)ring_forward(t, o, p->fwd_items.view,
                                       (const double2*)alm, (double2*)G, p->B, s);
 }
 
@@ -547,10 +549,8 @@ pfsht_status pfsht_ring_adjoint(pfsht_plan* p, const void* G, void* alm, void* s
     o.col_off = p->L;
     o.nrows = p->nrings;
     o.reflect = 0;
-    const size_t bytes = sizeof(double2) * (size_t)(p->L + 1) * (2 * p->L + 1) * p->B;
-    cudaError_t e = cudaMemsetAsync(alm, 0, bytes, s);
-    if (e != cudaSuccess) return (pfsht_status)fail(PFSHT_ERR_CUDA, cudaGetErrorString(e));
-    return (pfsht_status)ring_adjoint(t, o, p->items.as<RingItem>(), p->nitems, p->R,
+    o.nrings_out = p->nrings;
+    return (pfsht_status)ring_adjoint(t, o, p->adj_items.view,
                                       (const double2*)G, (double2*)alm, p->B, s);
 }
 
@@ -708,5 +708,7 @@ size_t pfsht_last_error(char* buf, size_t len) {
 }
 
 const char* pfsht_version(void) { return "pfsht_b200 0.1.0 (sm_100a)"; }
+
+int64_t pfsht_launch_count(void) { return (int64_t)launch_count(); }
 
 }  // extern "C"

@@ -2,22 +2,27 @@
 // alm_from_rings! (PartialFSHT.jl src/Legendre.jl:310-542; device analogue of
 // ext/PartialFSHTKernelAbstractionsExt.jl:86-230).
 //
-// Work decomposition: one warp per item (order m, tile of up to 128 consecutive retained
-// rings); a lane owns R rings (ring j0 + lane + 32 r) and carries their two-term recurrence
-// state and block-scaling exponent in registers. The recurrence is the reference's
+// Work decomposition: one warp per item (order m, tile of consecutive retained rings); a
+// lane owns R rings (ring j0 + lane + 32 r, R = ceil(tile / 32) chosen per item) and keeps
+// their two-term recurrence state and block-scaling exponent in registers. The recurrence
+// is the reference's
 //     P_m^m = (-1)^m 2^(m log2 sin + log2 c_m),   P_{m+1}^m = sqrt(2m+3) cos P_m^m,
 //     P_l^m = a_l^m cos P_{l-1}^m - b_l^m P_{l-2}^m
 // renormalised every 64 degrees (src/Legendre.jl:16,455-459). Each ring keeps its own
 // exponent (as the KernelAbstractions kernel does), so no chunk headroom rule is needed.
 // a_l^m, b_l^m come from a plan-time table built on the device with the reference's exact
-// expressions; per block of 32 degrees a warp stages them and the coefficients a_{l,+-m}
-// in shared memory, so the inner loop reads them as broadcasts.
+// expressions. Per chunk of 32 degrees a warp stages them and the coefficients a_{l,+-m}
+// in shared memory; the chunk is walked in fixed, fully unrolled blocks of degrees with no
+// branch inside a block, so successive degrees overlap in the pipeline; renormalisation
+// falls on block boundaries because 64 is a multiple of the block.
 //
 // Forward: acc(ring, +-m) += a_{l,+-m} P_l^m, written once per ring, windowed and, for a
-// pole/full periodisation, mirrored into the DFS row with sign (-1)^m (src/DFS.jl:26).
-// Adjoint: each lane sums P_l^m g_j over its R rings; per block of degrees the lanes'
-// partial sums are transposed through shared memory and each lane reduces one
-// (degree, component) over the 32 lanes, then adds it to alm once per item.
+// pole/full periodisation, mirrored into the DFS row with sign (-1)^m (src/DFS.jl:26). The
+// first tile of each order also writes the zeros of the rings the order does not retain.
+// Adjoint: each lane sums P_l^m g_j over its R rings; per block of degrees the lanes' partial
+// sums are transposed through shared memory and each lane reduces one (degree, component)
+// over the 32 lanes. An order covered by a single tile stores its coefficients; an order
+// split over several tiles adds them atomically (into zeros).
 #include <algorithm>
 #include <cmath>
 
@@ -26,8 +31,7 @@
 namespace pf {
 
 static constexpr int kWarpsPerBlock = 4;
-static constexpr int kTileRings = 128;  // rings per work item
-static constexpr int kStride = 64;      // _RESCALE_STRIDE (src/Legendre.jl:16)
+static constexpr int kStride = 64;  // _RESCALE_STRIDE (src/Legendre.jl:16)
 
 // ---------------------------------------------------------------------------------------
 // recurrence coefficient table, exact expressions of src/Legendre.jl:406-408
@@ -69,14 +73,20 @@ int build_ab_table(int L, int mmax, DevBuf& ab, DevBuf& aboff, cudaStream_t s) {
 }
 
 std::vector<RingItem> make_ring_items(const std::vector<int>& jlo, const std::vector<int>& jhi,
-                                      int L, int mmax, int /*R*/) {
+                                      int L, int mmax, int tile) {
     std::vector<RingItem> items;
     std::vector<int64_t> cost;
     for (int m = 0; m <= std::min(mmax, L); ++m) {
         int lo = jlo[m], hi = jhi[m];
-        for (int j0 = lo; j0 <= hi; j0 += kTileRings) {
-            int n = std::min(kTileRings, hi - j0 + 1);
-            items.push_back(RingItem{m, j0, n, 0});
+        if (hi < lo) continue;
+        const int ntiles = (hi - lo + tile) / tile;
+        for (int t = 0; t < ntiles; ++t) {
+            const int j0 = lo + t * tile;
+            const int n = std::min(tile, hi - j0 + 1);
+            int flags = 0;
+            if (t == 0) flags |= kItemFirst;
+            if (ntiles == 1) flags |= kItemSole;
+            items.push_back(RingItem{m, j0, n, flags});
             cost.push_back((int64_t)((n + 31) / 32) * (L - m + 1));
         }
     }
@@ -101,123 +111,134 @@ __device__ __forceinline__ double2 cmad(double2 acc, double2 a, double p) {
     return acc;
 }
 
+// seed of ring j for order m (src/Legendre.jl:379-382, exponent per ring as in
+// ext/PartialFSHTKernelAbstractionsExt.jl:96-99)
+__device__ __forceinline__ void ring_seed(const RingTables& t, int m, int j, double sgn,
+                                          double& x, double& p2, int& E) {
+    x = t.cos_t[j];
+    const double e0 = m == 0 ? t.log2c[0] : (double)m * t.log2sin[j] + t.log2c[m];
+    p2 = 0.0;
+    E = 0;
+    if (isfinite(e0)) {
+        const double Es = ceil(e0);
+        p2 = sgn * exp2(e0 - Es);
+        E = (int)Es;
+    }
+}
+
 // ---------------------------------------------------------------------------------------
 // forward: alm -> ring columns
 // ---------------------------------------------------------------------------------------
+template <int NB>
+struct FwdSmem {
+    double2 ab[kWarpsPerBlock][32];
+    double2 ap[kWarpsPerBlock][NB][32];
+    double2 am[kWarpsPerBlock][NB][32];
+};
+
 template <int R, int NB>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32)
-ring_fwd_kernel(RingTables t, RingOut o, const RingItem* __restrict__ items, int nitems,
-                const double2* __restrict__ alm, double2* __restrict__ out, int b0) {
-    __shared__ double2 s_ab[kWarpsPerBlock][32];
-    __shared__ double2 s_ap[kWarpsPerBlock][NB][32];
-    __shared__ double2 s_am[kWarpsPerBlock][NB][32];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int it = blockIdx.x * kWarpsPerBlock + warp;
-    if (it >= nitems) return;
-    const RingItem item = items[it];
+__device__ __forceinline__ void ring_fwd_item(const RingTables& t, const RingOut& o,
+                                              const RingItem& item, const double2* __restrict__ alm,
+                                              double2* __restrict__ out, int b0, FwdSmem<NB>& sm,
+                                              int warp, int lane) {
     const int m = item.m, L = t.lmax;
     const double sgn = (m & 1) ? -1.0 : 1.0;
     const int64_t albs = (int64_t)(L + 1) * (2 * L + 1);
     const double2* colp = alm + albs * b0 + (int64_t)(L + 1) * (2 * m);
     const double2* colm = alm + albs * b0 + (int64_t)(L + 1) * (m > 0 ? 2 * m - 1 : 0);
     const double2* abm = t.ab + t.aboff[m];
-    const double s23 = sqrt((double)(2 * m + 3));
     const double2 zero2 = make_double2(0.0, 0.0);
 
-    for (int pass = 0; pass * 32 * R < item.n; ++pass) {
-        const int kbase = pass * 32 * R;
-        double x[R], p1[R], p2[R];
-        int E[R];
-        double2 accp[R][NB], accm[R][NB];
+    double x[R], p1[R], p2[R];
+    int E[R];
+    double2 accp[R][NB], accm[R][NB];
 #pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const int k = kbase + lane + 32 * r;
-            x[r] = 0.0;
-            p1[r] = 0.0;
-            p2[r] = 0.0;
-            E[r] = 0;
-            if (k < item.n) {
-                const int j = item.j0 + k;
-                x[r] = t.cos_t[j];
-                const double e0 = m == 0 ? t.log2c[0] : (double)m * t.log2sin[j] + t.log2c[m];
-                if (isfinite(e0)) {
-                    const double Es = ceil(e0);
-                    p2[r] = sgn * exp2(e0 - Es);
-                    E[r] = (int)Es;
-                }
-            }
-#pragma unroll
-            for (int b = 0; b < NB; ++b) {
-                accp[r][b] = zero2;
-                accm[r][b] = zero2;
-            }
-        }
-        // l = m: P = seed
+    for (int r = 0; r < R; ++r) {
+        const int k = lane + 32 * r;
+        x[r] = 0.0;
+        p1[r] = 0.0;
+        p2[r] = 0.0;
+        E[r] = 0;
+        if (k < item.n) ring_seed(t, m, item.j0 + k, sgn, x[r], p2[r], E[r]);
 #pragma unroll
         for (int b = 0; b < NB; ++b) {
-            const double2 ap = colp[albs * b];
-            double2 am = m > 0 ? colm[albs * b] : zero2;
+            accp[r][b] = zero2;
+            accm[r][b] = zero2;
+        }
+    }
+    // l = m: P = seed
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+        const double2 ap = colp[albs * b];
+        double2 am = m > 0 ? colm[albs * b] : zero2;
+        am.x *= sgn;
+        am.y *= sgn;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            accp[r][b] = cmad(accp[r][b], ap, p2[r]);
+            accm[r][b] = cmad(accm[r][b], am, p2[r]);
+        }
+    }
+    if (m < L) {
+        const double s23 = sqrt((double)(2 * m + 3));
+#pragma unroll
+        for (int r = 0; r < R; ++r) p1[r] = s23 * x[r] * p2[r];
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            const double2 ap = colp[1 + albs * b];
+            double2 am = m > 0 ? colm[1 + albs * b] : zero2;
             am.x *= sgn;
             am.y *= sgn;
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-                accp[r][b] = cmad(accp[r][b], ap, p2[r]);
-                accm[r][b] = cmad(accm[r][b], am, p2[r]);
+                accp[r][b] = cmad(accp[r][b], ap, p1[r]);
+                accm[r][b] = cmad(accm[r][b], am, p1[r]);
             }
         }
-        if (m < L) {
-            // l = m + 1
+        auto step = [&](int i) {
+            const double2 ab = sm.ab[warp][i];
 #pragma unroll
-            for (int r = 0; r < R; ++r) p1[r] = s23 * x[r] * p2[r];
+            for (int r = 0; r < R; ++r) {
+                const double p = fma(ab.x * x[r], p1[r], -(ab.y * p2[r]));
+                p2[r] = p1[r];
+                p1[r] = p;
+            }
 #pragma unroll
             for (int b = 0; b < NB; ++b) {
-                const double2 ap = colp[1 + albs * b];
-                double2 am = m > 0 ? colm[1 + albs * b] : zero2;
-                am.x *= sgn;
-                am.y *= sgn;
+                const double2 ap = sm.ap[warp][b][i];
+                const double2 am = sm.am[warp][b][i];
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
                     accp[r][b] = cmad(accp[r][b], ap, p1[r]);
                     accm[r][b] = cmad(accm[r][b], am, p1[r]);
                 }
             }
-            int steps = 0;
-            for (int l0 = m + 2; l0 <= L; l0 += 32) {
-                const int nl = min(32, L - l0 + 1);
-                __syncwarp();
-                if (lane < nl) {
-                    const int l = l0 + lane;
-                    s_ab[warp][lane] = abm[l - m - 2];
+        };
+        int steps = 0;
+        for (int l0 = m + 2; l0 <= L; l0 += 32) {
+            const int nl = min(32, L - l0 + 1);
+            __syncwarp();
+            if (lane < nl) {
+                const int l = l0 + lane;
+                sm.ab[warp][lane] = abm[l - m - 2];
 #pragma unroll
-                    for (int b = 0; b < NB; ++b) {
-                        s_ap[warp][b][lane] = colp[(l - m) + albs * b];
-                        double2 am = m > 0 ? colm[(l - m) + albs * b] : zero2;
-                        am.x *= sgn;
-                        am.y *= sgn;
-                        s_am[warp][b][lane] = am;
-                    }
+                for (int b = 0; b < NB; ++b) {
+                    sm.ap[warp][b][lane] = colp[(l - m) + albs * b];
+                    double2 am = m > 0 ? colm[(l - m) + albs * b] : zero2;
+                    am.x *= sgn;
+                    am.y *= sgn;
+                    sm.am[warp][b][lane] = am;
                 }
-                __syncwarp();
-                for (int i = 0; i < nl; ++i) {
-                    const double2 ab = s_ab[warp][i];
+            }
+            __syncwarp();
+            const int nblk = nl >> 3;
+            for (int blk = 0; blk < nblk; ++blk) {
 #pragma unroll
-                    for (int r = 0; r < R; ++r) {
-                        const double p = fma(ab.x * x[r], p1[r], -(ab.y * p2[r]));
-                        p2[r] = p1[r];
-                        p1[r] = p;
-                    }
-#pragma unroll
-                    for (int b = 0; b < NB; ++b) {
-                        const double2 ap = s_ap[warp][b][i];
-                        const double2 am = s_am[warp][b][i];
-#pragma unroll
-                        for (int r = 0; r < R; ++r) {
-                            accp[r][b] = cmad(accp[r][b], ap, p1[r]);
-                            accm[r][b] = cmad(accm[r][b], am, p1[r]);
-                        }
-                    }
-                    if (++steps == kStride && l0 + i < L) {
-                        steps = 0;
+                for (int i = 0; i < 8; ++i) step(blk * 8 + i);
+                steps += 8;
+                if (steps == kStride) {
+                    steps = 0;
+                    if (l0 + blk * 8 + 7 < L) {
 #pragma unroll
                         for (int r = 0; r < R; ++r) {
                             const double mx = fmax(fabs(p1[r]), fabs(p2[r]));
@@ -241,175 +262,218 @@ ring_fwd_kernel(RingTables t, RingOut o, const RingItem* __restrict__ items, int
                     }
                 }
             }
+            for (int i = nblk * 8; i < nl; ++i) step(i);
         }
-        // write the ring columns (window and 2^E folded into one exact scale)
-        const double smir = o.spin_sgn * sgn;
+    }
+    // write the ring columns (window and 2^E folded into one exact scale)
+    const double smir = o.spin_sgn * sgn;
 #pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const int k = kbase + lane + 32 * r;
-            if (k >= item.n) continue;
-            const int j = item.j0 + k;
-            const double sc = scalbn(t.w ? t.w[j] : 1.0, E[r]);
+    for (int r = 0; r < R; ++r) {
+        const int k = lane + 32 * r;
+        if (k >= item.n) continue;
+        const int j = item.j0 + k;
+        const double sc = scalbn(t.w ? t.w[j] : 1.0, E[r]);
 #pragma unroll
-            for (int b = 0; b < NB; ++b) {
-                double2* ob = out + o.bstride * (b0 + b);
-                const double2 gp = make_double2(accp[r][b].x * sc, accp[r][b].y * sc);
-                const double2 gm = make_double2(accm[r][b].x * sc, accm[r][b].y * sc);
-                ob[j + o.ld * (o.col_off + m)] = gp;
-                if (m > 0) ob[j + o.ld * (o.col_off - m)] = gm;
-                if (o.reflect) {
-                    const int jj = o.nrows - 1 - j;
-                    ob[jj + o.ld * (o.col_off + m)] = make_double2(gp.x * smir, gp.y * smir);
-                    if (m > 0) ob[jj + o.ld * (o.col_off - m)] = make_double2(gm.x * smir, gm.y * smir);
-                }
+        for (int b = 0; b < NB; ++b) {
+            double2* ob = out + o.bstride * (b0 + b);
+            const double2 gp = make_double2(accp[r][b].x * sc, accp[r][b].y * sc);
+            const double2 gm = make_double2(accm[r][b].x * sc, accm[r][b].y * sc);
+            ob[j + o.ld * (o.col_off + m)] = gp;
+            if (m > 0) ob[j + o.ld * (o.col_off - m)] = gm;
+            if (o.reflect) {
+                const int jj = o.nrows - 1 - j;
+                ob[jj + o.ld * (o.col_off + m)] = make_double2(gp.x * smir, gp.y * smir);
+                if (m > 0) ob[jj + o.ld * (o.col_off - m)] = make_double2(gm.x * smir, gm.y * smir);
             }
         }
     }
 }
 
-// ---------------------------------------------------------------------------------------
-// adjoint: ring columns -> alm (alm must be zeroed; one atomic add per item and output)
-// ---------------------------------------------------------------------------------------
-template <int R, int NB>
+// zeros in the order's columns for the rings it does not retain (first tile only)
+template <int NB>
+__device__ __forceinline__ void ring_fwd_zero_rest(const RingOut& o, const RingItem& item,
+                                                   int lo, int hi, double2* __restrict__ out,
+                                                   int b0, int lane) {
+    const int m = item.m;
+    const double2 z = make_double2(0.0, 0.0);
+    for (int b = 0; b < NB; ++b) {
+        double2* ob = out + o.bstride * (b0 + b);
+        for (int j = lane; j < o.nrings_out; j += 32) {
+            if (j >= lo && j <= hi) continue;
+            ob[j + o.ld * (o.col_off + m)] = z;
+            if (m > 0) ob[j + o.ld * (o.col_off - m)] = z;
+            if (o.reflect) {
+                const int jj = o.nrows - 1 - j;
+                ob[jj + o.ld * (o.col_off + m)] = z;
+                if (m > 0) ob[jj + o.ld * (o.col_off - m)] = z;
+            }
+        }
+    }
+}
+
+template <int RMAX, int NB>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32)
-ring_adj_kernel(RingTables t, RingOut o, const RingItem* __restrict__ items, int nitems,
-                const double2* __restrict__ in, double* __restrict__ almd, int b0) {
-    constexpr int NV = 4 * NB;   // (+m re, +m im, -m re, -m im) per transform
-    constexpr int LB = 32 / NV;  // degrees per reduction block
-    __shared__ double s_red[kWarpsPerBlock][32][33];
-    __shared__ double2 s_ab[kWarpsPerBlock][32];
+ring_fwd_kernel(RingTables t, RingOut o, const RingItem* __restrict__ items, int nitems,
+                const int* __restrict__ jlo, const int* __restrict__ jhi,
+                const double2* __restrict__ alm, double2* __restrict__ out, int b0) {
+    __shared__ FwdSmem<NB> sm;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int it = blockIdx.x * kWarpsPerBlock + warp;
     if (it >= nitems) return;
     const RingItem item = items[it];
+    if ((item.flags & kItemFirst) && o.zero_rest)
+        ring_fwd_zero_rest<NB>(o, item, jlo[item.m], jhi[item.m], out, b0, lane);
+    for (int base = 0; base < item.n; base += 32 * RMAX) {
+        RingItem sub = item;
+        sub.j0 = item.j0 + base;
+        sub.n = min(32 * RMAX, item.n - base);
+        const int reff = (sub.n + 31) >> 5;
+        if (RMAX >= 4 && reff >= 3) ring_fwd_item<(RMAX >= 4 ? 4 : 1), NB>(t, o, sub, alm, out, b0, sm, warp, lane);
+        else if (RMAX >= 2 && reff == 2) ring_fwd_item<(RMAX >= 2 ? 2 : 1), NB>(t, o, sub, alm, out, b0, sm, warp, lane);
+        else ring_fwd_item<1, NB>(t, o, sub, alm, out, b0, sm, warp, lane);
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// adjoint: ring columns -> alm
+// ---------------------------------------------------------------------------------------
+struct AdjSmem {
+    double red[kWarpsPerBlock][32][33];
+    double2 ab[kWarpsPerBlock][32];
+};
+
+template <int R, int NB>
+__device__ __forceinline__ void ring_adj_item(const RingTables& t, const RingOut& o,
+                                              const RingItem& item, const double2* __restrict__ in,
+                                              double* __restrict__ almd, int b0, bool sole,
+                                              AdjSmem& sm, int warp, int lane) {
+    constexpr int NV = 4 * NB;   // (+m re, +m im, -m re, -m im) per transform
+    constexpr int LB = 32 / NV;  // degrees per reduction block
     const int m = item.m, L = t.lmax;
     const double sgn = (m & 1) ? -1.0 : 1.0;
     const double smir = o.spin_sgn * sgn;
     const int64_t albs = (int64_t)(L + 1) * (2 * L + 1);
     const double2* abm = t.ab + t.aboff[m];
-    const double s23 = sqrt((double)(2 * m + 3));
     const int64_t cp = (int64_t)(L + 1) * (2 * m);
     const int64_t cm = (int64_t)(L + 1) * (m > 0 ? 2 * m - 1 : 0);
 
-    for (int pass = 0; pass * 32 * R < item.n; ++pass) {
-        const int kbase = pass * 32 * R;
-        double x[R], p1[R], p2[R];
-        int E[R];
-        double2 gp[R][NB], gm[R][NB];
-        // ring data for (ring r, transform b): folded, windowed, scaled by 2^E; the -m
-        // column carries the (-1)^m of src/Legendre.jl:511
-        auto load_g = [&](int r) {
-            const int k = kbase + lane + 32 * r;
+    double x[R], p1[R], p2[R];
+    int E[R];
+    double2 gp[R][NB], gm[R][NB];
+    // ring data for (ring r, transform b): folded, windowed, scaled by 2^E; the -m column
+    // carries the (-1)^m of src/Legendre.jl:511
+    auto load_g = [&](int r) {
+        const int k = lane + 32 * r;
 #pragma unroll
-            for (int b = 0; b < NB; ++b) {
-                gp[r][b] = make_double2(0.0, 0.0);
-                gm[r][b] = make_double2(0.0, 0.0);
+        for (int b = 0; b < NB; ++b) {
+            gp[r][b] = make_double2(0.0, 0.0);
+            gm[r][b] = make_double2(0.0, 0.0);
+        }
+        if (k >= item.n) return;
+        const int j = item.j0 + k;
+        const double sc = scalbn(t.w ? t.w[j] : 1.0, E[r]);
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            const double2* ib = in + o.bstride * (b0 + b);
+            double2 v = ib[j + o.ld * (o.col_off + m)];
+            if (o.reflect) {
+                const double2 u = ib[(o.nrows - 1 - j) + o.ld * (o.col_off + m)];
+                v.x += smir * u.x;
+                v.y += smir * u.y;
             }
-            if (k >= item.n) return;
-            const int j = item.j0 + k;
-            const double sc = scalbn(t.w ? t.w[j] : 1.0, E[r]);
-#pragma unroll
-            for (int b = 0; b < NB; ++b) {
-                const double2* ib = in + o.bstride * (b0 + b);
-                double2 v = ib[j + o.ld * (o.col_off + m)];
+            gp[r][b] = make_double2(v.x * sc, v.y * sc);
+            if (m > 0) {
+                double2 u = ib[j + o.ld * (o.col_off - m)];
                 if (o.reflect) {
-                    const double2 u = ib[(o.nrows - 1 - j) + o.ld * (o.col_off + m)];
-                    v.x += smir * u.x;
-                    v.y += smir * u.y;
+                    const double2 q = ib[(o.nrows - 1 - j) + o.ld * (o.col_off - m)];
+                    u.x += smir * q.x;
+                    u.y += smir * q.y;
                 }
-                gp[r][b] = make_double2(v.x * sc, v.y * sc);
-                if (m > 0) {
-                    double2 u = ib[j + o.ld * (o.col_off - m)];
-                    if (o.reflect) {
-                        const double2 q = ib[(o.nrows - 1 - j) + o.ld * (o.col_off - m)];
-                        u.x += smir * q.x;
-                        u.y += smir * q.y;
-                    }
-                    gm[r][b] = make_double2(u.x * sc * sgn, u.y * sc * sgn);
-                }
+                gm[r][b] = make_double2(u.x * sc * sgn, u.y * sc * sgn);
             }
-        };
+        }
+    };
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int k = lane + 32 * r;
+        x[r] = 0.0;
+        p1[r] = 0.0;
+        p2[r] = 0.0;
+        E[r] = 0;
+        if (k < item.n) ring_seed(t, m, item.j0 + k, sgn, x[r], p2[r], E[r]);
+        load_g(r);
+    }
+    // partial sums over this lane's rings for degree slot `slot`
+    auto stage = [&](const double (&P)[R], int slot) {
+        double part[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) part[v] = 0.0;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-            const int k = kbase + lane + 32 * r;
-            x[r] = 0.0;
-            p1[r] = 0.0;
-            p2[r] = 0.0;
-            E[r] = 0;
-            if (k < item.n) {
-                const int j = item.j0 + k;
-                x[r] = t.cos_t[j];
-                const double e0 = m == 0 ? t.log2c[0] : (double)m * t.log2sin[j] + t.log2c[m];
-                if (isfinite(e0)) {
-                    const double Es = ceil(e0);
-                    p2[r] = sgn * exp2(e0 - Es);
-                    E[r] = (int)Es;
-                }
-            }
-            load_g(r);
-        }
-        int lb = 0, lfirst = m;
-        // reduce the staged degrees [lfirst, lfirst + cnt) over the lanes and add to alm
-        auto flush = [&](int cnt) {
-            __syncwarp();
-            if (lane < cnt * NV) {
-                const int li = lane / NV, v = lane % NV;
-                double s = 0.0;
-#pragma unroll 8
-                for (int q = 0; q < 32; ++q) s += s_red[warp][lane][q];
-                const int l = lfirst + li;
-                const int b = v >> 2, comp = v & 3;
-                if (comp < 2 || m > 0) {
-                    const int64_t idx = (l - m) + (comp < 2 ? cp : cm) + albs * (b0 + b);
-                    atomicAdd(almd + 2 * idx + (comp & 1), s);
-                }
-            }
-            __syncwarp();
-        };
-        auto stage = [&](const double (&P)[R]) {
-            double part[NV];
 #pragma unroll
-            for (int v = 0; v < NV; ++v) part[v] = 0.0;
+            for (int b = 0; b < NB; ++b) {
+                part[4 * b + 0] = fma(P[r], gp[r][b].x, part[4 * b + 0]);
+                part[4 * b + 1] = fma(P[r], gp[r][b].y, part[4 * b + 1]);
+                part[4 * b + 2] = fma(P[r], gm[r][b].x, part[4 * b + 2]);
+                part[4 * b + 3] = fma(P[r], gm[r][b].y, part[4 * b + 3]);
+            }
+        }
+#pragma unroll
+        for (int v = 0; v < NV; ++v) sm.red[warp][slot * NV + v][lane] = part[v];
+    };
+    // reduce the staged degrees [lfirst, lfirst + cnt) over the lanes and write alm
+    auto flush = [&](int lfirst, int cnt) {
+        __syncwarp();
+        if (lane < cnt * NV) {
+            const int li = lane / NV, v = lane % NV;
+            double s = 0.0;
+#pragma unroll 8
+            for (int q = 0; q < 32; ++q) s += sm.red[warp][lane][q];
+            const int l = lfirst + li;
+            const int b = v >> 2, comp = v & 3;
+            if (comp < 2 || m > 0) {
+                const int64_t idx = (l - m) + (comp < 2 ? cp : cm) + albs * (b0 + b);
+                double* dst = almd + 2 * idx + (comp & 1);
+                if (sole) *dst = s;
+                else atomicAdd(dst, s);
+            }
+        }
+        __syncwarp();
+    };
+    stage(p2, 0);  // l = m
+    if (m < L) {
+        const double s23 = sqrt((double)(2 * m + 3));
+#pragma unroll
+        for (int r = 0; r < R; ++r) p1[r] = s23 * x[r] * p2[r];
+        stage(p1, 1);  // l = m + 1
+        flush(m, 2);
+        auto rec = [&](int i) {
+            const double2 ab = sm.ab[warp][i];
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-#pragma unroll
-                for (int b = 0; b < NB; ++b) {
-                    part[4 * b + 0] = fma(P[r], gp[r][b].x, part[4 * b + 0]);
-                    part[4 * b + 1] = fma(P[r], gp[r][b].y, part[4 * b + 1]);
-                    part[4 * b + 2] = fma(P[r], gm[r][b].x, part[4 * b + 2]);
-                    part[4 * b + 3] = fma(P[r], gm[r][b].y, part[4 * b + 3]);
-                }
-            }
-#pragma unroll
-            for (int v = 0; v < NV; ++v) s_red[warp][lb * NV + v][lane] = part[v];
-            if (++lb == LB) {
-                flush(LB);
-                lfirst += LB;
-                lb = 0;
+                const double p = fma(ab.x * x[r], p1[r], -(ab.y * p2[r]));
+                p2[r] = p1[r];
+                p1[r] = p;
             }
         };
-        stage(p2);  // l = m
-        if (m < L) {
+        int steps = 0;
+        for (int l0 = m + 2; l0 <= L; l0 += 32) {
+            const int nl = min(32, L - l0 + 1);
+            __syncwarp();
+            if (lane < nl) sm.ab[warp][lane] = abm[l0 + lane - m - 2];
+            __syncwarp();
+            const int nblk = nl / LB;
+            for (int blk = 0; blk < nblk; ++blk) {
 #pragma unroll
-            for (int r = 0; r < R; ++r) p1[r] = s23 * x[r] * p2[r];
-            stage(p1);  // l = m + 1
-            int steps = 0;
-            for (int l0 = m + 2; l0 <= L; l0 += 32) {
-                const int nl = min(32, L - l0 + 1);
-                __syncwarp();
-                if (lane < nl) s_ab[warp][lane] = abm[l0 + lane - m - 2];
-                __syncwarp();
-                for (int i = 0; i < nl; ++i) {
-                    const double2 ab = s_ab[warp][i];
-#pragma unroll
-                    for (int r = 0; r < R; ++r) {
-                        const double p = fma(ab.x * x[r], p1[r], -(ab.y * p2[r]));
-                        p2[r] = p1[r];
-                        p1[r] = p;
-                    }
-                    stage(p1);
-                    if (++steps == kStride && l0 + i < L) {
-                        steps = 0;
+                for (int i = 0; i < LB; ++i) {
+                    rec(blk * LB + i);
+                    stage(p1, i);
+                }
+                flush(l0 + blk * LB, LB);
+                steps += LB;
+                if (steps == kStride) {
+                    steps = 0;
+                    if (l0 + blk * LB + LB - 1 < L) {
 #pragma unroll
                         for (int r = 0; r < R; ++r) {
                             const double mx = fmax(fabs(p1[r]), fabs(p2[r]));
@@ -427,69 +491,153 @@ ring_adj_kernel(RingTables t, RingOut o, const RingItem* __restrict__ items, int
                     }
                 }
             }
+            const int rem = nl - nblk * LB;
+            if (rem > 0) {
+                for (int i = 0; i < rem; ++i) {
+                    rec(nblk * LB + i);
+                    stage(p1, i);
+                }
+                flush(l0 + nblk * LB, rem);
+            }
         }
-        if (lb > 0) flush(lb);
+    } else {
+        flush(m, 1);
     }
 }
 
-template <int R, int NB>
+template <int RMAX, int NB>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+ring_adj_kernel(RingTables t, RingOut o, const RingItem* __restrict__ items, int nitems,
+                const double2* __restrict__ in, double* __restrict__ almd, int b0, int allow_sole) {
+    __shared__ AdjSmem sm;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int it = blockIdx.x * kWarpsPerBlock + warp;
+    if (it >= nitems) return;
+    const RingItem item = items[it];
+    const bool multi = item.n > 32 * RMAX;
+    const bool sole = allow_sole && (item.flags & kItemSole) && !multi;
+    for (int base = 0; base < item.n; base += 32 * RMAX) {
+        RingItem sub = item;
+        sub.j0 = item.j0 + base;
+        sub.n = min(32 * RMAX, item.n - base);
+        const int reff = (sub.n + 31) >> 5;
+        if (RMAX >= 4 && reff >= 3) ring_adj_item<(RMAX >= 4 ? 4 : 1), NB>(t, o, sub, in, almd, b0, sole, sm, warp, lane);
+        else if (RMAX >= 2 && reff == 2) ring_adj_item<(RMAX >= 2 ? 2 : 1), NB>(t, o, sub, in, almd, b0, sole, sm, warp, lane);
+        else ring_adj_item<1, NB>(t, o, sub, in, almd, b0, sole, sm, warp, lane);
+    }
+}
+
+// zero what the adjoint does not overwrite: padding rows of every column, the orders the
+// ring set does not retain, and the orders whose items add atomically
+__global__ void alm_prepare_kernel(double2* __restrict__ alm, int L, int B,
+                                   const unsigned char* __restrict__ sole_m, int allow_sole) {
+    const int c = blockIdx.x;  // column
+    const int b = blockIdx.y;
+    const int am = (c + 1) / 2;
+    double2* col = alm + (int64_t)(L + 1) * c + (int64_t)(L + 1) * (2 * L + 1) * b;
+    const int first = (allow_sole && sole_m[am]) ? L - am + 1 : 0;
+    for (int r = first + threadIdx.x; r <= L; r += blockDim.x) col[r] = make_double2(0.0, 0.0);
+}
+
+// ---------------------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------------------
+template <int RMAX, int NB>
 static int launch_fwd(const RingTables& t, const RingOut& o, const RingItem* items, int nitems,
-                      const double2* alm, double2* out, int b0, cudaStream_t s) {
+                      const int* jlo, const int* jhi, const double2* alm, double2* out, int b0,
+                      cudaStream_t s) {
     const int grid = (nitems + kWarpsPerBlock - 1) / kWarpsPerBlock;
-    ring_fwd_kernel<R, NB><<<grid, kWarpsPerBlock * 32, 0, s>>>(t, o, items, nitems, alm, out, b0);
+    ring_fwd_kernel<RMAX, NB><<<grid, kWarpsPerBlock * 32, 0, s>>>(t, o, items, nitems, jlo, jhi,
+                                                                  alm, out, b0);
     return check_launch("ring_fwd_kernel");
 }
 
-template <int R, int NB>
+template <int RMAX, int NB>
 static int launch_adj(const RingTables& t, const RingOut& o, const RingItem* items, int nitems,
-                      const double2* in, double2* alm, int b0, cudaStream_t s) {
+                      const double2* in, double2* alm, int b0, int allow_sole, cudaStream_t s) {
     const int grid = (nitems + kWarpsPerBlock - 1) / kWarpsPerBlock;
-    ring_adj_kernel<R, NB><<<grid, kWarpsPerBlock * 32, 0, s>>>(t, o, items, nitems, in,
-                                                                 reinterpret_cast<double*>(alm), b0);
+    ring_adj_kernel<RMAX, NB><<<grid, kWarpsPerBlock * 32, 0, s>>>(
+        t, o, items, nitems, in, reinterpret_cast<double*>(alm), b0, allow_sole);
     return check_launch("ring_adj_kernel");
 }
 
-int ring_forward(const RingTables& t, const RingOut& o, const RingItem* items, int nitems, int R,
-                 const double2* alm, double2* out, int B, cudaStream_t s) {
-    if (nitems <= 0) return 0;
+int ring_forward(const RingTables& t, const RingOut& o, const RingItems& it, const double2* alm,
+                 double2* out, int B, cudaStream_t s) {
+    if (it.nitems <= 0) return 0;
     int b0 = 0;
     while (b0 < B) {
-        int rem = B - b0;
+        const int rem = B - b0;
         if (rem >= 4) {
-            PF_TRY((launch_fwd<1, 4>(t, o, items, nitems, alm, out, b0, s)));
+            PF_TRY((launch_fwd<1, 4>(t, o, it.items, it.nitems, it.jlo, it.jhi, alm, out, b0, s)));
             b0 += 4;
         } else if (rem >= 2) {
-            PF_TRY((launch_fwd<2, 2>(t, o, items, nitems, alm, out, b0, s)));
+            PF_TRY((launch_fwd<2, 2>(t, o, it.items, it.nitems, it.jlo, it.jhi, alm, out, b0, s)));
             b0 += 2;
         } else {
-            if (R >= 4) PF_TRY((launch_fwd<4, 1>(t, o, items, nitems, alm, out, b0, s)));
-            else if (R >= 2) PF_TRY((launch_fwd<2, 1>(t, o, items, nitems, alm, out, b0, s)));
-            else PF_TRY((launch_fwd<1, 1>(t, o, items, nitems, alm, out, b0, s)));
+            if (it.rmax >= 4) PF_TRY((launch_fwd<4, 1>(t, o, it.items, it.nitems, it.jlo, it.jhi, alm, out, b0, s)));
+            else PF_TRY((launch_fwd<2, 1>(t, o, it.items, it.nitems, it.jlo, it.jhi, alm, out, b0, s)));
             b0 += 1;
         }
     }
     return 0;
 }
 
-int ring_adjoint(const RingTables& t, const RingOut& o, const RingItem* items, int nitems, int R,
-                 const double2* in, double2* alm, int B, cudaStream_t s) {
-    if (nitems <= 0) return 0;
+int alm_prepare(double2* alm, int L, int B, const unsigned char* sole_m, int allow_sole,
+                cudaStream_t s) {
+    dim3 grid(2 * L + 1, B);
+    alm_prepare_kernel<<<grid, 128, 0, s>>>(alm, L, B, sole_m, allow_sole);
+    return check_launch("alm_prepare_kernel");
+}
+
+int ring_adjoint(const RingTables& t, const RingOut& o, const RingItems& it, const double2* in,
+                 double2* alm, int B, cudaStream_t s) {
+    // a single transform with the item's own tile shape stores sole orders directly; the
+    // multi-transform kernels split items into passes and always add
+    const int allow_sole = (B == 1 && it.rmax >= 2) ? 1 : 0;
+    PF_TRY(alm_prepare(alm, t.lmax, B, it.sole_m, allow_sole, s));
+    if (it.nitems <= 0) return 0;
     int b0 = 0;
     while (b0 < B) {
-        int rem = B - b0;
+        const int rem = B - b0;
         if (rem >= 4) {
-            PF_TRY((launch_adj<1, 4>(t, o, items, nitems, in, alm, b0, s)));
+            PF_TRY((launch_adj<1, 4>(t, o, it.items, it.nitems, in, alm, b0, allow_sole, s)));
             b0 += 4;
         } else if (rem >= 2) {
-            PF_TRY((launch_adj<2, 2>(t, o, items, nitems, in, alm, b0, s)));
+            PF_TRY((launch_adj<2, 2>(t, o, it.items, it.nitems, in, alm, b0, allow_sole, s)));
             b0 += 2;
         } else {
-            if (R >= 4) PF_TRY((launch_adj<4, 1>(t, o, items, nitems, in, alm, b0, s)));
-            else if (R >= 2) PF_TRY((launch_adj<2, 1>(t, o, items, nitems, in, alm, b0, s)));
-            else PF_TRY((launch_adj<1, 1>(t, o, items, nitems, in, alm, b0, s)));
+            if (it.rmax >= 4) PF_TRY((launch_adj<4, 1>(t, o, it.items, it.nitems, in, alm, b0, allow_sole, s)));
+            else PF_TRY((launch_adj<2, 1>(t, o, it.items, it.nitems, in, alm, b0, allow_sole, s)));
             b0 += 1;
         }
     }
+    return 0;
+}
+
+// item lists of one ring set: tiles of 32 * rmax rings, the order flags, the device tables
+int build_ring_items(const std::vector<int>& jlo, const std::vector<int>& jhi, int L, int mmax,
+                     int rmax, RingItemsOwner& own, cudaStream_t s) {
+    std::vector<RingItem> items = make_ring_items(jlo, jhi, L, mmax, 32 * rmax);
+    std::vector<unsigned char> sole(L + 1, 0);
+    for (const RingItem& r : items)
+        if (r.flags & kItemSole) sole[r.m] = 1;
+    PF_TRY(own.items.alloc(sizeof(RingItem) * std::max<size_t>(items.size(), 1)));
+    PF_TRY(own.sole.alloc(L + 1));
+    PF_TRY(own.jlo.alloc(sizeof(int) * (L + 1)));
+    PF_TRY(own.jhi.alloc(sizeof(int) * (L + 1)));
+    if (!items.empty())
+        PF_CUDA(cudaMemcpyAsync(own.items.p, items.data(), sizeof(RingItem) * items.size(),
+                                cudaMemcpyHostToDevice, s));
+    PF_CUDA(cudaMemcpyAsync(own.sole.p, sole.data(), L + 1, cudaMemcpyHostToDevice, s));
+    PF_CUDA(cudaMemcpyAsync(own.jlo.p, jlo.data(), sizeof(int) * (L + 1), cudaMemcpyHostToDevice, s));
+    PF_CUDA(cudaMemcpyAsync(own.jhi.p, jhi.data(), sizeof(int) * (L + 1), cudaMemcpyHostToDevice, s));
+    PF_CUDA(cudaStreamSynchronize(s));
+    own.view.items = own.items.as<RingItem>();
+    own.view.nitems = (int)items.size();
+    own.view.rmax = rmax;
+    own.view.sole_m = own.sole.as<unsigned char>();
+    own.view.jlo = own.jlo.as<int>();
+    own.view.jhi = own.jhi.as<int>();
     return 0;
 }
 
