@@ -1,0 +1,394 @@
+"""Benchmark: PartialFSHT.jl's stretched-leaf forward + exact adjoint on B200.
+
+Workload (the configuration the headline metric is quoted on): lmax = 2048, a 20-degree
+polar cap with M = round(4 (lmax theta*)^2) = 2,044,253 points (cos theta uniform on the cap,
+phi uniform, 1% of the points moved to the cap boundary), tol = 1e-8, plain FP64, ntrans = 1,
+coefficients complex N(0,1)/(l+1) in every valid sph_mode slot. One step = one forward
+apply mul!(f, plan, alm) plus one adjoint apply mul!(alm, plan', f) on inputs resident in HBM.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Multi-GPU: one process per GPU (torchrun), each GPU runs an independent replica of the
+workload (the path does not shard: replicas only); the time is the max over ranks.
+`--impl reference` times the CPU restatement of the reference's apply (the oracle port) on
+the host cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+THETA_STAR = np.deg2rad(20.0)
+
+
+def workload(lmax, seed=2048):
+    """Seeded synthetic inputs of the benchmark configuration."""
+    rng = np.random.default_rng(seed)
+    M = int(round(4 * (lmax * THETA_STAR) ** 2))
+    theta = np.arccos(1 - (1 - np.cos(THETA_STAR)) * rng.random(M))
+    phi = 2 * np.pi * rng.random(M)
+    nb = M // 100  # 1% jittered to the boundary (within 1e-9 theta* of it)
+    idx = rng.choice(M, nb, replace=False)
+    theta[idx] = THETA_STAR * (1 - 1e-9 * rng.random(nb))
+    return M, theta, phi, rng
+
+
+def rand_alm_host(lmax, rng, ntrans=1):
+    """complex N(0,1)/(l+1) in the valid modes, zero padding; Julia layout, column-major."""
+    nr, nc = lmax + 1, 2 * lmax + 1
+    a = np.zeros((ntrans, nc, nr), dtype=np.complex128)  # memory order = Julia (nr, nc, B)
+    l = np.arange(nr)
+    for c in range(nc):
+        am = (c + 1) // 2
+        n = nr - am
+        v = rng.standard_normal((ntrans, n)) + 1j * rng.standard_normal((ntrans, n))
+        a[:, c, :n] = v / (l[:n] + am + 1)
+    return a
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"pfsht_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        try:
+            os.remove(self.path)
+        except OSError:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for n, v in zip(names, r[5:9]):
+                if v.lower() in ("active", "1"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(rows),
+                "power_w_max": max((float(r[3]) for r in rows if r[3].replace(".", "").isdigit()),
+                                   default=None)}
+
+
+def dist_setup(gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def cpu_port_apply_time(lmax, tol, nthreads, napply=1):
+    """Time the CPU restatement (oracle port) of the reference apply on this host."""
+    from oracle import oracle as O
+    M, theta, phi, rng = workload(lmax)
+    alm = np.asfortranarray(rand_alm_host(lmax, rng).transpose(2, 1, 0))
+    t0 = time.perf_counter()
+    S = O.Stretch(theta, phi, lmax, tol, nufft="es")
+    build = time.perf_counter() - t0
+    g = np.asfortranarray((rng.standard_normal(M) + 1j * rng.standard_normal(M))[:, None])
+    times = []
+    for _ in range(napply):
+        t0 = time.perf_counter()
+        S.forward(alm, nthreads=nthreads)
+        S.adjoint(g, nthreads=nthreads)
+        times.append(time.perf_counter() - t0)
+    return min(times), build, M
+
+
+def run_reference(args, world, rank):
+    """--impl reference: the CPU restatement of the reference apply, all host threads."""
+    if rank != 0:
+        return 0
+    nthreads = os.cpu_count() or 1
+    from oracle import oracle as O
+    M, theta, phi, rng = workload(args.lmax)
+    alm = np.asfortranarray(rand_alm_host(args.lmax, rng).transpose(2, 1, 0))
+    S = O.Stretch(theta, phi, args.lmax, args.tol, nufft="es")
+    g = np.asfortranarray((rng.standard_normal(M) + 1j * rng.standard_normal(M))[:, None])
+    for _ in range(args.warmup):
+        S.forward(alm, nthreads=nthreads)
+        S.adjoint(g, nthreads=nthreads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        S.forward(alm, nthreads=nthreads)
+        S.adjoint(g, nthreads=nthreads)
+    T = (time.perf_counter() - t0) * 1e3
+    ms = T / args.steps
+    line = {
+        "impl": "reference", "metric": "ms per fwd+adj apply", "value": ms, "unit": "ms",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": config_dict(args, M),
+        "cpu_baseline": {"value": ms, "unit": "ms", "cores": nthreads, "kind": "port",
+                         "sample": "full workload, one fwd+adj per step (C restatement of the "
+                                   "reference's CPU apply with an ES-kernel NUFFT, OpenMP)"},
+        "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "Julia and FINUFFT are absent on this image, so the reference's own apply "
+                "cannot run; this arm times the repository's C restatement of it",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def config_dict(args, M):
+    return {"workload": f"stretched-leaf fwd+adj, lmax={args.lmax}, 20deg polar cap, M={M}, "
+                        f"tol={args.tol:g}, {args.precision}, ntrans=1",
+            "lmax": args.lmax, "npts": M, "cap_deg": 20.0, "tol": args.tol,
+            "precision": args.precision, "ntrans": 1,
+            "alm": "complex N(0,1)/(l+1) in valid sph_mode slots",
+            "points": "cos(theta) uniform on the cap, phi uniform, 1% on the boundary",
+            "l2": "3 rotating input sets, each apply's buffers larger than L2",
+            "parallelism": f"replicas x{args.gpus}"}
+
+
+def load_traffic():
+    p = os.path.join(ROOT, "profiles", "traffic_per_launch.json")
+    try:
+        return json.load(open(p))
+    except (OSError, ValueError):
+        return {}
+
+
+def stage_work(info, stage, B=1):
+    """Algorithmic work per launch of a stage: (flops, bytes)."""
+    L, M, w = info["lmax"], info["npts"], info["nufft_w"]
+    rw = info["ring_work"]
+    nth, ncols, nf1, nf2, nrows = info["nth"], info["ncols"], info["nf1"], info["nf2"], info["nrows"]
+    touched_alm = sum(2 * (L - m + 1) for m in range(info["mmax"] + 1)) * 16 * B
+    H = nth * ncols * 16 * B
+    U = nrows * nf2 * 16 * B
+    pts = M * (16 + 4)
+    if stage in ("ring_fwd", "ring_adj"):
+        return 10.0 * rw * B, touched_alm + H
+    if stage == "interp":
+        return 8.0 * M * w * w * B, U + pts + M * 16 * B
+    if stage == "spread":
+        return 8.0 * M * w * w * B, U + pts + M * 16 * B
+    return 0.0, 0.0
+
+
+def run_b200(args, world, rank, local):
+    import ctypes as C
+
+    import torch
+    from __graft_entry__ import load_package
+    pf = load_package()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    lib = pf._lib.load()
+
+    # FP64 FMA peak on this GPU (the ring pass and NUFFT roof; MEASURED_PEAKS.json has none)
+    fl = C.c_double()
+    ms = C.c_double()
+    pf._lib.check(lib.pfsht_fma_peak(1, 4000, C.byref(fl), C.byref(ms)))
+    fp64_peak = fl.value / 1e12
+
+    M, theta, phi, rng = workload(args.lmax)
+    t0 = time.perf_counter()
+    plan = pf.Plan(theta, phi, lmax=args.lmax, tol=args.tol, precision=args.precision,
+                   device=local)
+    torch.cuda.synchronize()
+    build_s = time.perf_counter() - t0
+    info = plan.info
+    nset = 3
+    alms, fins = [], []
+    for _ in range(nset):
+        ah = rand_alm_host(args.lmax, rng)
+        alms.append(torch.from_numpy(ah).to(dev).permute(2, 1, 0)[:, :, 0])
+        fh = (rng.standard_normal(M) + 1j * rng.standard_normal(M)) / np.sqrt(2)
+        fins.append(torch.from_numpy(fh).to(dev))
+    fout = pf.zeros_field(M, device=dev)
+    aout = pf.zeros_alm(args.lmax, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step(i):
+        k = i % nset
+        pf.mul(fout, plan, alms[k])
+        pf.mul(aout, plan.H, fins[k])
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    n0 = lib.pfsht_launch_count()
+    plan.profile_start(64 * (args.steps + 2))
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for i in range(args.steps):
+        step(i)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    launches = lib.pfsht_launch_count() - n0
+    stages = plan.profile_stop()
+    clk = clocks.stop()
+    T = e0.elapsed_time(e1)
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([T], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        T = float(t.item())
+        c = torch.tensor([launches], device=dev, dtype=torch.int64)
+        dist.all_reduce(c, op=dist.ReduceOp.SUM)
+        launches = int(c.item())
+
+    # end to end through the public API with pinned host buffers
+    ah = torch.from_numpy(rand_alm_host(args.lmax, rng)).pin_memory()
+    a_host = ah.numpy().transpose(2, 1, 0)[:, :, 0]
+    f_in = torch.from_numpy((rng.standard_normal(M) + 1j * rng.standard_normal(M))).pin_memory().numpy()
+    f_out = torch.zeros(M, dtype=torch.complex128).pin_memory().numpy()
+    a_out = torch.zeros(ah.shape, dtype=torch.complex128).pin_memory().numpy().transpose(2, 1, 0)[:, :, 0]
+    for _ in range(2):
+        plan.mul(f_out, a_host)
+        plan.mul_adjoint(a_out, f_in)
+    t0 = time.perf_counter()
+    ne2e = max(3, min(args.steps, 10))
+    for _ in range(ne2e):
+        plan.mul(f_out, a_host)
+        plan.mul_adjoint(a_out, f_in)
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / ne2e
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+
+    if rank != 0:
+        return 0
+
+    ms_per_step = T / args.steps
+    value = ms_per_step / world
+    # roofline of the dominant stage of our kernels
+    ours = {k: v for k, v in stages.items() if not k.startswith("fft_")}
+    dom = max(ours, key=lambda k: ours[k][0])
+    dom_ms = ours[dom][0] / ours[dom][1]
+    flops, byts = stage_work(info, dom)
+    hbm = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs", 6650.0) \
+        if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else 6650.0
+    traffic = load_traffic().get(dom)
+    if flops / (fp64_peak * 1e12) >= byts / (hbm * 1e9):
+        achieved = flops / (dom_ms * 1e-3) / 1e12
+        roof = {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                "frac": achieved / fp64_peak}
+    else:
+        achieved = byts / (dom_ms * 1e-3) / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm}
+    roof.update({"kernel": dom, "ms_per_launch": dom_ms, "traffic": traffic,
+                 "peak_source": "FP64 FMA microbenchmark pfsht_fma_peak run in this bench "
+                                "(MEASURED_PEAKS.json has no FP64 figure)"
+                 if roof["bound"] == "fp64" else "MEASURED_PEAKS.json hbm_gbs (measured)"})
+    stage_ms = {k: round(v[0] / v[1], 4) for k, v in stages.items()}
+
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        nthreads = os.cpu_count() or 1
+        t_cpu, _, _ = cpu_port_apply_time(args.lmax, args.tol, nthreads, napply=2)
+        cpu = {"value": t_cpu * 1e3, "unit": "ms", "cores": nthreads, "kind": "port",
+               "sample": "full workload (lmax 2048, M 2.04e6), best of 2 fwd+adj applies of the "
+                         "C restatement of the reference's CPU apply, OpenMP"}
+
+    alm_bytes = (args.lmax + 1) * (2 * args.lmax + 1) * 16
+    line = {
+        "metric": "ms per fwd+adj apply", "value": value, "unit": "ms", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": config_dict(args, M),
+        "ns_per_triple": ms_per_step * 1e6 / info["ring_work"],
+        "ring_work": info["ring_work"],
+        "plan_build_s": build_s,
+        "roofline": roof,
+        "stages_ms": stage_ms,
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_ms / world, "unit": "ms", "h2d_bytes_per_step": alm_bytes + M * 16,
+                "d2h_bytes_per_step": alm_bytes + M * 16,
+                "note": "host-buffer C-ABI applies (pfsht_forward_host / pfsht_adjoint_host), "
+                        "pinned memory, wall clock"},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--lmax", type=int, default=2048)
+    ap.add_argument("--tol", type=float, default=1e-8)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    if args.impl == "reference":
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        return run_reference(args, world, rank)
+    world, rank, local = dist_setup(args.gpus)
+    try:
+        return run_b200(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -140,6 +140,15 @@ pfsht_status pfsht_fma_peak(int32_t fp64, int32_t iters, double* flops_per_s, do
  * kernels are not counted). */
 int64_t pfsht_launch_count(void);
 
+/* Per-stage CUDA-event timing of a plan's applies (no reference counterpart; the reference's
+ * benchmark/calibrate.jl:68-79 times stages on the host). Between start and stop every apply
+ * records an event at each stage boundary on its stream; stop sums the durations per stage
+ * (stage_ms and stage_count sized pfsht_num_stages()). max_marks bounds the events kept. */
+pfsht_status pfsht_profile_start(pfsht_plan* plan, int32_t max_marks);
+pfsht_status pfsht_profile_stop(pfsht_plan* plan, double* stage_ms, int32_t* stage_count);
+int32_t pfsht_num_stages(void);
+const char* pfsht_stage_name(int32_t stage);
+
 /* Thread-local message of the last failing call; returns its length. */
 size_t pfsht_last_error(char* buf, size_t len);
 /* Library version string. */

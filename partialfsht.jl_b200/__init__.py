@@ -225,6 +225,19 @@ class Plan:
     def workspace_bytes(self) -> int:
         return int(_lib.load().pfsht_workspace_bytes(self._h))
 
+    def profile_start(self, max_marks: int = 4096):
+        """Start per-stage CUDA-event timing of this plan's applies."""
+        _lib.check(_lib.load().pfsht_profile_start(self._h, int(max_marks)), "profile_start")
+
+    def profile_stop(self) -> dict:
+        """Stop stage timing; returns {stage: (total_ms, launches)} for stages that ran."""
+        lib = _lib.load()
+        n = int(lib.pfsht_num_stages())
+        ms = (C.c_double * n)()
+        cnt = (C.c_int32 * n)()
+        _lib.check(lib.pfsht_profile_stop(self._h, ms, cnt), "profile_stop")
+        return {lib.pfsht_stage_name(i).decode(): (ms[i], cnt[i]) for i in range(n) if cnt[i]}
+
     def __repr__(self):
         return (f"PartialFSHT.Plan(lmax={self.lmax}, npts={self.npts}, ntrans={self.ntrans}, "
                 f"spin=0, algorithm={self.algorithm})")

@@ -116,6 +116,26 @@ int ring_adjoint(const RingTables& t, const RingOut& o, const RingItems& it, con
                  double2* alm, int B, cudaStream_t s);
 
 // ---------------------------------------------------------------------------------------
+// per-stage CUDA-event timing of applies (diagnostics; off unless a profile is active)
+// ---------------------------------------------------------------------------------------
+enum Stage {
+    kStRingFwd, kStFftThetaFwd, kStPad, kStFft1Fwd, kStRowsFwd, kStFft2Fwd, kStInterp,
+    kStSpread, kStFft2Adj, kStRowsAdj, kStFft1Adj, kStUnpad, kStFftThetaAdj, kStRingAdj,
+    kStDirect, kNumStages
+};
+struct StageClock {
+    bool on = false;
+    int cap = 0, used = 0;
+    cudaEvent_t prev = nullptr;
+    std::vector<cudaEvent_t> ev;       // cap events, reused
+    std::vector<int> stage;            // stage ending at ev[i] (-1: a start mark)
+    void begin(cudaStream_t s);
+    void mark(int st, cudaStream_t s);
+};
+inline void clock_begin(StageClock* c, cudaStream_t s) { if (c && c->on) c->begin(s); }
+inline void clock_mark(StageClock* c, int st, cudaStream_t s) { if (c && c->on) c->mark(st, s); }
+
+// ---------------------------------------------------------------------------------------
 // NUFFT stages (nufft.cu)
 // ---------------------------------------------------------------------------------------
 struct NufftGrid {
@@ -152,10 +172,10 @@ int nufft_setpts(NufftGrid& g, NufftDev& d, const double* x, const double* y, cu
 int nufft_alloc(NufftGrid& g, NufftDev& d, int B);
 // type 2 from mode columns (n1 x ncols x B, FFT order along dim 1) to values f (M x B)
 int nufft_type2(const NufftGrid& g, NufftDev& d, const double2* modes, double2* f, int B,
-                int iflag, cudaStream_t s);
+                int iflag, cudaStream_t s, StageClock* clk = nullptr);
 // type 1 from values to mode columns
 int nufft_type1(const NufftGrid& g, NufftDev& d, const double2* f, double2* modes, int B,
-                int iflag, cudaStream_t s);
+                int iflag, cudaStream_t s, StageClock* clk = nullptr);
 
 // point transform of the leaf (src/Stretch.jl:202-213) on the device
 int leaf_points(const Geom& g, bool flip, const double* theta, const double* phi, int64_t M,

@@ -48,6 +48,22 @@ int DevBuf::alloc(size_t n) {
     return 0;
 }
 
+void StageClock::begin(cudaStream_t s) {
+    if (used >= cap) return;
+    cudaEventRecord(ev[used], s);
+    stage[used] = -1;
+    prev = ev[used];
+    ++used;
+}
+
+void StageClock::mark(int st, cudaStream_t s) {
+    if (used >= cap || !prev) return;
+    cudaEventRecord(ev[used], s);
+    stage[used] = st;
+    prev = ev[used];
+    ++used;
+}
+
 NufftDev::~NufftDev() {
     if (have_f1) cufftDestroy(f1);
     if (have_f2) cufftDestroy(f2);
@@ -135,10 +151,14 @@ int minmax_device(const double* x, int64_t M, double* mn, double* mx, cudaStream
 // ---------------------------------------------------------------------------------------
 // plan-time: grid coordinates, bin keys, sort
 // ---------------------------------------------------------------------------------------
+// Bins are aligned to the kernel's first cell (origin) i0 = ceil(g - w/2) of each point:
+// bin (br, bc) holds the points with origin row in [br BR, br BR + BR) and origin column in
+// [bc BC, bc BC + BC) (columns, and rows when every row is kept, taken modulo the grid).
+// Within a bin the points are sorted by origin row, then origin column.
 __global__ void bin_keys_kernel(const double* __restrict__ x, const double* __restrict__ y,
                                 int64_t M, double s1, double s2, int row0, int row_wrap,
-                                int nf1, int nf2, int bin_rows, int bin_cols, int nbr, int nbc,
-                                double2* __restrict__ g, int* __restrict__ key,
+                                int nf1, int nf2, int nrows, int w, int bin_rows, int bin_cols,
+                                int nbr, int nbc, double2* __restrict__ g, int* __restrict__ key,
                                 int* __restrict__ idx, int* __restrict__ counts) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < M;
          i += (int64_t)gridDim.x * blockDim.x) {
@@ -152,16 +172,16 @@ __global__ void bin_keys_kernel(const double* __restrict__ x, const double* __re
         }
         g2 = dev_jl_mod(g2, (double)nf2);
         if (g2 >= nf2) g2 -= nf2;
-        int br = (int)floor(g1 / bin_rows);
-        int bc = (int)floor(g2 / bin_cols);
-        br = min(max(br, 0), nbr - 1);
-        bc = min(max(bc, 0), nbc - 1);
+        int r = (int)ceil(g1 - 0.5 * w);
+        int c = (int)ceil(g2 - 0.5 * w);
+        if (row_wrap) r = ((r % nrows) + nrows) % nrows;
+        r = min(max(r, 0), nrows - 1);
+        c = ((c % nf2) + nf2) % nf2;
+        const int br = min(r / bin_rows, nbr - 1);
+        const int bc = min(c / bin_cols, nbc - 1);
         const int k = br * nbc + bc;
-        // cell of the point inside its bin, so that a bin's points are in row-major cell order
-        const int cr = min(max((int)floor(g1) - br * bin_rows, 0), bin_rows - 1);
-        const int cc = min(max((int)floor(g2) - bc * bin_cols, 0), bin_cols - 1);
         g[i] = make_double2(g1, g2);
-        key[i] = (k * bin_rows + cr) * bin_cols + cc;
+        key[i] = (k * bin_rows + (r - br * bin_rows)) * bin_cols + (c - bc * bin_cols);
         idx[i] = (int)i;
         atomicAdd(counts + k, 1);
     }
@@ -199,7 +219,8 @@ int nufft_setpts(NufftGrid& g, NufftDev& d, const double* x, const double* y, cu
     PF_CUDA(cudaMemsetAsync(counts.p, 0, sizeof(int) * (nbins + 1), s));
     const double s1 = (double)g.nf1 / (2 * M_PI), s2 = (double)g.nf2 / (2 * M_PI);
     bin_keys_kernel<<<nblk(M, 256), 256, 0, s>>>(x, y, M, s1, s2, g.row0, g.row_wrap, g.nf1,
-                                                 g.nf2, g.bin_rows, g.bin_cols, g.nbr, g.nbc,
+                                                 g.nf2, g.nrows, g.w, g.bin_rows, g.bin_cols,
+                                                 g.nbr, g.nbc,
                                                  gg.as<double2>(), key.as<int>(), idx.as<int>(),
                                                  counts.as<int>());
     PF_TRY(check_launch("bin_keys_kernel"));
@@ -374,21 +395,48 @@ __device__ __forceinline__ int wrap(int i, int n) {
     return r < 0 ? r + n : r;
 }
 
-// bin geometry: rows [br*BR - hc, +TR) x cols [bc*BC - hc, +TC) of the kept fine grid
+// tile of a bin: the rows and columns its points' kernels reach,
+// rows [br BR, br BR + BR + W - 1) x columns [bc BC, bc BC + BC + W - 1)
 struct TileGeom {
     int tr0, tc0, TR, TC;
 };
 template <int W>
 __device__ __forceinline__ TileGeom tile_geom(int bin, int nbc, int BR, int BC) {
-    constexpr int hc = (W + 1) / 2;
     const int br = bin / nbc, bc = bin % nbc;
-    return TileGeom{br * BR - hc, bc * BC - hc, BR + W + 1, BC + W + 1};
+    return TileGeom{br * BR, bc * BC, BR + W - 1, BC + W - 1};
+}
+
+// origin cell of a point inside its bin's tile (the binning of bin_keys_kernel)
+template <int W>
+__device__ __forceinline__ void local_origin(double2 g, const TileGeom& tg, int nrows, int nf2,
+                                             int row_wrap, int& r0, int& c0, double& v1,
+                                             double& v2) {
+    const int i10 = (int)ceil(g.x - 0.5 * W);
+    const int i20 = (int)ceil(g.y - 0.5 * W);
+    v1 = ((double)i10 - g.x) + (0.5 * W - 0.5);
+    v2 = ((double)i20 - g.y) + (0.5 * W - 0.5);
+    int r = i10, c = i20;
+    if (row_wrap) r = wrap(r, nrows);
+    c = wrap(c, nf2);
+    r0 = r - tg.tr0;
+    c0 = c - tg.tc0;
+}
+
+template <int W>
+__device__ __forceinline__ double es_poly(int a, double v) {
+    constexpr int NC = EsHorner<W>::NC;
+    const double* cf = EsHorner<W>::coef();
+    double p = cf[a * NC + NC - 1];
+#pragma unroll
+    for (int q = NC - 2; q >= 0; --q) p = fma(p, v, cf[a * NC + q]);
+    return p;
 }
 
 // Type-2 interpolation: one CTA per bin copies the bin's tile of U into shared memory, then
-// each thread interpolates points of the bin from it.
+// each thread interpolates points of the bin from it. The row weights are evaluated row by
+// row inside the tap loop so only the column weights are held in registers.
 template <int W>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 5)
 interp_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
               const int* __restrict__ binstart, int nbc, int BR, int BC, int64_t M,
               const double2* __restrict__ U, int nrows, int nf2, int row_wrap, int B,
@@ -410,14 +458,19 @@ interp_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
         __syncthreads();
         for (int p = s + threadIdx.x; p < e; p += blockDim.x) {
             const double2 g = pts[p];
-            double k1[W], k2[W];
-            const int i10 = es_taps<W>(g.x, k1) - tg.tr0;
-            const int i20 = es_taps<W>(g.y, k2) - tg.tc0;
+            const int j = perm[p];
+            int r0, c0;
+            double v1, v2;
+            local_origin<W>(g, tg, nrows, nf2, row_wrap, r0, c0, v1, v2);
+            double k2[W];
+#pragma unroll
+            for (int c = 0; c < W; ++c) k2[c] = es_poly<W>(c, v2);
             double2 acc = make_double2(0.0, 0.0);
-            if (i10 >= 0 && i10 + W <= tg.TR && i20 >= 0 && i20 + W <= tg.TC) {
+            if (r0 >= 0 && r0 + W <= tg.TR && c0 >= 0 && c0 + W <= tg.TC) {
 #pragma unroll
                 for (int a = 0; a < W; ++a) {
-                    const double2* row = tile + (i10 + a) * tg.TC + i20;
+                    const double k1 = es_poly<W>(a, v1);
+                    const double2* row = tile + (r0 + a) * tg.TC + c0;
                     double2 sr = make_double2(0.0, 0.0);
 #pragma unroll
                     for (int c = 0; c < W; ++c) {
@@ -425,90 +478,130 @@ interp_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
                         sr.x = fma(u.x, k2[c], sr.x);
                         sr.y = fma(u.y, k2[c], sr.y);
                     }
-                    acc.x = fma(sr.x, k1[a], acc.x);
-                    acc.y = fma(sr.y, k1[a], acc.y);
+                    acc.x = fma(sr.x, k1, acc.x);
+                    acc.y = fma(sr.y, k1, acc.y);
                 }
             }
-            f[perm[p] + M * b] = acc;
+            f[j + M * b] = acc;
         }
         __syncthreads();
     }
 }
 
-// Type-1 spreading: one warp per bin accumulates the bin's points into a tile of its own
-// in shared memory (no atomics), thread per point, then adds the tile to U. Lanes of one
-// round have distinct first rows, and the warp synchronises after every kernel row, so two
-// lanes never update one cell in the same row step.
+// Type-1 spreading, output stationary: one warp per bin, lane l owns tile column l (the
+// tile is BC + W - 1 = 32 columns wide) and keeps in registers the W rows a point's kernel
+// can reach. The bin's points arrive sorted by origin row, so when the origin row advances
+// the rows left behind are complete: each is added to U exactly once (atomically, since
+// neighbouring bins' tiles overlap it). Per batch of 32 points each lane evaluates one
+// point's 2W tap weights into a per-warp staging area; the points are then applied one by
+// one from it (broadcast reads), with no shared-memory read-modify-write.
+template <int W>
+struct SpreadStage {
+    static constexpr int KP = (W + 1) / 2;  // row weights as pairs
+    double2 k1[32][KP];        // row weights (pairs; the odd tail padded with 0)
+    double k2[32][W + 1];      // column weights
+    double2 v[32];             // point value
+    int org[32][2];            // origin row and column inside the tile (row < 0: skip)
+};
+
 template <int W>
 __global__ void __launch_bounds__(128)
 spread_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
               const int* __restrict__ binstart, int nbins, int nbc, int BR, int BC, int64_t M,
               const double2* __restrict__ fin, int b, int nrows, int nf2, int row_wrap,
               double2* __restrict__ U) {
-    extern __shared__ double2 smem[];
+    __shared__ SpreadStage<W> stg[4];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int bin = blockIdx.x * (blockDim.x >> 5) + warp;
+    const int bin = blockIdx.x * 4 + warp;
     if (bin >= nbins) return;
     const int s = binstart[bin], e = binstart[bin + 1];
     if (s == e) return;
     const TileGeom tg = tile_geom<W>(bin, nbc, BR, BC);
-    double2* tile = smem + warp * tg.TR * tg.TC;
-    for (int t = lane; t < tg.TR * tg.TC; t += 32) tile[t] = make_double2(0.0, 0.0);
-    __syncwarp();
-    const int n = e - s;
-    const int nb = (n + 31) >> 5;
-    for (int bt = 0; bt < nb; ++bt) {
-        // interleave: lane l takes sorted position l*nb + bt, so one batch spans the bin
-        const int pos = lane * nb + bt;
-        const bool act = pos < n;
-        const unsigned amask = __ballot_sync(0xffffffffu, act);
-        if (!act) continue;
-        const int p = s + pos;
-        const double2 g = pts[p];
-        const double2 v = fin[perm[p] + M * b];
-        double k1[W], k2[W];
-        const int i10 = es_taps<W>(g.x, k1) - tg.tr0;
-        const int i20 = es_taps<W>(g.y, k2) - tg.tc0;
-        const bool inside = i10 >= 0 && i10 + W <= tg.TR && i20 >= 0 && i20 + W <= tg.TC;
-        const unsigned peers = __match_any_sync(amask, i10);
-        const int rank = __popc(peers & ((1u << lane) - 1u));
-        const int nround = __reduce_max_sync(amask, (unsigned)__popc(peers));
-        for (int rd = 0; rd < nround; ++rd) {
-            const bool mine = rank == rd && inside;
+    SpreadStage<W>& st = stg[warp];
+    double2* ub = U + (int64_t)nrows * nf2 * b;
+    const bool col_ok = lane < tg.TC;
+    const int gcol = wrap(tg.tc0 + lane, nf2);
+    double2 acc[W];
 #pragma unroll
-            for (int a = 0; a < W; ++a) {
-                if (mine) {
-                    double2* row = tile + (i10 + a) * tg.TC + i20;
-                    const double vx = v.x * k1[a], vy = v.y * k1[a];
+    for (int a = 0; a < W; ++a) acc[a] = make_double2(0.0, 0.0);
+    int rbase = -1;
+    // add tile row r (a local row) held in acc[a] to U
+    auto flush = [&](int r, const double2& v) {
+        int gr = tg.tr0 + r;
+        if (row_wrap) gr = wrap(gr, nrows);
+        if (col_ok && gr >= 0 && gr < nrows && (v.x != 0.0 || v.y != 0.0)) {
+            double* qd = reinterpret_cast<double*>(ub + (int64_t)gr * nf2 + gcol);
+            atomicAdd(qd, v.x);
+            atomicAdd(qd + 1, v.y);
+        }
+    };
+    for (int base = s; base < e; base += 32) {
+        const int nb = min(32, e - base);
+        __syncwarp();
+        if (lane < nb) {
+            const double2 g = pts[base + lane];
+            const double2 v = fin[perm[base + lane] + M * b];
+            int r0, c0;
+            double v1, v2;
+            local_origin<W>(g, tg, nrows, nf2, row_wrap, r0, c0, v1, v2);
 #pragma unroll
-                    for (int c = 0; c < W; ++c) {
-                        double2 u = row[c];
-                        u.x = fma(vx, k2[c], u.x);
-                        u.y = fma(vy, k2[c], u.y);
-                        row[c] = u;
-                    }
+            for (int q = 0; q < SpreadStage<W>::KP; ++q)
+                st.k1[lane][q] = make_double2(es_poly<W>(2 * q, v1),
+                                              2 * q + 1 < W ? es_poly<W>(2 * q + 1, v1) : 0.0);
+#pragma unroll
+            for (int q = 0; q < W; ++q) st.k2[lane][q] = es_poly<W>(q, v2);
+            st.v[lane] = v;
+            const bool inside = r0 >= 0 && r0 + W <= tg.TR && c0 >= 0 && c0 + W <= tg.TC;
+            st.org[lane][0] = inside ? r0 : -1;
+            st.org[lane][1] = c0;
+        }
+        __syncwarp();
+        for (int q = 0; q < nb; ++q) {
+            const int r0 = st.org[q][0], c0 = st.org[q][1];
+            if (r0 < 0) continue;  // outside its bin's tile: cannot happen for binned points
+            if (rbase < 0) rbase = r0;
+            int d = r0 - rbase;
+            if (d >= W) {
+#pragma unroll
+                for (int a = 0; a < W; ++a) {
+                    flush(rbase + a, acc[a]);
+                    acc[a] = make_double2(0.0, 0.0);
                 }
-                __syncwarp(amask);
+                rbase = r0;
+                d = 0;
+            }
+            for (; d > 0; --d) {
+                flush(rbase, acc[0]);
+#pragma unroll
+                for (int a = 0; a < W - 1; ++a) acc[a] = acc[a + 1];
+                acc[W - 1] = make_double2(0.0, 0.0);
+                ++rbase;
+            }
+            const unsigned dc = (unsigned)(lane - c0);
+            const double k2 = dc < (unsigned)W ? st.k2[q][dc] : 0.0;
+            const double2 v = st.v[q];
+            const double vx = v.x * k2, vy = v.y * k2;
+#pragma unroll
+            for (int a2 = 0; a2 < SpreadStage<W>::KP; ++a2) {
+                const double2 kk = st.k1[q][a2];
+                acc[2 * a2].x = fma(vx, kk.x, acc[2 * a2].x);
+                acc[2 * a2].y = fma(vy, kk.x, acc[2 * a2].y);
+                if (2 * a2 + 1 < W) {
+                    acc[2 * a2 + 1].x = fma(vx, kk.y, acc[2 * a2 + 1].x);
+                    acc[2 * a2 + 1].y = fma(vy, kk.y, acc[2 * a2 + 1].y);
+                }
             }
         }
     }
-    __syncwarp();
-    double2* ub = U + (int64_t)nrows * nf2 * b;
-    for (int t = lane; t < tg.TR * tg.TC; t += 32) {
-        const double2 val = tile[t];
-        if (val.x == 0.0 && val.y == 0.0) continue;
-        int r = tg.tr0 + t / tg.TC;
-        if (row_wrap) r = wrap(r, nrows);
-        if (r < 0 || r >= nrows) continue;
-        double* q = reinterpret_cast<double*>(ub + (int64_t)r * nf2 + wrap(tg.tc0 + t % tg.TC, nf2));
-        atomicAdd(q, val.x);
-        atomicAdd(q + 1, val.y);
+    if (rbase >= 0) {
+#pragma unroll
+        for (int a = 0; a < W; ++a) flush(rbase + a, acc[a]);
     }
 }
 
 template <int W>
 static int launch_interp(const NufftGrid& g, NufftDev& d, double2* f, int B, cudaStream_t s) {
-    const size_t smem = sizeof(double2) * (g.bin_rows + W + 1) * (g.bin_cols + W + 1);
+    const size_t smem = sizeof(double2) * (g.bin_rows + W - 1) * (g.bin_cols + W - 1);
     if (smem > 48 * 1024)
         PF_CUDA(cudaFuncSetAttribute(interp_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     interp_kernel<W><<<g.nbr * g.nbc, 128, smem, s>>>(
@@ -519,13 +612,9 @@ static int launch_interp(const NufftGrid& g, NufftDev& d, double2* f, int B, cud
 
 template <int W>
 static int launch_spread(const NufftGrid& g, NufftDev& d, const double2* f, int B, cudaStream_t s) {
-    constexpr int kWarps = 4;
-    const size_t smem = kWarps * sizeof(double2) * (g.bin_rows + W + 1) * (g.bin_cols + W + 1);
-    if (smem > 48 * 1024)
-        PF_CUDA(cudaFuncSetAttribute(spread_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int nbins = g.nbr * g.nbc;
     for (int b = 0; b < B; ++b) {
-        spread_kernel<W><<<(nbins + kWarps - 1) / kWarps, 32 * kWarps, smem, s>>>(
+        spread_kernel<W><<<(nbins + 3) / 4, 128, 0, s>>>(
             d.pts.as<double2>(), d.perm.as<int>(), d.binstart.as<int>(), nbins, g.nbc,
             g.bin_rows, g.bin_cols, g.M, f, b, g.nrows, g.nf2, g.row_wrap, d.U.as<double2>());
         PF_TRY(check_launch("spread_kernel"));
@@ -560,7 +649,7 @@ static int spread_any(const NufftGrid& g, NufftDev& d, const double2* f, int B, 
 }
 
 int nufft_type2(const NufftGrid& g, NufftDev& d, const double2* modes, double2* f, int B,
-                int iflag, cudaStream_t s) {
+                int iflag, cudaStream_t s, StageClock* clk) {
     const int dir = iflag > 0 ? CUFFT_INVERSE : CUFFT_FORWARD;
     {
         dim3 grid(nblk(g.nf1, 256), g.ncols, B);
@@ -568,8 +657,10 @@ int nufft_type2(const NufftGrid& g, NufftDev& d, const double2* modes, double2* 
                                         d.dec2.as<double>(), d.pad.as<double2>());
         PF_TRY(check_launch("pad_kernel"));
     }
+    clock_mark(clk, kStPad, s);
     PF_CUFFT(cufftSetStream(d.f1, s));
     PF_CUFFT(cufftExecZ2Z(d.f1, d.pad.as<cufftDoubleComplex>(), d.pad.as<cufftDoubleComplex>(), dir));
+    clock_mark(clk, kStFft1Fwd, s);
     {
         dim3 grid((g.nf2 + 31) / 32, (g.nrows + 31) / 32, B);
         rows_fwd_kernel<<<grid, dim3(32, 8), 0, s>>>(d.pad.as<double2>(), g.nf1, g.ncols, g.row0,
@@ -577,18 +668,24 @@ int nufft_type2(const NufftGrid& g, NufftDev& d, const double2* modes, double2* 
                                                      d.U.as<double2>());
         PF_TRY(check_launch("rows_fwd_kernel"));
     }
+    clock_mark(clk, kStRowsFwd, s);
     PF_CUFFT(cufftSetStream(d.f2, s));
     PF_CUFFT(cufftExecZ2Z(d.f2, d.U.as<cufftDoubleComplex>(), d.U.as<cufftDoubleComplex>(), dir));
-    return interp_any(g, d, f, B, s);
+    clock_mark(clk, kStFft2Fwd, s);
+    PF_TRY(interp_any(g, d, f, B, s));
+    clock_mark(clk, kStInterp, s);
+    return 0;
 }
 
 int nufft_type1(const NufftGrid& g, NufftDev& d, const double2* f, double2* modes, int B,
-                int iflag, cudaStream_t s) {
+                int iflag, cudaStream_t s, StageClock* clk) {
     const int dir = iflag > 0 ? CUFFT_INVERSE : CUFFT_FORWARD;
     PF_CUDA(cudaMemsetAsync(d.U.p, 0, sizeof(double2) * (size_t)g.nrows * g.nf2 * B, s));
     PF_TRY(spread_any(g, d, f, B, s));
+    clock_mark(clk, kStSpread, s);
     PF_CUFFT(cufftSetStream(d.f2, s));
     PF_CUFFT(cufftExecZ2Z(d.f2, d.U.as<cufftDoubleComplex>(), d.U.as<cufftDoubleComplex>(), dir));
+    clock_mark(clk, kStFft2Adj, s);
     {
         dim3 grid((g.ncols + 31) / 32, (g.nf1 + 31) / 32, B);
         rows_adj_kernel<<<grid, dim3(32, 8), 0, s>>>(d.U.as<double2>(), g.nf1, g.ncols, g.row0,
@@ -596,14 +693,17 @@ int nufft_type1(const NufftGrid& g, NufftDev& d, const double2* f, double2* mode
                                                      d.pad.as<double2>());
         PF_TRY(check_launch("rows_adj_kernel"));
     }
+    clock_mark(clk, kStRowsAdj, s);
     PF_CUFFT(cufftSetStream(d.f1, s));
     PF_CUFFT(cufftExecZ2Z(d.f1, d.pad.as<cufftDoubleComplex>(), d.pad.as<cufftDoubleComplex>(), dir));
+    clock_mark(clk, kStFft1Adj, s);
     {
         dim3 grid(nblk(g.n1, 256), g.ncols, B);
         unpad_kernel<<<grid, 256, 0, s>>>(d.pad.as<double2>(), g.n1, g.ncols, g.nf1,
                                           d.mult1.as<double2>(), d.dec2.as<double>(), modes);
         PF_TRY(check_launch("unpad_kernel"));
     }
+    clock_mark(clk, kStUnpad, s);
     return 0;
 }
 

@@ -63,9 +63,11 @@ struct pfsht_plan {
     DevBuf st_alm, st_f;
     cudaStream_t st_stream = nullptr;
     pfsht_plan_info info{};
+    StageClock clk;
     ~pfsht_plan() {
         if (have_fth) cufftDestroy(fth);
         if (st_stream) cudaStreamDestroy(st_stream);
+        for (cudaEvent_t e : clk.ev) cudaEventDestroy(e);
     }
 };
 
@@ -117,8 +119,10 @@ int setup_nufft_grid(NufftGrid& g, NufftDev& d, int n1, int nmodes2, const std::
     g.n1 = n1;
     g.ncols = (int)colk2.size();
     g.M = M;
-    g.bin_rows = bin_rows > 0 ? bin_rows : 32;
-    g.bin_cols = bin_cols > 0 ? bin_cols : 8;
+    g.bin_rows = bin_rows > 0 ? bin_rows : 12;
+    // the spreading tile (bin width + w - 1 columns) is one warp wide
+    g.bin_cols = 33 - g.w;
+    if (bin_cols > 0 && bin_cols < g.bin_cols) g.bin_cols = bin_cols;
     if (full_rows) {
         g.row0 = 0;
         g.nrows = g.nf1;
@@ -416,28 +420,38 @@ int plan_create(const double* theta, const double* phi, int64_t npts, int lmax, 
 
 int apply_forward(pfsht_plan* p, const double2* alm, double2* f, cudaStream_t s) {
     const int B = p->B;
-    PF_TRY(ring_forward(p->rt, p->ro_cols, p->fwd_items.view, alm,
-                        p->H.as<double2>(), B, s));
-    if (p->kind == kDirect)
-        return direct_phase_sum(p->H.as<double2>(), p->phi_pts.as<double>(), p->M, p->L, B, f, s);
+    StageClock* clk = &p->clk;
+    clock_begin(clk, s);
+    PF_TRY(ring_forward(p->rt, p->ro_cols, p->fwd_items.view, alm, p->H.as<double2>(), B, s));
+    if (p->kind == kDirect) {
+        PF_TRY(direct_phase_sum(p->H.as<double2>(), p->phi_pts.as<double>(), p->M, p->L, B, f, s));
+        clock_mark(clk, kStDirect, s);
+        return 0;
+    }
+    clock_mark(clk, kStRingFwd, s);
     PF_CUFFT(cufftSetStream(p->fth, s));
     PF_CUFFT(cufftExecZ2Z(p->fth, p->H.as<cufftDoubleComplex>(), p->H.as<cufftDoubleComplex>(),
                           CUFFT_FORWARD));
-    return nufft_type2(p->ng, p->nd, p->H.as<double2>(), f, B, +1, s);
+    clock_mark(clk, kStFftThetaFwd, s);
+    return nufft_type2(p->ng, p->nd, p->H.as<double2>(), f, B, +1, s, clk);
 }
 
 int apply_adjoint(pfsht_plan* p, const double2* f, double2* alm, cudaStream_t s) {
     const int B = p->B;
+    StageClock* clk = &p->clk;
+    clock_begin(clk, s);
     if (p->kind == kDirect) {
         PF_TRY(direct_phase_spread(f, p->phi_pts.as<double>(), p->M, p->L, B, p->H.as<double2>(), s));
     } else {
-        PF_TRY(nufft_type1(p->ng, p->nd, f, p->H.as<double2>(), B, -1, s));
+        PF_TRY(nufft_type1(p->ng, p->nd, f, p->H.as<double2>(), B, -1, s, clk));
         PF_CUFFT(cufftSetStream(p->fth, s));
         PF_CUFFT(cufftExecZ2Z(p->fth, p->H.as<cufftDoubleComplex>(), p->H.as<cufftDoubleComplex>(),
                               CUFFT_INVERSE));
+        clock_mark(clk, kStFftThetaAdj, s);
     }
-    return ring_adjoint(p->rt, p->ro_cols, p->adj_items.view,
-                        p->H.as<double2>(), alm, B, s);
+    PF_TRY(ring_adjoint(p->rt, p->ro_cols, p->adj_items.view, p->H.as<double2>(), alm, B, s));
+    clock_mark(clk, p->kind == kDirect ? kStDirect : kStRingAdj, s);
+    return 0;
 }
 
 }  // namespace
@@ -710,5 +724,60 @@ size_t pfsht_last_error(char* buf, size_t len) {
 const char* pfsht_version(void) { return "pfsht_b200 0.1.0 (sm_100a)"; }
 
 int64_t pfsht_launch_count(void) { return (int64_t)launch_count(); }
+
+static const char* kStageNames[kNumStages] = {
+    "ring_fwd", "fft_theta_fwd", "nufft_pad", "fft_fine1_fwd", "rows_fwd", "fft_fine2_fwd",
+    "interp", "spread", "fft_fine2_adj", "rows_adj", "fft_fine1_adj", "nufft_unpad",
+    "fft_theta_adj", "ring_adj", "direct"};
+
+int32_t pfsht_num_stages(void) { return kNumStages; }
+
+const char* pfsht_stage_name(int32_t stage) {
+    return stage >= 0 && stage < kNumStages ? kStageNames[stage] : "";
+}
+
+pfsht_status pfsht_profile_start(pfsht_plan* p, int32_t max_marks) {
+    if (!p || max_marks < 2) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "bad profile arguments");
+    DeviceGuard dg(p->device);
+    StageClock& c = p->clk;
+    while ((int)c.ev.size() < max_marks) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return (pfsht_status)fail(PFSHT_ERR_CUDA, "cudaEventCreate");
+        c.ev.push_back(e);
+    }
+    c.stage.assign(c.ev.size(), -1);
+    c.cap = (int)c.ev.size();
+    c.used = 0;
+    c.prev = nullptr;
+    c.on = true;
+    return PFSHT_OK;
+}
+
+pfsht_status pfsht_profile_stop(pfsht_plan* p, double* stage_ms, int32_t* stage_count) {
+    if (!p || !stage_ms || !stage_count) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "NULL argument");
+    DeviceGuard dg(p->device);
+    StageClock& c = p->clk;
+    for (int i = 0; i < kNumStages; ++i) {
+        stage_ms[i] = 0.0;
+        stage_count[i] = 0;
+    }
+    if (c.used > 0 && cudaEventSynchronize(c.ev[c.used - 1]) != cudaSuccess)
+        return (pfsht_status)fail(PFSHT_ERR_CUDA, "cudaEventSynchronize");
+    for (int i = 1; i < c.used; ++i) {
+        const int st = c.stage[i];
+        if (st < 0) continue;
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, c.ev[i - 1], c.ev[i]) != cudaSuccess)
+            return (pfsht_status)fail(PFSHT_ERR_CUDA, "cudaEventElapsedTime");
+        stage_ms[st] += ms;
+        stage_count[st] += 1;
+    }
+    const int overflow = c.used >= c.cap;
+    c.on = false;
+    c.used = 0;
+    c.prev = nullptr;
+    if (overflow) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "profile buffer filled; raise max_marks");
+    return PFSHT_OK;
+}
 
 }  // extern "C"
