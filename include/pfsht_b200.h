@@ -149,6 +149,19 @@ pfsht_status pfsht_profile_stop(pfsht_plan* plan, double* stage_ms, int32_t* sta
 int32_t pfsht_num_stages(void);
 const char* pfsht_stage_name(int32_t stage);
 
+/* Direct synthesis without any allocation (no counterpart in the reference): for callers
+ * that cannot allocate device memory at the call (a framework owning the device's memory
+ * through its own pool, memory reserved in advance, or calls too small to pay for a plan).
+ * Computes f_i = sum_lm a_lm Y_lm(theta_i, phi_i) (the Direct leaf, src/Direct.jl:279-305)
+ * for device arrays theta, phi (npts), alm ((lmax+1) x (2lmax+1)) and f (npts), with all
+ * intermediates in one fixed 32 MiB array the library declares in device memory; it makes no
+ * cudaMalloc, cudaFree or other allocating call. Sizes needing more (about
+ * npts (2 lmax + 1) 16 bytes) are rejected with PFSHT_ERR_ARGUMENT. The first call on a
+ * device looks up the array's address and should come before any stream capture. Calls share
+ * the array: calls that overlap on the GPU race and must be serialised by the caller. */
+pfsht_status pfsht_direct_forward_noalloc(const double* theta, const double* phi, int64_t npts,
+                                          int32_t lmax, const void* alm, void* f, void* stream);
+
 /* Thread-local message of the last failing call; returns its length. */
 size_t pfsht_last_error(char* buf, size_t len);
 /* Library version string. */

@@ -67,6 +67,7 @@ SIGNATURES = {
     "pfsht_version": (C.c_char_p, []),
     "pfsht_fma_peak": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "pfsht_launch_count": (C.c_int64, []),
+    "pfsht_direct_forward_noalloc": (C.c_int, [_vp, _vp, C.c_int64, C.c_int32, _vp, _vp, _vp]),
     "pfsht_profile_start": (C.c_int, [_vp, C.c_int32]),
     "pfsht_profile_stop": (C.c_int, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
     "pfsht_num_stages": (C.c_int32, []),

@@ -104,6 +104,7 @@ struct RingItemsOwner {
 };
 
 int build_ab_table(int lmax, int mmax, DevBuf& ab, DevBuf& aboff, cudaStream_t s);
+int launch_ab_table(int lmax, int mmax, const int64_t* aboff, double2* ab, cudaStream_t s);
 // items over the retained (m, ring) set, tiles of `tile` rings, heaviest first
 std::vector<RingItem> make_ring_items(const std::vector<int>& jlo, const std::vector<int>& jhi,
                                       int lmax, int mmax, int tile);

@@ -72,6 +72,13 @@ int build_ab_table(int L, int mmax, DevBuf& ab, DevBuf& aboff, cudaStream_t s) {
     return 0;
 }
 
+// the coefficient-table kernel on caller-provided offsets and storage (no allocation)
+int launch_ab_table(int L, int mmax, const int64_t* aboff, double2* ab, cudaStream_t s) {
+    dim3 grid((unsigned)std::min(64, (L + 255) / 256 + 1), (unsigned)(mmax + 1));
+    ab_table_kernel<<<grid, 256, 0, s>>>(L, mmax, aboff, ab);
+    return check_launch("ab_table_kernel");
+}
+
 std::vector<RingItem> make_ring_items(const std::vector<int>& jlo, const std::vector<int>& jhi,
                                       int L, int mmax, int tile) {
     std::vector<RingItem> items;
