@@ -58,7 +58,10 @@ typedef struct pfsht_opts {
     double oversample_theta;    /* src/Plan.jl:95 */
     double oversample_phi;      /* src/Plan.jl:96 */
     double eps_apo_max;         /* src/Plan.jl:97 */
-    int32_t reserved[8];
+    int32_t ring_segment_degrees; /* adjoint ring pass: split each order into degree segments of
+                                     about this length, started from recurrence states saved at
+                                     plan time (0 = auto, < 0 = never split) */
+    int32_t reserved[7];
 } pfsht_opts;
 
 typedef struct pfsht_plan pfsht_plan;

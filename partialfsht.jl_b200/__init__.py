@@ -142,12 +142,13 @@ class Plan:
     refused, src/Cost.jl:121-122), "stretch" (refusal raises RefusedGeometry) or "direct".
     ``precision`` is "fp64" (plain form) or "mixed". Points may be host arrays or CUDA
     tensors (float64). ``rings_per_lane`` / ``bin_rows`` / ``bin_cols`` are device tile
-    shapes (0 = defaults).
+    shapes (0 = defaults); ``segment_degrees`` splits the adjoint ring pass along the degree
+    axis (0 = auto, negative = never).
     """
 
     def __init__(self, theta, phi, *, lmax, tol=1e-10, ntrans=1, method="auto",
                  precision="fp64", oversample_theta=1.0, oversample_phi=1.0, eps_apo_max=1.0,
-                 device=None, rings_per_lane=0, bin_rows=0, bin_cols=0):
+                 device=None, rings_per_lane=0, bin_rows=0, bin_cols=0, segment_degrees=0):
         self._h = None
         if len(theta) != len(phi):
             raise DimensionMismatch("θ and φ must have the same length")
@@ -167,6 +168,7 @@ class Plan:
         o.ring_rings_per_lane = int(rings_per_lane)
         o.nufft_bin_rows = int(bin_rows)
         o.nufft_bin_cols = int(bin_cols)
+        o.ring_segment_degrees = int(segment_degrees)
         if _is_torch(theta):
             torch = _torch()
             th = theta.to(torch.float64).contiguous()
@@ -336,6 +338,27 @@ def ring_adjoint(plan: Plan, G, alm, stream=None):
     _lib.check(_lib.load().pfsht_ring_adjoint(plan._h, _ptr(G), _ptr(alm), _stream_of(G, stream)),
                "alm_from_rings!")
     return alm
+
+
+def dfs_double(F, Ft, spin=0, stream=None):
+    """dfs_double!(Ft, F, spin) (src/DFS.jl:13-33): CUDA tensors, F of Julia shape
+    (Nth, Nph[, B]) and Ft (2Nth, Nph[, B])."""
+    nth, nph = int(F.shape[0]), int(F.shape[1])
+    B = int(F.shape[2]) if F.dim() > 2 else 1
+    _check_array(Ft, [(2 * nth, nph, B)] + ([(2 * nth, nph)] if B == 1 else []), "Ft")
+    _lib.check(_lib.load().pfsht_dfs_double(_ptr(F), _ptr(Ft), nth, nph, B, int(spin),
+                                            _stream_of(F, stream)), "dfs_double!")
+    return Ft
+
+
+def dfs_fold(Ft, F, spin=0, stream=None):
+    """dfs_fold!(F, Ft, spin) (src/DFS.jl:35-56), the transpose of dfs_double!."""
+    nth, nph = int(F.shape[0]), int(F.shape[1])
+    B = int(F.shape[2]) if F.dim() > 2 else 1
+    _check_array(Ft, [(2 * nth, nph, B)] + ([(2 * nth, nph)] if B == 1 else []), "Ft")
+    _lib.check(_lib.load().pfsht_dfs_fold(_ptr(F), _ptr(Ft), nth, nph, B, int(spin),
+                                          _stream_of(Ft, stream)), "dfs_fold!")
+    return F
 
 
 def plan_geometry(theta, phi, *, lmax, tol=1e-10, ntrans=1, method="auto",

@@ -23,7 +23,7 @@ class Opts(C.Structure):
                 ("ring_rings_per_lane", C.c_int32), ("nufft_bin_rows", C.c_int32),
                 ("nufft_bin_cols", C.c_int32), ("oversample_theta", C.c_double),
                 ("oversample_phi", C.c_double), ("eps_apo_max", C.c_double),
-                ("reserved", C.c_int32 * 8)]
+                ("ring_segment_degrees", C.c_int32), ("reserved", C.c_int32 * 7)]
 
 
 class PlanInfo(C.Structure):

@@ -58,11 +58,19 @@ struct DevBuf {
 // ---------------------------------------------------------------------------------------
 // ring pass (ring.cu)
 // ---------------------------------------------------------------------------------------
-// One work item: order m, rings [j0, j0 + n).
+// One work item: order m, rings [j0, j0 + n), degrees [lbeg, lend]. An item that starts at
+// lbeg = m seeds its recurrence from the sectorial value; a later degree segment (lbeg > m)
+// starts from the recurrence state saved at plan time, ck_p/ck_E[ck + k] for ring j0 + k.
 enum { kItemFirst = 1, kItemSole = 2 };  // first tile of its order / only tile of its order
 struct RingItem {
     int m, j0, n, flags;
+    int lbeg, lend;
+    int ck;   // checkpoint index of ring j0 (-1: seed at l = m)
+    int pad_;
 };
+__host__ __device__ inline RingItem whole_item(int m, int j0, int n, int flags, int lmax) {
+    return RingItem{m, j0, n, flags, m, lmax, -1, 0};
+}
 
 struct RingTables {
     const double* cos_t = nullptr;    // nrings, reflection sign folded in
@@ -71,8 +79,27 @@ struct RingTables {
     const double* w = nullptr;        // nrings window, or null for 1
     const double2* ab = nullptr;      // recurrence coefficients, per m from l = m + 2
     const int64_t* aboff = nullptr;   // lmax + 1 offsets into ab
+    const double2* ck_p = nullptr;    // saved recurrence state (P_{l-1}, P_{l-2}) at segment starts
+    const int* ck_E = nullptr;        // and its block exponent
     int lmax = 0;
     int nrings = 0;
+};
+
+// Degree segments of the ring pass: order m is walked as nseg[m] pieces that start on the
+// renormalisation schedule (l = m + 2 + 64 q), so each piece can run as its own item from
+// a recurrence state saved once at plan time. Checkpoint of segment s >= 1, ring j:
+// ckbase[m] + (s - 1) * (jhi[m] - jlo[m] + 1) + (j - jlo[m]).
+struct RingSegments {
+    int seg_degrees = 0;               // target segment length (multiple of 64); 0 = none
+    std::vector<int> nseg;             // lmax + 1
+    std::vector<int> nblk;             // lmax + 1: 64-degree blocks from l = m + 2
+    std::vector<int64_t> ckbase;       // lmax + 1
+    int64_t nstates = 0;
+    DevBuf ck_p, ck_E;
+    // first degree of segment s of order m (s >= 1)
+    int seg_first(int m, int s) const {
+        return m + 2 + 64 * (int)(((int64_t)s * nblk[m]) / nseg[m]);
+    }
 };
 
 // Layout of the ring-side array: column-major (ld x ncols x B), column of order m at
@@ -105,11 +132,20 @@ struct RingItemsOwner {
 
 int build_ab_table(int lmax, int mmax, DevBuf& ab, DevBuf& aboff, cudaStream_t s);
 int launch_ab_table(int lmax, int mmax, const int64_t* aboff, double2* ab, cudaStream_t s);
-// items over the retained (m, ring) set, tiles of `tile` rings, heaviest first
+// items over the retained (m, ring) set, tiles of `tile` rings, split into the degree
+// segments of `seg` when given, heaviest first
 std::vector<RingItem> make_ring_items(const std::vector<int>& jlo, const std::vector<int>& jhi,
-                                      int lmax, int mmax, int tile);
+                                      int lmax, int mmax, int tile,
+                                      const RingSegments* seg = nullptr);
 int build_ring_items(const std::vector<int>& jlo, const std::vector<int>& jhi, int lmax, int mmax,
-                     int rmax, RingItemsOwner& own, cudaStream_t s);
+                     int rmax, RingItemsOwner& own, cudaStream_t s,
+                     const RingSegments* seg = nullptr);
+// choose the degree segments for a ring set (seg_degrees > 0: target length; 0: none) and
+// save the recurrence state at every segment start; t.ab/aboff must be built. Returns the
+// segments unused (nseg all 1) when the state would exceed max_bytes.
+int build_ring_segments(const RingTables& t, const std::vector<int>& jlo,
+                        const std::vector<int>& jhi, int lmax, int mmax, int seg_degrees,
+                        int64_t max_bytes, RingSegments& seg, cudaStream_t s);
 // launchers: B transforms, alm complex (lmax+1, 2lmax+1, B); the adjoint writes all of alm
 int ring_forward(const RingTables& t, const RingOut& o, const RingItems& it, const double2* alm,
                  double2* out, int B, cudaStream_t s);
@@ -148,6 +184,7 @@ struct NufftGrid {
     int n1 = 0;                // modes along dim 1 (FFT order)
     int ncols = 0;             // mode columns
     int bin_rows = 16, bin_cols = 16, nbr = 0, nbc = 0;
+    int nbusy = 0;             // bins holding at least one point
     int64_t M = 0;
 };
 
@@ -155,6 +192,7 @@ struct NufftDev {
     DevBuf pts;       // double2 (g1 - row0, g2) in bin order
     DevBuf perm;      // int32 original index, bin order
     DevBuf binstart;  // int32 nbins + 1
+    DevBuf binorder;  // int32 nbusy: non-empty bins, most points first
     DevBuf colp2;     // int32 ncols: fine column of each mode column
     DevBuf p2col;     // int32 nf2: mode column of each fine column or -1
     DevBuf mult1;     // double2 n1: per-mode complex factor along dim 1 (deconv incl.)

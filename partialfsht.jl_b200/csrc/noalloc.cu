@@ -111,7 +111,7 @@ __global__ void noalloc_prep_kernel(const double* __restrict__ theta, int64_t M,
         const int m = (int)(k / ntile), t = (int)(k % ntile);
         const int j0 = t * kNoAllocTile;
         const int n = (int)min((int64_t)kNoAllocTile, M - j0);
-        items[k] = RingItem{m, j0, n, (t == 0 ? kItemFirst : 0) | (ntile == 1 ? kItemSole : 0)};
+        items[k] = whole_item(m, j0, n, (t == 0 ? kItemFirst : 0) | (ntile == 1 ? kItemSole : 0), L);
     }
     for (int m = (int)tid; m <= L; m += (int)nthr) {
         int64_t off = 0;

@@ -244,7 +244,22 @@ int nufft_setpts(NufftGrid& g, NufftDev& d, const double* x, const double* y, cu
     gather_points_kernel<<<nblk(M, 256), 256, 0, s>>>(gg.as<double2>(), idx2.as<int>(), M,
                                                       d.pts.as<double2>(), d.perm.as<int>());
     PF_TRY(check_launch("gather_points_kernel"));
+    // launch order of the bins: non-empty bins, most points first, so the heavy bins start
+    // in the first wave and the tail of the grid is the light ones
+    std::vector<int> cnt(nbins);
+    PF_CUDA(cudaMemcpyAsync(cnt.data(), counts.p, sizeof(int) * nbins, cudaMemcpyDeviceToHost, s));
     // temporaries are freed when this returns, so finish using them first
+    PF_CUDA(cudaStreamSynchronize(s));
+    std::vector<int> order;
+    order.reserve(nbins);
+    for (int b = 0; b < nbins; ++b)
+        if (cnt[b] > 0) order.push_back(b);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cnt[a] > cnt[b]; });
+    g.nbusy = (int)order.size();
+    PF_TRY(d.binorder.alloc(sizeof(int) * std::max<size_t>(order.size(), 1)));
+    if (!order.empty())
+        PF_CUDA(cudaMemcpyAsync(d.binorder.p, order.data(), sizeof(int) * order.size(),
+                                cudaMemcpyHostToDevice, s));
     PF_CUDA(cudaStreamSynchronize(s));
     return 0;
 }
@@ -438,13 +453,12 @@ __device__ __forceinline__ double es_poly(int a, double v) {
 template <int W>
 __global__ void __launch_bounds__(128, 5)
 interp_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
-              const int* __restrict__ binstart, int nbc, int BR, int BC, int64_t M,
-              const double2* __restrict__ U, int nrows, int nf2, int row_wrap, int B,
-              double2* __restrict__ f) {
+              const int* __restrict__ binstart, const int* __restrict__ binorder, int nbc,
+              int BR, int BC, int64_t M, const double2* __restrict__ U, int nrows, int nf2,
+              int row_wrap, int B, double2* __restrict__ f) {
     extern __shared__ double2 tile[];
-    const int bin = blockIdx.x;
+    const int bin = binorder[blockIdx.x];
     const int s = binstart[bin], e = binstart[bin + 1];
-    if (s == e) return;
     const TileGeom tg = tile_geom<W>(bin, nbc, BR, BC);
     for (int b = 0; b < B; ++b) {
         const double2* ub = U + (int64_t)nrows * nf2 * b;
@@ -493,29 +507,34 @@ interp_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
 // can reach. The bin's points arrive sorted by origin row, so when the origin row advances
 // the rows left behind are complete: each is added to U exactly once (atomically, since
 // neighbouring bins' tiles overlap it). Per batch of 32 points each lane evaluates one
-// point's 2W tap weights into a per-warp staging area; the points are then applied one by
-// one from it (broadcast reads), with no shared-memory read-modify-write.
+// point's row weights and its value times the column weights into a per-warp staging area;
+// the points are then applied one by one from it, the next point's operands loaded while the
+// current one's W complex FMA pairs run, with no shared-memory read-modify-write.
 template <int W>
 struct SpreadStage {
     static constexpr int KP = (W + 1) / 2;  // row weights as pairs
     double2 k1[32][KP];        // row weights (pairs; the odd tail padded with 0)
-    double k2[32][W + 1];      // column weights
-    double2 v[32];             // point value
-    int org[32][2];            // origin row and column inside the tile (row < 0: skip)
+    double2 vk[32][W + 1];     // value x column weight; slot W is 0 for lanes off the point
+    int2 org[32];              // origin row (or -1: skip) and column inside the tile
 };
 
+// warps (bins) per block: the staging area of the wide kernels needs more shared memory
+template <int W> struct SpreadWarps { static constexpr int N = W > 12 ? 2 : 4; };
+
 template <int W>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(SpreadWarps<W>::N * 32)
 spread_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
-              const int* __restrict__ binstart, int nbins, int nbc, int BR, int BC, int64_t M,
-              const double2* __restrict__ fin, int b, int nrows, int nf2, int row_wrap,
-              double2* __restrict__ U) {
-    __shared__ SpreadStage<W> stg[4];
+              const int* __restrict__ binstart, const int* __restrict__ binorder, int nbusy,
+              int nbc, int BR, int BC, int64_t M, const double2* __restrict__ fin, int b,
+              int nrows, int nf2, int row_wrap, double2* __restrict__ U) {
+    constexpr int KP = SpreadStage<W>::KP;
+    constexpr int NW = SpreadWarps<W>::N;
+    __shared__ SpreadStage<W> stg[NW];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int bin = blockIdx.x * 4 + warp;
-    if (bin >= nbins) return;
+    const int slot = blockIdx.x * NW + warp;
+    if (slot >= nbusy) return;
+    const int bin = binorder[slot];
     const int s = binstart[bin], e = binstart[bin + 1];
-    if (s == e) return;
     const TileGeom tg = tile_geom<W>(bin, nbc, BR, BC);
     SpreadStage<W>& st = stg[warp];
     double2* ub = U + (int64_t)nrows * nf2 * b;
@@ -535,6 +554,10 @@ spread_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
             atomicAdd(qd + 1, v.y);
         }
     };
+    if (lane == 0) {
+#pragma unroll
+        for (int q = 0; q < 32; ++q) st.vk[q][W] = make_double2(0.0, 0.0);
+    }
     for (int base = s; base < e; base += 32) {
         const int nb = min(32, e - base);
         __syncwarp();
@@ -545,50 +568,65 @@ spread_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
             double v1, v2;
             local_origin<W>(g, tg, nrows, nf2, row_wrap, r0, c0, v1, v2);
 #pragma unroll
-            for (int q = 0; q < SpreadStage<W>::KP; ++q)
+            for (int q = 0; q < KP; ++q)
                 st.k1[lane][q] = make_double2(es_poly<W>(2 * q, v1),
                                               2 * q + 1 < W ? es_poly<W>(2 * q + 1, v1) : 0.0);
 #pragma unroll
-            for (int q = 0; q < W; ++q) st.k2[lane][q] = es_poly<W>(q, v2);
-            st.v[lane] = v;
+            for (int q = 0; q < W; ++q) {
+                const double k2 = es_poly<W>(q, v2);
+                st.vk[lane][q] = make_double2(v.x * k2, v.y * k2);
+            }
             const bool inside = r0 >= 0 && r0 + W <= tg.TR && c0 >= 0 && c0 + W <= tg.TC;
-            st.org[lane][0] = inside ? r0 : -1;
-            st.org[lane][1] = c0;
+            st.org[lane] = make_int2(inside ? r0 : -1, c0);
         }
         __syncwarp();
+        // operands of point q for this lane
+        auto fetch = [&](int q, int2& o, double2& vk, double2 (&k1)[KP]) {
+            o = st.org[q];
+            const unsigned dc = (unsigned)(lane - o.y);
+            vk = st.vk[q][dc < (unsigned)W ? dc : W];
+#pragma unroll
+            for (int a2 = 0; a2 < KP; ++a2) k1[a2] = st.k1[q][a2];
+        };
+        int2 o_n;
+        double2 vk_n, k1_n[KP];
+        fetch(0, o_n, vk_n, k1_n);
         for (int q = 0; q < nb; ++q) {
-            const int r0 = st.org[q][0], c0 = st.org[q][1];
+            const int2 o = o_n;
+            const double2 vk = vk_n;
+            double2 k1[KP];
+#pragma unroll
+            for (int a2 = 0; a2 < KP; ++a2) k1[a2] = k1_n[a2];
+            if (q + 1 < nb) fetch(q + 1, o_n, vk_n, k1_n);
+            const int r0 = o.x;
             if (r0 < 0) continue;  // outside its bin's tile: cannot happen for binned points
-            if (rbase < 0) rbase = r0;
-            int d = r0 - rbase;
-            if (d >= W) {
+            if (r0 != rbase) {
+                if (rbase < 0) rbase = r0;
+                int d = r0 - rbase;
+                if (d >= W) {
 #pragma unroll
-                for (int a = 0; a < W; ++a) {
-                    flush(rbase + a, acc[a]);
-                    acc[a] = make_double2(0.0, 0.0);
+                    for (int a = 0; a < W; ++a) {
+                        flush(rbase + a, acc[a]);
+                        acc[a] = make_double2(0.0, 0.0);
+                    }
+                    rbase = r0;
+                    d = 0;
                 }
-                rbase = r0;
-                d = 0;
-            }
-            for (; d > 0; --d) {
-                flush(rbase, acc[0]);
+                for (; d > 0; --d) {
+                    flush(rbase, acc[0]);
 #pragma unroll
-                for (int a = 0; a < W - 1; ++a) acc[a] = acc[a + 1];
-                acc[W - 1] = make_double2(0.0, 0.0);
-                ++rbase;
+                    for (int a = 0; a < W - 1; ++a) acc[a] = acc[a + 1];
+                    acc[W - 1] = make_double2(0.0, 0.0);
+                    ++rbase;
+                }
             }
-            const unsigned dc = (unsigned)(lane - c0);
-            const double k2 = dc < (unsigned)W ? st.k2[q][dc] : 0.0;
-            const double2 v = st.v[q];
-            const double vx = v.x * k2, vy = v.y * k2;
 #pragma unroll
-            for (int a2 = 0; a2 < SpreadStage<W>::KP; ++a2) {
-                const double2 kk = st.k1[q][a2];
-                acc[2 * a2].x = fma(vx, kk.x, acc[2 * a2].x);
-                acc[2 * a2].y = fma(vy, kk.x, acc[2 * a2].y);
+            for (int a2 = 0; a2 < KP; ++a2) {
+                acc[2 * a2].x = fma(vk.x, k1[a2].x, acc[2 * a2].x);
+                acc[2 * a2].y = fma(vk.y, k1[a2].x, acc[2 * a2].y);
                 if (2 * a2 + 1 < W) {
-                    acc[2 * a2 + 1].x = fma(vx, kk.y, acc[2 * a2 + 1].x);
-                    acc[2 * a2 + 1].y = fma(vy, kk.y, acc[2 * a2 + 1].y);
+                    acc[2 * a2 + 1].x = fma(vk.x, k1[a2].y, acc[2 * a2 + 1].x);
+                    acc[2 * a2 + 1].y = fma(vk.y, k1[a2].y, acc[2 * a2 + 1].y);
                 }
             }
         }
@@ -599,24 +637,164 @@ spread_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
     }
 }
 
+// Type-1 spreading for tiles at most 16 columns wide (bins of BC <= 17 - W columns): one warp
+// per bin, lane (h, c) = (lane / 16, lane % 16) owns tile column c and, of the W rows a point's
+// kernel reaches, those of parity h, RH = ceil(W / 2) of them in registers (row base_h + 2 i,
+// base_h the first row of parity h at or after the current origin row). A point of origin row
+// r0 gives lanes of parity r0 & 1 its even-offset row weights and the other half its odd ones,
+// so each lane does RH complex FMA pairs per point where the 32-column layout does W. When the
+// origin row advances past a row, the half holding it adds it to U and slides its window by
+// one register; the other half is untouched.
+template <int W>
+struct Spread16Stage {
+    static constexpr int RH = (W + 1) / 2;
+    static constexpr int RP = (RH + 1) / 2;  // row weights of one parity, as pairs
+    double2 k1[32][2][RP];     // [point][parity][pair]: even / odd offset row weights, 0-padded
+    double2 vk[32][W + 1];     // value x column weight; slot W is 0 for lanes off the point
+    int2 org[32];              // origin row (or -1: skip) and column inside the tile
+};
+
+template <int W>
+__global__ void __launch_bounds__(128)
+spread16_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
+                const int* __restrict__ binstart, const int* __restrict__ binorder, int nbusy,
+                int nbc, int BR, int BC, int64_t M, const double2* __restrict__ fin, int b,
+                int nrows, int nf2, int row_wrap, double2* __restrict__ U) {
+    constexpr int RH = Spread16Stage<W>::RH;
+    constexpr int RP = Spread16Stage<W>::RP;
+    __shared__ Spread16Stage<W> stg[4];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int h = lane >> 4, c = lane & 15;
+    const int slot = blockIdx.x * 4 + warp;
+    if (slot >= nbusy) return;
+    const int bin = binorder[slot];
+    const int s = binstart[bin], e = binstart[bin + 1];
+    const TileGeom tg = tile_geom<W>(bin, nbc, BR, BC);
+    Spread16Stage<W>& st = stg[warp];
+    double2* ub = U + (int64_t)nrows * nf2 * b;
+    const bool col_ok = c < tg.TC;
+    const int gcol = wrap(tg.tc0 + c, nf2);
+    double2 acc[RH];
+#pragma unroll
+    for (int i = 0; i < RH; ++i) acc[i] = make_double2(0.0, 0.0);
+    int rbase = -1;  // current origin row (local); this half holds rows base_h + 2 i
+    auto flush = [&](int r, const double2& v) {
+        int gr = tg.tr0 + r;
+        if (row_wrap) gr = wrap(gr, nrows);
+        if (col_ok && gr >= 0 && gr < nrows && (v.x != 0.0 || v.y != 0.0)) {
+            double* qd = reinterpret_cast<double*>(ub + (int64_t)gr * nf2 + gcol);
+            atomicAdd(qd, v.x);
+            atomicAdd(qd + 1, v.y);
+        }
+    };
+    // add every row this half holds and clear the window
+    auto flush_all = [&]() {
+        const int base_h = rbase + ((h - rbase) & 1);
+#pragma unroll
+        for (int i = 0; i < RH; ++i) {
+            flush(base_h + 2 * i, acc[i]);
+            acc[i] = make_double2(0.0, 0.0);
+        }
+    };
+    if (lane == 0) {
+#pragma unroll
+        for (int q = 0; q < 32; ++q) st.vk[q][W] = make_double2(0.0, 0.0);
+    }
+    for (int base = s; base < e; base += 32) {
+        const int nb = min(32, e - base);
+        __syncwarp();
+        if (lane < nb) {
+            const double2 g = pts[base + lane];
+            const double2 v = fin[perm[base + lane] + M * b];
+            int r0, c0;
+            double v1, v2;
+            local_origin<W>(g, tg, nrows, nf2, row_wrap, r0, c0, v1, v2);
+#pragma unroll
+            for (int par = 0; par < 2; ++par) {
+#pragma unroll
+                for (int p = 0; p < RP; ++p) {
+                    const int a0 = par + 4 * p, a1 = par + 4 * p + 2;
+                    st.k1[lane][par][p] = make_double2(a0 < W ? es_poly<W>(a0, v1) : 0.0,
+                                                       a1 < W ? es_poly<W>(a1, v1) : 0.0);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < W; ++q) {
+                const double k2 = es_poly<W>(q, v2);
+                st.vk[lane][q] = make_double2(v.x * k2, v.y * k2);
+            }
+            const bool inside = r0 >= 0 && r0 + W <= tg.TR && c0 >= 0 && c0 + W <= tg.TC;
+            st.org[lane] = make_int2(inside ? r0 : -1, c0);
+        }
+        __syncwarp();
+        for (int q = 0; q < nb; ++q) {
+            const int2 o = st.org[q];
+            const int r0 = o.x;
+            if (r0 < 0) continue;  // outside its bin's tile: cannot happen for binned points
+            if (r0 != rbase) {
+                if (rbase >= 0 && r0 - rbase >= W) flush_all();
+                if (rbase < 0 || r0 - rbase >= W) {
+                    rbase = r0;
+                } else {
+                    // rows rbase .. r0 - 1 are complete: the half of each row's parity adds it
+                    // and slides its window
+                    for (; rbase < r0; ++rbase) {
+                        if ((rbase & 1) == h) {
+                            flush(rbase, acc[0]);
+#pragma unroll
+                            for (int i = 0; i < RH - 1; ++i) acc[i] = acc[i + 1];
+                            acc[RH - 1] = make_double2(0.0, 0.0);
+                        }
+                    }
+                }
+            }
+            const unsigned dc = (unsigned)(c - o.y);
+            const double2 vk = st.vk[q][dc < (unsigned)W ? dc : W];
+            const int par = (h ^ r0) & 1;  // 0: this half holds the even-offset rows
+#pragma unroll
+            for (int p = 0; p < RP; ++p) {
+                const double2 kk = st.k1[q][par][p];
+                acc[2 * p].x = fma(vk.x, kk.x, acc[2 * p].x);
+                acc[2 * p].y = fma(vk.y, kk.x, acc[2 * p].y);
+                if (2 * p + 1 < RH) {
+                    acc[2 * p + 1].x = fma(vk.x, kk.y, acc[2 * p + 1].x);
+                    acc[2 * p + 1].y = fma(vk.y, kk.y, acc[2 * p + 1].y);
+                }
+            }
+        }
+    }
+    if (rbase >= 0) flush_all();
+}
+
 template <int W>
 static int launch_interp(const NufftGrid& g, NufftDev& d, double2* f, int B, cudaStream_t s) {
     const size_t smem = sizeof(double2) * (g.bin_rows + W - 1) * (g.bin_cols + W - 1);
     if (smem > 48 * 1024)
         PF_CUDA(cudaFuncSetAttribute(interp_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    interp_kernel<W><<<g.nbr * g.nbc, 128, smem, s>>>(
-        d.pts.as<double2>(), d.perm.as<int>(), d.binstart.as<int>(), g.nbc, g.bin_rows,
-        g.bin_cols, g.M, d.U.as<double2>(), g.nrows, g.nf2, g.row_wrap, B, f);
+    interp_kernel<W><<<g.nbusy, 128, smem, s>>>(
+        d.pts.as<double2>(), d.perm.as<int>(), d.binstart.as<int>(), d.binorder.as<int>(), g.nbc,
+        g.bin_rows, g.bin_cols, g.M, d.U.as<double2>(), g.nrows, g.nf2, g.row_wrap, B, f);
     return check_launch("interp_kernel");
 }
 
 template <int W>
 static int launch_spread(const NufftGrid& g, NufftDev& d, const double2* f, int B, cudaStream_t s) {
-    const int nbins = g.nbr * g.nbc;
+    if (W <= 10 && g.bin_cols + W - 1 <= 16) {
+        for (int b = 0; b < B; ++b) {
+            spread16_kernel<(W <= 10 ? W : 2)><<<(g.nbusy + 3) / 4, 128, 0, s>>>(
+                d.pts.as<double2>(), d.perm.as<int>(), d.binstart.as<int>(), d.binorder.as<int>(),
+                g.nbusy, g.nbc, g.bin_rows, g.bin_cols, g.M, f, b, g.nrows, g.nf2, g.row_wrap,
+                d.U.as<double2>());
+            PF_TRY(check_launch("spread16_kernel"));
+        }
+        return 0;
+    }
     for (int b = 0; b < B; ++b) {
-        spread_kernel<W><<<(nbins + 3) / 4, 128, 0, s>>>(
-            d.pts.as<double2>(), d.perm.as<int>(), d.binstart.as<int>(), nbins, g.nbc,
-            g.bin_rows, g.bin_cols, g.M, f, b, g.nrows, g.nf2, g.row_wrap, d.U.as<double2>());
+        constexpr int NW = SpreadWarps<W>::N;
+        spread_kernel<W><<<(g.nbusy + NW - 1) / NW, NW * 32, 0, s>>>(
+            d.pts.as<double2>(), d.perm.as<int>(), d.binstart.as<int>(), d.binorder.as<int>(),
+            g.nbusy, g.nbc, g.bin_rows, g.bin_cols, g.M, f, b, g.nrows, g.nf2, g.row_wrap,
+            d.U.as<double2>());
         PF_TRY(check_launch("spread_kernel"));
     }
     return 0;

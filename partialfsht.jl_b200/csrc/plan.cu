@@ -48,6 +48,8 @@ struct pfsht_plan {
     // ring pass
     DevBuf cos_t, log2sin, log2c, w, ab, aboff;
     RingItemsOwner fwd_items, adj_items;
+    RingSegments adj_seg;  // degree segments of the adjoint items
+    int seg_degrees = 0;   // requested segment length (0 = auto, < 0 = none)
     RingTables rt;
     RingOut ro_cols;  // the apply's column array H (or G for the direct leaf)
     // column array: nth x ncols x B (stretch) or M x (2L+1) x B (direct)
@@ -119,9 +121,11 @@ int setup_nufft_grid(NufftGrid& g, NufftDev& d, int n1, int nmodes2, const std::
     g.n1 = n1;
     g.ncols = (int)colk2.size();
     g.M = M;
-    g.bin_rows = bin_rows > 0 ? bin_rows : 12;
-    // the spreading tile (bin width + w - 1 columns) is one warp wide
-    g.bin_cols = 33 - g.w;
+    // the spreading tile (bin width + w - 1 columns) is half a warp wide for kernels up to
+    // 10 cells (two half-warps share its rows by parity), one warp wide beyond
+    const bool half = g.w <= 10;
+    g.bin_rows = bin_rows > 0 ? bin_rows : (half ? 24 : 12);
+    g.bin_cols = (half ? 17 : 33) - g.w;
     if (bin_cols > 0 && bin_cols < g.bin_cols) g.bin_cols = bin_cols;
     if (full_rows) {
         g.row0 = 0;
@@ -213,11 +217,36 @@ void fill_info(pfsht_plan* p) {
     }
     int64_t bytes = 0;
     for (const DevBuf* b : {&p->cos_t, &p->log2sin, &p->log2c, &p->w, &p->ab, &p->aboff, &p->fwd_items.items, &p->adj_items.items,
+                            &p->adj_seg.ck_p, &p->adj_seg.ck_E,
                             &p->H, &p->phi_pts, &p->nd.pts, &p->nd.perm, &p->nd.binstart,
                             &p->nd.colp2, &p->nd.p2col, &p->nd.mult1, &p->nd.dec2, &p->nd.pad,
                             &p->nd.U, &p->st_alm, &p->st_f})
         bytes += (int64_t)b->bytes;
     in.device_bytes = bytes;
+}
+
+// Adjoint items: tiles of 32 * R rings, each order split into degree segments of about
+// seg_degrees when the unsplit items would give fewer than ~8 warps per resident warp slot
+// (12 per SM at the adjoint's register count). The saved recurrence state is bounded by
+// 512 MiB; past that, or with seg_degrees < 0, the items stay whole.
+int build_adjoint_items(pfsht_plan* p, const std::vector<int>& jlo, const std::vector<int>& jhi,
+                        int mmax, cudaStream_t s) {
+    const int L = p->L;
+    const int rmax = p->R > 0 ? p->R : 4;
+    int seg = p->seg_degrees;
+    if (seg == 0) {
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device);
+        const size_t whole = make_ring_items(jlo, jhi, L, mmax, 32 * rmax).size();
+        seg = whole >= (size_t)sms * 12 * 8 ? -1 : 256;
+    }
+    if (seg > 0) {
+        PF_TRY(build_ring_segments(p->rt, jlo, jhi, L, mmax, seg, (int64_t)512 << 20, p->adj_seg, s));
+        p->rt.ck_p = p->adj_seg.ck_p.as<double2>();
+        p->rt.ck_E = p->adj_seg.ck_E.as<int>();
+    }
+    return build_ring_items(jlo, jhi, L, mmax, rmax, p->adj_items, s,
+                            p->adj_seg.seg_degrees > 0 ? &p->adj_seg : nullptr);
 }
 
 int build_stretch(pfsht_plan* p, const double* d_theta, const double* d_phi, const pfsht_opts& o,
@@ -231,9 +260,6 @@ int build_stretch(pfsht_plan* p, const double* d_theta, const double* d_phi, con
     PF_TRY(upload(p->log2c, lf.log2c, s));
     PF_TRY(upload(p->w, lf.w, s));
     PF_TRY(build_ab_table(L, lf.mmax, p->ab, p->aboff, s));
-    // forward tiles of 64 rings (more warps), adjoint tiles of 128 (amortises its reduction)
-    PF_TRY(build_ring_items(lf.jlo, lf.jhi, L, lf.mmax, p->R > 0 ? p->R : 2, p->fwd_items, s));
-    PF_TRY(build_ring_items(lf.jlo, lf.jhi, L, lf.mmax, p->R > 0 ? p->R : 4, p->adj_items, s));
     p->rt.cos_t = p->cos_t.as<double>();
     p->rt.log2sin = p->log2sin.as<double>();
     p->rt.log2c = p->log2c.as<double>();
@@ -242,6 +268,10 @@ int build_stretch(pfsht_plan* p, const double* d_theta, const double* d_phi, con
     p->rt.aboff = p->aboff.as<int64_t>();
     p->rt.lmax = L;
     p->rt.nrings = lf.nth_half;
+    // forward tiles of 64 rings (more warps), adjoint tiles of 128 (amortises its reduction)
+    // split along the degree axis when the tiles alone leave the GPU under-filled
+    PF_TRY(build_ring_items(lf.jlo, lf.jhi, L, lf.mmax, p->R > 0 ? p->R : 2, p->fwd_items, s));
+    PF_TRY(build_adjoint_items(p, lf.jlo, lf.jhi, lf.mmax, s));
     p->ncols = 2 * lf.mmax + 1;
     p->ro_cols.ld = lf.nth;
     p->ro_cols.bstride = (int64_t)lf.nth * p->ncols;
@@ -302,10 +332,6 @@ int build_direct(pfsht_plan* p, const double* h_theta, const double* h_phi, cuda
     PF_TRY(upload(p->log2c, l2c, s));
     PF_TRY(upload(p->phi_pts, ph, s));
     PF_TRY(build_ab_table(L, L, p->ab, p->aboff, s));
-    // eps = 0: every order on every point (src/Direct.jl:262-263)
-    std::vector<int> jlo(L + 1, 0), jhi(L + 1, (int)M - 1);
-    PF_TRY(build_ring_items(jlo, jhi, L, L, p->R > 0 ? p->R : 2, p->fwd_items, s));
-    PF_TRY(build_ring_items(jlo, jhi, L, L, p->R > 0 ? p->R : 4, p->adj_items, s));
     p->rt.cos_t = p->cos_t.as<double>();
     p->rt.log2sin = p->log2sin.as<double>();
     p->rt.log2c = p->log2c.as<double>();
@@ -314,6 +340,10 @@ int build_direct(pfsht_plan* p, const double* h_theta, const double* h_phi, cuda
     p->rt.aboff = p->aboff.as<int64_t>();
     p->rt.lmax = L;
     p->rt.nrings = (int)M;
+    // eps = 0: every order on every point (src/Direct.jl:262-263)
+    std::vector<int> jlo(L + 1, 0), jhi(L + 1, (int)M - 1);
+    PF_TRY(build_ring_items(jlo, jhi, L, L, p->R > 0 ? p->R : 2, p->fwd_items, s));
+    PF_TRY(build_adjoint_items(p, jlo, jhi, L, s));
     p->ncols = 2 * L + 1;
     p->ro_cols.ld = M;
     p->ro_cols.bstride = M * (2 * L + 1);
@@ -353,7 +383,9 @@ int plan_create(const double* theta, const double* phi, int64_t npts, int lmax, 
     p->B = ntrans;
     p->M = npts;
     p->tol = tol;
-    p->R = o.ring_rings_per_lane == 2 || o.ring_rings_per_lane == 4 ? o.ring_rings_per_lane : 0;
+    p->R = o.ring_rings_per_lane == 2 || o.ring_rings_per_lane == 4 || o.ring_rings_per_lane == 8
+               ? o.ring_rings_per_lane : 0;
+    p->seg_degrees = o.ring_segment_degrees;
     PF_CUDA(cudaStreamCreateWithFlags(&p->st_stream, cudaStreamNonBlocking));
     cudaStream_t s = p->st_stream;
 

@@ -80,21 +80,30 @@ int launch_ab_table(int L, int mmax, const int64_t* aboff, double2* ab, cudaStre
 }
 
 std::vector<RingItem> make_ring_items(const std::vector<int>& jlo, const std::vector<int>& jhi,
-                                      int L, int mmax, int tile) {
+                                      int L, int mmax, int tile, const RingSegments* seg) {
     std::vector<RingItem> items;
     std::vector<int64_t> cost;
     for (int m = 0; m <= std::min(mmax, L); ++m) {
         int lo = jlo[m], hi = jhi[m];
         if (hi < lo) continue;
         const int ntiles = (hi - lo + tile) / tile;
+        const int K = seg && seg->seg_degrees > 0 ? seg->nseg[m] : 1;
         for (int t = 0; t < ntiles; ++t) {
             const int j0 = lo + t * tile;
             const int n = std::min(tile, hi - j0 + 1);
             int flags = 0;
             if (t == 0) flags |= kItemFirst;
             if (ntiles == 1) flags |= kItemSole;
-            items.push_back(RingItem{m, j0, n, flags});
-            cost.push_back((int64_t)((n + 31) / 32) * (L - m + 1));
+            for (int s = 0; s < K; ++s) {
+                RingItem it = whole_item(m, j0, n, s == 0 ? flags : flags & ~kItemFirst, L);
+                if (s > 0) {
+                    it.lbeg = seg->seg_first(m, s);
+                    it.ck = (int)(seg->ckbase[m] + (int64_t)(s - 1) * (hi - lo + 1) + (j0 - lo));
+                }
+                if (s + 1 < K) it.lend = seg->seg_first(m, s + 1) - 1;
+                items.push_back(it);
+                cost.push_back((int64_t)((n + 31) / 32) * (it.lend - it.lbeg + 1));
+            }
         }
     }
     std::vector<size_t> idx(items.size());
@@ -131,6 +140,111 @@ __device__ __forceinline__ void ring_seed(const RingTables& t, int m, int j, dou
         p2 = sgn * exp2(e0 - Es);
         E = (int)Es;
     }
+}
+
+__device__ __forceinline__ void ring_renorm(double& p1, double& p2, int& E) {
+    const double mx = fmax(fabs(p1), fabs(p2));
+    if (mx > 0.0 && isfinite(mx)) {
+        const int s = ceil_log2(mx);
+        if (s != 0) {
+            const double f = scalbn(1.0, -s);
+            p1 *= f;
+            p2 *= f;
+            E += s;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// plan-time recurrence checkpoints: one thread per (order, ring) walks the same recurrence
+// and renormalisation schedule as the apply kernels and saves (P_{l-1}, P_{l-2}, E) at the
+// first degree l of every later segment
+// ---------------------------------------------------------------------------------------
+struct CkptJob {
+    int m, j0, n, nseg, nblk;
+    int ck;        // checkpoint index of (segment 1, ring j0)
+    int stride;    // between segments: retained rings of the order
+    int pad_;
+};
+
+__global__ void ring_ckpt_kernel(RingTables t, const CkptJob* __restrict__ jobs,
+                                 double2* __restrict__ ckp, int* __restrict__ ckE) {
+    const CkptJob jb = jobs[blockIdx.x];
+    const int k = threadIdx.x;
+    if (k >= jb.n) return;
+    const int m = jb.m, L = t.lmax, j = jb.j0 + k;
+    const double sgn = (m & 1) ? -1.0 : 1.0;
+    double x, p1, p2;
+    int E;
+    ring_seed(t, m, j, sgn, x, p2, E);
+    p1 = sqrt((double)(2 * m + 3)) * x * p2;
+    const double2* abm = t.ab + t.aboff[m];
+    int s = 1;
+    int lnext = m + 2 + 64 * (int)(((int64_t)jb.nblk) / jb.nseg);
+    int steps = 0;
+    for (int l = m + 2; l <= L; ++l) {
+        if (l == lnext) {
+            const int64_t idx = jb.ck + (int64_t)(s - 1) * jb.stride + k;
+            ckp[idx] = make_double2(p1, p2);
+            ckE[idx] = E;
+            if (++s == jb.nseg) break;
+            lnext = m + 2 + 64 * (int)(((int64_t)s * jb.nblk) / jb.nseg);
+        }
+        const double2 ab = abm[l - m - 2];
+        const double p = fma(ab.x * x, p1, -(ab.y * p2));
+        p2 = p1;
+        p1 = p;
+        if (++steps == kStride) {
+            steps = 0;
+            if (l < L) ring_renorm(p1, p2, E);
+        }
+    }
+}
+
+int build_ring_segments(const RingTables& t, const std::vector<int>& jlo,
+                        const std::vector<int>& jhi, int L, int mmax, int seg_degrees,
+                        int64_t max_bytes, RingSegments& seg, cudaStream_t s) {
+    seg.nseg.assign(L + 1, 1);
+    seg.nblk.assign(L + 1, 0);
+    seg.ckbase.assign(L + 1, 0);
+    seg.nstates = 0;
+    seg.seg_degrees = 0;
+    if (seg_degrees <= 0) return 0;
+    const int q = std::max(1, (seg_degrees + 32) / 64);
+    std::vector<CkptJob> jobs;
+    int64_t tot = 0;
+    for (int m = 0; m <= std::min(mmax, L); ++m) {
+        const int nret = jhi[m] - jlo[m] + 1;
+        const int nb = L >= m + 2 ? (L - m - 1 + 63) / 64 : 0;
+        seg.nblk[m] = nb;
+        const int K = std::max(1, std::min(nb, (nb + q / 2) / q));
+        if (nret <= 0 || K <= 1) continue;
+        seg.nseg[m] = K;
+        seg.ckbase[m] = tot;
+        for (int j0 = jlo[m]; j0 <= jhi[m]; j0 += 128)
+            jobs.push_back(CkptJob{m, j0, std::min(128, jhi[m] - j0 + 1), K, nb,
+                                   (int)(tot + (j0 - jlo[m])), nret, 0});
+        tot += (int64_t)(K - 1) * nret;
+    }
+    if (jobs.empty()) return 0;
+    if (tot * (int64_t)(sizeof(double2) + sizeof(int)) > max_bytes || tot > INT32_MAX) {
+        seg.nseg.assign(L + 1, 1);
+        return 0;
+    }
+    DevBuf djobs;
+    PF_TRY(djobs.alloc(sizeof(CkptJob) * jobs.size()));
+    PF_TRY(seg.ck_p.alloc(sizeof(double2) * tot));
+    PF_TRY(seg.ck_E.alloc(sizeof(int) * tot));
+    PF_CUDA(cudaMemcpyAsync(djobs.p, jobs.data(), sizeof(CkptJob) * jobs.size(),
+                            cudaMemcpyHostToDevice, s));
+    ring_ckpt_kernel<<<(unsigned)jobs.size(), 128, 0, s>>>(t, djobs.as<CkptJob>(),
+                                                           seg.ck_p.as<double2>(),
+                                                           seg.ck_E.as<int>());
+    PF_TRY(check_launch("ring_ckpt_kernel"));
+    PF_CUDA(cudaStreamSynchronize(s));
+    seg.nstates = tot;
+    seg.seg_degrees = seg_degrees;
+    return 0;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -344,9 +458,12 @@ ring_fwd_kernel(RingTables t, RingOut o, const RingItem* __restrict__ items, int
 // ---------------------------------------------------------------------------------------
 // adjoint: ring columns -> alm
 // ---------------------------------------------------------------------------------------
+// Two warps per block: each warp double-buffers its reduction area, so one block's partial
+// sums are reduced while the next block's degrees are computed.
+static constexpr int kAdjWarps = 2;
 struct AdjSmem {
-    double red[kWarpsPerBlock][32][33];
-    double2 ab[kWarpsPerBlock][32];
+    double red[kAdjWarps][2][32][33];
+    double2 ab[kAdjWarps][32];
 };
 
 template <int R, int NB>
@@ -400,6 +517,7 @@ __device__ __forceinline__ void ring_adj_item(const RingTables& t, const RingOut
             }
         }
     };
+    const bool seeded = item.ck < 0;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int k = lane + 32 * r;
@@ -407,9 +525,22 @@ __device__ __forceinline__ void ring_adj_item(const RingTables& t, const RingOut
         p1[r] = 0.0;
         p2[r] = 0.0;
         E[r] = 0;
-        if (k < item.n) ring_seed(t, m, item.j0 + k, sgn, x[r], p2[r], E[r]);
+        if (k < item.n) {
+            if (seeded) {
+                ring_seed(t, m, item.j0 + k, sgn, x[r], p2[r], E[r]);
+            } else {
+                x[r] = t.cos_t[item.j0 + k];
+                const double2 c = t.ck_p[item.ck + k];
+                p1[r] = c.x;
+                p2[r] = c.y;
+                E[r] = t.ck_E[item.ck + k];
+            }
+        }
         load_g(r);
     }
+    int cur = 0;     // reduction buffer the current block stages into
+    int pend = -1;   // first degree of the block waiting in buffer cur ^ 1 (-1: none)
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;  // this lane's sums of the pending block
     // partial sums over this lane's rings for degree slot `slot`
     auto stage = [&](const double (&P)[R], int slot) {
         double part[NV];
@@ -426,34 +557,68 @@ __device__ __forceinline__ void ring_adj_item(const RingTables& t, const RingOut
             }
         }
 #pragma unroll
-        for (int v = 0; v < NV; ++v) sm.red[warp][slot * NV + v][lane] = part[v];
+        for (int v = 0; v < NV; ++v) sm.red[warp][cur][slot * NV + v][lane] = part[v];
     };
-    // reduce the staged degrees [lfirst, lfirst + cnt) over the lanes and write alm
+    // lane's output (degree lfirst + lane / NV, component lane % NV) of a reduced block
+    auto write_out = [&](int lfirst, double s) {
+        const int li = lane / NV, v = lane % NV;
+        const int l = lfirst + li;
+        const int b = v >> 2, comp = v & 3;
+        if (comp < 2 || m > 0) {
+            const int64_t idx = (l - m) + (comp < 2 ? cp : cm) + albs * (b0 + b);
+            double* dst = almd + 2 * idx + (comp & 1);
+            if (sole) *dst = s;
+            else atomicAdd(dst, s);
+        }
+    };
+    // reduce the staged degrees [lfirst, lfirst + cnt) of buffer cur over the lanes at once
     auto flush = [&](int lfirst, int cnt) {
         __syncwarp();
         if (lane < cnt * NV) {
-            const int li = lane / NV, v = lane % NV;
-            double s = 0.0;
-#pragma unroll 8
-            for (int q = 0; q < 32; ++q) s += sm.red[warp][lane][q];
-            const int l = lfirst + li;
-            const int b = v >> 2, comp = v & 3;
-            if (comp < 2 || m > 0) {
-                const int64_t idx = (l - m) + (comp < 2 ? cp : cm) + albs * (b0 + b);
-                double* dst = almd + 2 * idx + (comp & 1);
-                if (sole) *dst = s;
-                else atomicAdd(dst, s);
+            // four independent partial sums: the chain of dependent adds is 8 long, not 32
+            double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+#pragma unroll
+            for (int q = 0; q < 32; q += 4) {
+                s0 += sm.red[warp][cur][lane][q];
+                s1 += sm.red[warp][cur][lane][q + 1];
+                s2 += sm.red[warp][cur][lane][q + 2];
+                s3 += sm.red[warp][cur][lane][q + 3];
             }
+            write_out(lfirst, (s0 + s1) + (s2 + s3));
         }
         __syncwarp();
     };
-    stage(p2, 0);  // l = m
-    if (m < L) {
+    // NV of the pending block's 32 values, read while degree slot i of the next block runs
+    auto drain = [&](int i) {
+#pragma unroll
+        for (int k = 0; k < NV; k += 4) {
+            const double* rowp = &sm.red[warp][cur ^ 1][lane][i * NV + k];
+            a0 += rowp[0];
+            a1 += rowp[1];
+            a2 += rowp[2];
+            a3 += rowp[3];
+        }
+    };
+    auto finish = [&]() {
+        write_out(pend, (a0 + a1) + (a2 + a3));
+        a0 = a1 = a2 = a3 = 0.0;
+        pend = -1;
+    };
+    int lstart = item.lbeg;
+    if (seeded) {
+        stage(p2, 0);  // l = m
+        if (m == L) {
+            flush(m, 1);
+            return;
+        }
         const double s23 = sqrt((double)(2 * m + 3));
 #pragma unroll
         for (int r = 0; r < R; ++r) p1[r] = s23 * x[r] * p2[r];
         stage(p1, 1);  // l = m + 1
         flush(m, 2);
+        lstart = m + 2;
+    }
+    {
         auto rec = [&](int i) {
             const double2 ab = sm.ab[warp][i];
 #pragma unroll
@@ -463,20 +628,34 @@ __device__ __forceinline__ void ring_adj_item(const RingTables& t, const RingOut
                 p1[r] = p;
             }
         };
+        // segments start on the renormalisation schedule, so the count restarts at 0
         int steps = 0;
-        for (int l0 = m + 2; l0 <= L; l0 += 32) {
-            const int nl = min(32, L - l0 + 1);
+        for (int l0 = lstart; l0 <= item.lend; l0 += 32) {
+            const int nl = min(32, item.lend - l0 + 1);
             __syncwarp();
             if (lane < nl) sm.ab[warp][lane] = abm[l0 + lane - m - 2];
             __syncwarp();
             const int nblk = nl / LB;
             for (int blk = 0; blk < nblk; ++blk) {
+                if (pend >= 0) {
 #pragma unroll
-                for (int i = 0; i < LB; ++i) {
-                    rec(blk * LB + i);
-                    stage(p1, i);
+                    for (int i = 0; i < LB; ++i) {
+                        rec(blk * LB + i);
+                        stage(p1, i);
+                        drain(i);
+                    }
+                } else {
+#pragma unroll
+                    for (int i = 0; i < LB; ++i) {
+                        rec(blk * LB + i);
+                        stage(p1, i);
+                    }
                 }
-                flush(l0 + blk * LB, LB);
+                // this block's sums are visible, and every lane is done with the other buffer
+                __syncwarp();
+                if (pend >= 0) finish();
+                pend = l0 + blk * LB;
+                cur ^= 1;
                 steps += LB;
                 if (steps == kStride) {
                     steps = 0;
@@ -490,8 +669,22 @@ __device__ __forceinline__ void ring_adj_item(const RingTables& t, const RingOut
                                     const double f = scalbn(1.0, -s);
                                     p1[r] *= f;
                                     p2[r] *= f;
+                                    const int Eold = E[r];
                                     E[r] += s;
-                                    load_g(r);
+                                    if (Eold >= -900) {
+                                        // the scaled ring data were normal: 2^s keeps them
+                                        // exactly what a reload would give
+                                        const double u = scalbn(1.0, s);
+#pragma unroll
+                                        for (int b = 0; b < NB; ++b) {
+                                            gp[r][b].x *= u;
+                                            gp[r][b].y *= u;
+                                            gm[r][b].x *= u;
+                                            gm[r][b].y *= u;
+                                        }
+                                    } else {
+                                        load_g(r);
+                                    }
                                 }
                             }
                         }
@@ -500,6 +693,11 @@ __device__ __forceinline__ void ring_adj_item(const RingTables& t, const RingOut
             }
             const int rem = nl - nblk * LB;
             if (rem > 0) {
+                if (pend >= 0) {
+#pragma unroll
+                    for (int i = 0; i < LB; ++i) drain(i);
+                    finish();
+                }
                 for (int i = 0; i < rem; ++i) {
                     rec(nblk * LB + i);
                     stage(p1, i);
@@ -507,18 +705,21 @@ __device__ __forceinline__ void ring_adj_item(const RingTables& t, const RingOut
                 flush(l0 + nblk * LB, rem);
             }
         }
-    } else {
-        flush(m, 1);
+        if (pend >= 0) {
+#pragma unroll
+            for (int i = 0; i < LB; ++i) drain(i);
+            finish();
+        }
     }
 }
 
 template <int RMAX, int NB>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+__global__ void __launch_bounds__(kAdjWarps * 32)
 ring_adj_kernel(RingTables t, RingOut o, const RingItem* __restrict__ items, int nitems,
                 const double2* __restrict__ in, double* __restrict__ almd, int b0, int allow_sole) {
     __shared__ AdjSmem sm;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int it = blockIdx.x * kWarpsPerBlock + warp;
+    const int it = blockIdx.x * kAdjWarps + warp;
     if (it >= nitems) return;
     const RingItem item = items[it];
     const bool multi = item.n > 32 * RMAX;
@@ -527,8 +728,10 @@ ring_adj_kernel(RingTables t, RingOut o, const RingItem* __restrict__ items, int
         RingItem sub = item;
         sub.j0 = item.j0 + base;
         sub.n = min(32 * RMAX, item.n - base);
+        if (sub.ck >= 0) sub.ck += base;
         const int reff = (sub.n + 31) >> 5;
-        if (RMAX >= 4 && reff >= 3) ring_adj_item<(RMAX >= 4 ? 4 : 1), NB>(t, o, sub, in, almd, b0, sole, sm, warp, lane);
+        if (RMAX >= 8 && reff >= 5) ring_adj_item<(RMAX >= 8 ? 8 : 1), NB>(t, o, sub, in, almd, b0, sole, sm, warp, lane);
+        else if (RMAX >= 4 && reff >= 3) ring_adj_item<(RMAX >= 4 ? 4 : 1), NB>(t, o, sub, in, almd, b0, sole, sm, warp, lane);
         else if (RMAX >= 2 && reff == 2) ring_adj_item<(RMAX >= 2 ? 2 : 1), NB>(t, o, sub, in, almd, b0, sole, sm, warp, lane);
         else ring_adj_item<1, NB>(t, o, sub, in, almd, b0, sole, sm, warp, lane);
     }
@@ -562,8 +765,8 @@ static int launch_fwd(const RingTables& t, const RingOut& o, const RingItem* ite
 template <int RMAX, int NB>
 static int launch_adj(const RingTables& t, const RingOut& o, const RingItem* items, int nitems,
                       const double2* in, double2* alm, int b0, int allow_sole, cudaStream_t s) {
-    const int grid = (nitems + kWarpsPerBlock - 1) / kWarpsPerBlock;
-    ring_adj_kernel<RMAX, NB><<<grid, kWarpsPerBlock * 32, 0, s>>>(
+    const int grid = (nitems + kAdjWarps - 1) / kAdjWarps;
+    ring_adj_kernel<RMAX, NB><<<grid, kAdjWarps * 32, 0, s>>>(
         t, o, items, nitems, in, reinterpret_cast<double*>(alm), b0, allow_sole);
     return check_launch("ring_adj_kernel");
 }
@@ -613,7 +816,8 @@ int ring_adjoint(const RingTables& t, const RingOut& o, const RingItems& it, con
             PF_TRY((launch_adj<2, 2>(t, o, it.items, it.nitems, in, alm, b0, allow_sole, s)));
             b0 += 2;
         } else {
-            if (it.rmax >= 4) PF_TRY((launch_adj<4, 1>(t, o, it.items, it.nitems, in, alm, b0, allow_sole, s)));
+            if (it.rmax >= 8) PF_TRY((launch_adj<8, 1>(t, o, it.items, it.nitems, in, alm, b0, allow_sole, s)));
+            else if (it.rmax >= 4) PF_TRY((launch_adj<4, 1>(t, o, it.items, it.nitems, in, alm, b0, allow_sole, s)));
             else PF_TRY((launch_adj<2, 1>(t, o, it.items, it.nitems, in, alm, b0, allow_sole, s)));
             b0 += 1;
         }
@@ -623,8 +827,8 @@ int ring_adjoint(const RingTables& t, const RingOut& o, const RingItems& it, con
 
 // item lists of one ring set: tiles of 32 * rmax rings, the order flags, the device tables
 int build_ring_items(const std::vector<int>& jlo, const std::vector<int>& jhi, int L, int mmax,
-                     int rmax, RingItemsOwner& own, cudaStream_t s) {
-    std::vector<RingItem> items = make_ring_items(jlo, jhi, L, mmax, 32 * rmax);
+                     int rmax, RingItemsOwner& own, cudaStream_t s, const RingSegments* seg) {
+    std::vector<RingItem> items = make_ring_items(jlo, jhi, L, mmax, 32 * rmax, seg);
     std::vector<unsigned char> sole(L + 1, 0);
     for (const RingItem& r : items)
         if (r.flags & kItemSole) sole[r.m] = 1;

@@ -1,0 +1,281 @@
+"""Device applies against the direct sum, on the reference's own transform test cases
+(test/test_transforms.jl), plus the lower seams (NUFFT, DFS), the host-buffer entry points,
+batching, determinism and the degree-split adjoint ring pass."""
+import numpy as np
+import pytest
+
+from helpers import cap_points, cn, dot_rel, rel, to_dev, to_host
+
+pytestmark = pytest.mark.gpu
+
+THETA_STAR = np.deg2rad(20.0)
+
+
+def _sqrt_cap(rng, n):
+    # test/test_transforms.jl:67-68: theta* sqrt(u), phi uniform
+    return THETA_STAR * np.sqrt(rng.random(n)), 2 * np.pi * rng.random(n)
+
+
+def _randn_alm(O, L, rng, B=1):
+    # randn(ComplexF64, coeff_size(L)...) with the padding slots cleared
+    return O.rand_alm(L, ntrans=B, rng=rng)
+
+
+def _fwd(plan, alm):
+    return to_host(plan * to_dev(alm if alm.shape[2] > 1 else alm[:, :, 0]))
+
+
+def _adj(plan, g):
+    return to_host(plan.H * to_dev(g))
+
+
+@pytest.mark.parametrize("L", [128, 256, 512])
+@pytest.mark.parametrize("tol", [1e-4, 1e-8])
+def test_stretch_vs_direct_across_degree_and_tolerance(pf, O, cuda, L, tol):
+    # test/test_transforms.jl:59-83: delivered accuracy at or better than the tolerance
+    rng = np.random.default_rng(32 + L)
+    th, ph = _sqrt_cap(rng, 150)
+    ps = pf.Plan(th, ph, lmax=L, tol=tol, method="stretch")
+    pd = pf.Plan(th, ph, lmax=L, method="direct")
+    alm = _randn_alm(O, L, rng)
+    fd_ref = O.Direct(th, ph, L).forward(alm, nthreads=8)[:, 0]
+    fd = _fwd(pd, alm)
+    fs = _fwd(ps, alm)
+    assert rel(fd, fd_ref) < 1e-12
+    assert rel(fs, fd_ref) < 10 * tol
+    assert ps.info["nph"] % 2 == 0
+
+
+def test_worst_case_spectra(pf, O, cuda):
+    # test/test_transforms.jl:85-110: a single l = lmax row, and a red spectrum
+    rng = np.random.default_rng(33)
+    L, tol = 256, 1e-8
+    th, ph = _sqrt_cap(rng, 200)
+    ps = pf.Plan(th, ph, lmax=L, tol=tol, method="stretch")
+    ref = O.Direct(th, ph, L)
+    alm = O.zeros_alm(L)
+    for m in range(-L, L + 1):
+        alm[O.sph_mode(L, m) + (0,)] = rng.standard_normal() + 1j * rng.standard_normal()
+    assert rel(_fwd(ps, alm), ref.forward(alm)[:, 0]) < 10 * tol
+    almr = O.rand_alm(L, rng=rng, weight=lambda l: 1.0 / (1 + l) ** 2)
+    assert rel(_fwd(ps, almr), ref.forward(almr)[:, 0]) < 10 * tol
+
+
+@pytest.mark.parametrize("L", [256, 512])
+def test_adjoint_is_exact_transpose(pf, O, cuda, L):
+    # test/test_transforms.jl:112-123
+    rng = np.random.default_rng(34)
+    th, ph = _sqrt_cap(rng, 120)
+    ps = pf.Plan(th, ph, lmax=L, tol=1e-8, method="stretch")
+    alm = _randn_alm(O, L, rng)
+    g = cn(rng, 120)
+    assert dot_rel(_fwd(ps, alm), g, alm[:, :, 0], _adj(ps, g)) < 1e-12
+
+
+@pytest.mark.parametrize("centre", [0.9, np.pi - 0.3])
+def test_off_pole_and_southern_patches(pf, O, cuda, centre):
+    # test/test_transforms.jl:125-140
+    rng = np.random.default_rng(35)
+    L, tol = 256, 1e-8
+    th = centre + 0.12 * (2 * rng.random(150) - 1)
+    ph = 1.0 + 0.4 * rng.random(150)
+    ps = pf.Plan(th, ph, lmax=L, tol=tol, method="stretch")
+    if centre > np.pi / 2:
+        assert ps.info["flip"] == 1
+    alm = _randn_alm(O, L, rng)
+    f = _fwd(ps, alm)
+    assert rel(f, O.Direct(th, ph, L).forward(alm)[:, 0]) < 10 * tol
+    g = cn(rng, 150)
+    assert dot_rel(f, g, alm[:, :, 0], _adj(ps, g)) < 1e-12
+    # and the device apply agrees with the oracle's own stretched leaf at round-off
+    so = O.Stretch(th, ph, L, tol, nufft="es")
+    assert rel(f, so.forward(alm)[:, 0]) < 1e-11
+    assert O.alm_reldiff(_adj(ps, g), so.adjoint(g)[:, :, 0], L) < 1e-10
+
+
+def test_interior_patch_matches_oracle(pf, O, cuda):
+    # a band that is cheapest as an interior periodisation (no DFS reflection)
+    rng = np.random.default_rng(4)
+    L = 1024
+    th = 0.9 + 0.12 * (2 * rng.random(3000) - 1)
+    ph = 2 * np.pi * rng.random(3000)
+    ps = pf.Plan(th, ph, lmax=L, tol=1e-8, method="stretch")
+    assert ps.info["kind"] == "interior"
+    so = O.Stretch(th, ph, L, 1e-8, nufft="es")
+    alm = O.rand_alm(L, rng=rng)
+    f = _fwd(ps, alm)
+    assert rel(f, so.forward(alm, nthreads=8)[:, 0]) < 1e-11
+    g = cn(rng, 3000)
+    a = _adj(ps, g)
+    assert O.alm_reldiff(a, so.adjoint(g, nthreads=8)[:, :, 0], L) < 1e-10
+    assert dot_rel(f, g, alm[:, :, 0], a) < 1e-12
+
+
+@pytest.mark.parametrize("B", [3, 5])
+def test_ntrans_batching(pf, O, cuda, B):
+    # test/test_transforms.jl:142-156; B = 3 runs the 2-transform kernels then a single one,
+    # B = 5 the 4-transform kernels then a single one
+    rng = np.random.default_rng(36)
+    L = 256
+    th, ph = _sqrt_cap(rng, 100)
+    p1 = pf.Plan(th, ph, lmax=L, tol=1e-8, method="stretch")
+    pB = pf.Plan(th, ph, lmax=L, tol=1e-8, method="stretch", ntrans=B)
+    almB = _randn_alm(O, L, rng, B)
+    fB = _fwd(pB, almB)
+    g = np.asfortranarray(cn(rng, 100, B))
+    aB = _adj(pB, g)
+    for b in range(B):
+        assert rel(fB[:, b], _fwd(p1, almB[:, :, b:b + 1])) < 1e-9
+        assert O.alm_reldiff(aB[:, :, b], _adj(p1, np.ascontiguousarray(g[:, b])), L) < 1e-9
+
+
+def test_direct_leaf_matches_ylm(pf, O, cuda):
+    # test/test_transforms.jl:20-57: the Direct leaf against the closed form and its adjoint
+    rng = np.random.default_rng(31)
+    L = 64
+    th = np.pi * rng.random(300)
+    ph = 2 * np.pi * rng.random(300)
+    pd = pf.Plan(th, ph, lmax=L, method="direct")
+    assert pd.algorithm == "DirectAlgorithm"
+    alm = _randn_alm(O, L, rng)
+    ref = O.Direct(th, ph, L)
+    f = _fwd(pd, alm)
+    assert rel(f, ref.forward(alm)[:, 0]) < 1e-13
+    g = cn(rng, 300)
+    a = _adj(pd, g)
+    assert O.alm_reldiff(a, ref.adjoint(g)[:, :, 0], L) < 1e-13
+    assert dot_rel(f, g, alm[:, :, 0], a) < 1e-13
+    # single harmonics against the closed form (test/test_transforms.jl:33-43)
+    for (l, m) in [(0, 0), (5, -3), (17, 17), (64, -1)]:
+        e = O.zeros_alm(L)
+        e[O.sph_mode(l, m) + (0,)] = 1.0
+        y = np.array([O.ylm(l, m, t, p) for t, p in zip(th[:20], ph[:20])])
+        assert np.abs(_fwd(pd, e)[:20] - y).max() < 1e-13
+
+
+def test_host_buffers_equal_device_applies(pf, O, cuda):
+    # pfsht_forward_host / pfsht_adjoint_host copy in, apply and copy out
+    rng = np.random.default_rng(40)
+    L = 256
+    th, ph = cap_points(20000, rng=rng)
+    ps = pf.Plan(th, ph, lmax=L, tol=1e-8)
+    alm = np.asfortranarray(O.rand_alm(L, rng=rng)[:, :, 0])
+    f_host = pf.zeros_field(len(th), device="cpu")
+    ps.mul(f_host, alm)
+    assert np.array_equal(f_host, _fwd(ps, alm[:, :, None]))
+    g = cn(rng, len(th))
+    a_host = pf.zeros_alm(L, device="cpu")
+    ps.mul_adjoint(a_host, g)
+    assert O.alm_reldiff(a_host, _adj(ps, g), L) < 1e-14
+
+
+def test_forward_is_deterministic(pf, O, cuda):
+    # the forward path has no atomics: two applies agree bit for bit
+    rng = np.random.default_rng(41)
+    L = 512
+    th, ph = cap_points(50000, rng=rng)
+    ps = pf.Plan(th, ph, lmax=L, tol=1e-8)
+    alm = to_dev(O.rand_alm(L, rng=rng)[:, :, 0])
+    f1 = to_host(ps * alm)
+    f2 = to_host(ps * alm)
+    assert np.array_equal(f1, f2)
+
+
+@pytest.mark.parametrize("seg", [-1, 64, 192, 256, 1024])
+def test_adjoint_degree_segments_match_oracle(pf, O, cuda, seg):
+    # the adjoint ring pass split along the degree axis, each piece started from the
+    # recurrence state saved at plan time, against the oracle's unsplit walk
+    rng = np.random.default_rng(42)
+    L = 512
+    th, ph = cap_points(6000, rng=rng)
+    plan = pf.Plan(th, ph, lmax=L, tol=1e-8, segment_degrees=seg)
+    ref = O.Stretch(th, ph, L, 1e-8, nufft="es")
+    n = plan.info["nrings"]
+    Gr = np.asfortranarray(cn(rng, n, 2 * L + 1, 1))
+    a = to_dev(np.zeros((L + 1, 2 * L + 1, 1), np.complex128, order="F"))
+    pf.ring_adjoint(plan, to_dev(Gr), a)
+    assert O.alm_reldiff(to_host(a), ref.rings.alm_from_rings(Gr), L) < 1e-12
+    g = cn(rng, len(th))
+    assert O.alm_reldiff(_adj(plan, g), ref.adjoint(g, nthreads=8)[:, :, 0], L) < 1e-10
+
+
+def test_direct_plan_adjoint_segments(pf, O, cuda):
+    # a direct plan over few points splits every order along the degree axis
+    rng = np.random.default_rng(43)
+    L = 700
+    th = np.pi * rng.random(100)
+    ph = 2 * np.pi * rng.random(100)
+    ref = O.Direct(th, ph, L)
+    g = cn(rng, 100)
+    a_ref = ref.adjoint(g, nthreads=8)[:, :, 0]
+    for seg in (-1, 128, 0):
+        pd = pf.Plan(th, ph, lmax=L, method="direct", segment_degrees=seg)
+        assert O.alm_reldiff(_adj(pd, g), a_ref, L) < 1e-12
+
+
+@pytest.mark.parametrize("typ", [1, 2])
+def test_nufft_seam_matches_direct_sum(pf, O, cuda, typ):
+    # src/NUFFT.jl:17-25 seam against the DirectSum backend (src/NUFFT.jl:155-199)
+    rng = np.random.default_rng(44)
+    n1, n2, M, tol = 40, 30, 500, 1e-9
+    x = 2 * np.pi * rng.random(M) - np.pi
+    y = 4 * np.pi * rng.random(M) - 2 * np.pi   # any real values, taken modulo 2 pi
+    p = pf.NUFFT(typ, n1, n2, +1 if typ == 2 else -1, x, y, tol)
+    if typ == 2:
+        c = np.asfortranarray(cn(rng, n1, n2))
+        out = to_dev(np.zeros(M, np.complex128))
+        p.exec(to_dev(c), out)
+        ref = O.nufft_direct(2, n1, n2, +1, x, y, c)[:, 0]
+    else:
+        c = cn(rng, M)
+        out = to_dev(np.zeros((n1, n2), np.complex128, order="F"))
+        p.exec(to_dev(c), out)
+        ref = O.nufft_direct(1, n1, n2, -1, x, y, c)[:, :, 0]
+    assert rel(to_host(out), ref) < 200 * tol
+
+
+@pytest.mark.parametrize("spin", [0, 1])
+def test_dfs_kernels_match_oracle(pf, O, cuda, spin):
+    # src/DFS.jl:13-56: device dfs_double! / dfs_fold! against the oracle, bit for bit
+    rng = np.random.default_rng(45)
+    F = np.asfortranarray(cn(rng, 9, 12, 2))
+    Ft = to_dev(np.zeros((18, 12, 2), np.complex128, order="F"))
+    pf.dfs_double(to_dev(F), Ft, spin=spin)
+    assert np.array_equal(to_host(Ft), O.dfs_double(F, spin=spin))
+    T = np.asfortranarray(cn(rng, 18, 12, 2))
+    Fd = to_dev(np.zeros((9, 12, 2), np.complex128, order="F"))
+    pf.dfs_fold(to_dev(T), Fd, spin=spin)
+    assert np.array_equal(to_host(Fd), O.dfs_fold(T, spin=spin))
+
+
+def test_refused_geometry_runs_the_direct_leaf(pf, O, cuda):
+    # src/Windows.jl:66-75 with src/Cost.jl:121-122: AUTO answers a refused geometry with the
+    # direct leaf on the device
+    rng = np.random.default_rng(0)
+    th = 0.02 + 0.03 * rng.random(50)
+    ph = rng.random(50)
+    with pytest.raises(pf.RefusedGeometry):
+        pf.Plan(th, ph, lmax=32, tol=1e-10, method="stretch")
+    p = pf.Plan(th, ph, lmax=32, tol=1e-10)
+    assert p.info["kind"] == "direct"
+    alm = _randn_alm(O, 32, rng)
+    assert rel(_fwd(p, alm), O.Direct(th, ph, 32).forward(alm)[:, 0]) < 1e-13
+
+
+def test_bench_workload_dot_and_direct_subsample(pf, O, cuda):
+    # lmax 2048 on the 20-degree cap: size-independent checks at full size. The adjoint is
+    # the transpose at round-off; on a subsample of points the forward matches the direct sum
+    # within 10 tol (the reference's accuracy gate)
+    rng = np.random.default_rng(46)
+    L, tol = 2048, 1e-8
+    M = int(round((L * THETA_STAR) ** 2 * 4))
+    th, ph = cap_points(M, rng=rng)
+    ps = pf.Plan(th, ph, lmax=L, tol=tol)
+    alm = O.rand_alm(L, rng=rng)
+    f = _fwd(ps, alm)
+    g = cn(rng, M)
+    a = _adj(ps, g)
+    assert dot_rel(f, g, alm[:, :, 0], a) < 1e-12
+    idx = rng.choice(M, 24, replace=False)
+    fd = O.Direct(th[idx], ph[idx], L).forward(alm, nthreads=8)[:, 0]
+    assert rel(f[idx], fd) < 10 * tol
