@@ -101,6 +101,12 @@ pfsht_status pfsht_adjoint(pfsht_plan* plan, const void* f, void* alm, void* str
 pfsht_status pfsht_forward_host(pfsht_plan* plan, const void* alm, void* f);
 pfsht_status pfsht_adjoint_host(pfsht_plan* plan, const void* f, void* alm);
 
+/* Bytes the two host-buffer applies move across PCIe per call (no reference counterpart):
+ * the coefficient array travels as its sph_mode staircase (rows 0..lmax-m of each order, in
+ * blocks of orders; the adjoint zeroes the host padding itself), the field whole. */
+pfsht_status pfsht_host_bytes(const pfsht_plan* plan, int64_t* h2d_forward, int64_t* d2h_forward,
+                              int64_t* h2d_adjoint, int64_t* d2h_adjoint);
+
 /* rings_from_alm! / alm_from_rings! (src/Legendre.jl:310-341) on the plan's ring set:
  * G is nrings x (2lmax+1) x ntrans on the device. For parity tests of the ring pass. */
 pfsht_status pfsht_ring_forward(pfsht_plan* plan, const void* alm, void* G, void* stream);

@@ -224,6 +224,13 @@ class Plan:
         """ring_work(plan) (src/Plan.jl:44): retained (l, m, ring) triples per apply."""
         return int(_lib.load().pfsht_ring_work(self._h))
 
+    def host_bytes(self) -> dict:
+        """Bytes one host-buffer forward / adjoint moves between host and device."""
+        v = [C.c_int64() for _ in range(4)]
+        _lib.check(_lib.load().pfsht_host_bytes(self._h, *[C.byref(x) for x in v]), "host_bytes")
+        return {"h2d_forward": v[0].value, "d2h_forward": v[1].value,
+                "h2d_adjoint": v[2].value, "d2h_adjoint": v[3].value}
+
     def workspace_bytes(self) -> int:
         return int(_lib.load().pfsht_workspace_bytes(self._h))
 

@@ -53,6 +53,8 @@ SIGNATURES = {
     "pfsht_ring_forward": (C.c_int, [_vp, _vp, _vp, _vp]),
     "pfsht_ring_adjoint": (C.c_int, [_vp, _vp, _vp, _vp]),
     "pfsht_ring_work": (C.c_int64, [_vp]),
+    "pfsht_host_bytes": (C.c_int, [_vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                   C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "pfsht_plan_get_info": (C.c_int, [_vp, C.POINTER(PlanInfo)]),
     "pfsht_workspace_bytes": (C.c_int64, [_vp]),
     "pfsht_plan_geometry": (C.c_int, [_vp, _vp, C.c_int64, C.c_int32, C.c_int32, C.c_double,

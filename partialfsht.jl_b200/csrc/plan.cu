@@ -530,6 +530,71 @@ pfsht_status pfsht_adjoint(pfsht_plan* p, const void* f, void* alm, void* stream
     return (pfsht_status)apply_adjoint(p, (const double2*)f, (double2*)alm, (cudaStream_t)stream);
 }
 
+// The sph_mode coefficient array (src/Layout.jl:13-20) holds order m in the columns 2m - 1 and
+// 2m, rows 0 .. lmax - m: a staircase filling half of the (lmax + 1) x (2 lmax + 1) array.
+// Host copies move it as blocks of orders [m0, m1): the contiguous columns
+// [max(0, 2 m0 - 1), 2 m1 - 1), rows 0 .. lmax - m0, one 2-D copy each. Blocks of about
+// (lmax + 1) / 16 orders keep both the number of copies and the padding they carry small.
+struct AlmBlock {
+    int c0, c1, rows;
+};
+static std::vector<AlmBlock> alm_blocks(int L) {
+    const int G = std::max(32, (L + 1 + 15) / 16);
+    std::vector<AlmBlock> v;
+    for (int m0 = 0; m0 <= L; m0 += G) {
+        const int m1 = std::min(L + 1, m0 + G);
+        v.push_back(AlmBlock{m0 == 0 ? 0 : 2 * m0 - 1, 2 * m1 - 1, L + 1 - m0});
+    }
+    return v;
+}
+
+// bytes a host apply moves: the coefficient blocks and the field
+static void host_bytes(const pfsht_plan* p, int64_t* alm_bytes, int64_t* f_bytes) {
+    int64_t a = 0;
+    for (const AlmBlock& b : alm_blocks(p->L)) a += (int64_t)b.rows * (b.c1 - b.c0);
+    *alm_bytes = a * (int64_t)sizeof(double2) * p->B;
+    *f_bytes = (int64_t)sizeof(double2) * p->M * p->B;
+}
+
+static int alm_copy(pfsht_plan* p, void* host, bool to_device, cudaStream_t s) {
+    const int L = p->L;
+    const size_t col = sizeof(double2) * (size_t)(L + 1);
+    const size_t tr = col * (2 * L + 1);
+    char* h = static_cast<char*>(host);
+    char* d = p->st_alm.as<char>();
+    for (int b = 0; b < p->B; ++b) {
+        for (const AlmBlock& k : alm_blocks(L)) {
+            const size_t off = tr * b + col * k.c0;
+            const size_t width = sizeof(double2) * (size_t)k.rows;
+            if (to_device)
+                PF_CUDA(cudaMemcpy2DAsync(d + off, col, h + off, col, width, k.c1 - k.c0,
+                                          cudaMemcpyHostToDevice, s));
+            else
+                PF_CUDA(cudaMemcpy2DAsync(h + off, col, d + off, col, width, k.c1 - k.c0,
+                                          cudaMemcpyDeviceToHost, s));
+        }
+    }
+    return 0;
+}
+
+// zero the padding rows of the host array that the block copies leave out (rows past each
+// block's height), on host threads while the copies run
+static void alm_zero_host_padding(const pfsht_plan* p, void* host) {
+    const int L = p->L;
+    const std::vector<AlmBlock> blocks = alm_blocks(L);
+    std::vector<int> rows(2 * L + 1);
+    for (const AlmBlock& k : blocks)
+        for (int c = k.c0; c < k.c1; ++c) rows[c] = k.rows;
+    double2* h = static_cast<double2*>(host);
+    const int64_t ncol = (int64_t)(2 * L + 1) * p->B;
+#pragma omp parallel for schedule(static) num_threads(16) if (ncol > 512)
+    for (int64_t q = 0; q < ncol; ++q) {
+        const int c = (int)(q % (2 * L + 1));
+        if (rows[c] <= L)
+            std::memset(h + q * (L + 1) + rows[c], 0, sizeof(double2) * (size_t)(L + 1 - rows[c]));
+    }
+}
+
 static int host_apply(pfsht_plan* p, const void* in, void* out, bool fwd) {
     DeviceGuard dg(p->device);
     const size_t na = sizeof(double2) * (size_t)(p->L + 1) * (2 * p->L + 1) * p->B;
@@ -538,16 +603,30 @@ static int host_apply(pfsht_plan* p, const void* in, void* out, bool fwd) {
     if (!p->st_f.p) PF_TRY(p->st_f.alloc(nf));
     cudaStream_t s = p->st_stream;
     if (fwd) {
-        PF_CUDA(cudaMemcpyAsync(p->st_alm.p, in, na, cudaMemcpyHostToDevice, s));
+        // the forward reads rows 0 .. lmax - m of each order only
+        PF_TRY(alm_copy(p, const_cast<void*>(in), true, s));
         PF_TRY(apply_forward(p, p->st_alm.as<double2>(), p->st_f.as<double2>(), s));
         PF_CUDA(cudaMemcpyAsync(out, p->st_f.p, nf, cudaMemcpyDeviceToHost, s));
     } else {
         PF_CUDA(cudaMemcpyAsync(p->st_f.p, in, nf, cudaMemcpyHostToDevice, s));
         PF_TRY(apply_adjoint(p, p->st_f.as<double2>(), p->st_alm.as<double2>(), s));
-        PF_CUDA(cudaMemcpyAsync(out, p->st_alm.p, na, cudaMemcpyDeviceToHost, s));
+        PF_TRY(alm_copy(p, out, false, s));
+        alm_zero_host_padding(p, out);
     }
     PF_CUDA(cudaStreamSynchronize(s));
     return 0;
+}
+
+pfsht_status pfsht_host_bytes(const pfsht_plan* p, int64_t* h2d_forward, int64_t* d2h_forward,
+                              int64_t* h2d_adjoint, int64_t* d2h_adjoint) {
+    if (!p) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "NULL plan");
+    int64_t a = 0, f = 0;
+    host_bytes(p, &a, &f);
+    if (h2d_forward) *h2d_forward = a;
+    if (d2h_forward) *d2h_forward = f;
+    if (h2d_adjoint) *h2d_adjoint = f;
+    if (d2h_adjoint) *d2h_adjoint = a;
+    return PFSHT_OK;
 }
 
 pfsht_status pfsht_forward_host(pfsht_plan* p, const void* alm, void* f) {

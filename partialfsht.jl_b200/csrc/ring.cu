@@ -336,22 +336,34 @@ __device__ __forceinline__ void ring_fwd_item(const RingTables& t, const RingOut
             }
         };
         int steps = 0;
+        // the coefficients of the next 32 degrees are loaded while this chunk runs
+        double2 ab_n = zero2, ap_n[NB], am_n[NB];
+        auto fetch = [&](int l) {
+            if (l <= L) {
+                ab_n = abm[l - m - 2];
+#pragma unroll
+                for (int b = 0; b < NB; ++b) {
+                    ap_n[b] = colp[(l - m) + albs * b];
+                    am_n[b] = m > 0 ? colm[(l - m) + albs * b] : zero2;
+                }
+            }
+        };
+#pragma unroll
+        for (int b = 0; b < NB; ++b) ap_n[b] = am_n[b] = zero2;
+        fetch(m + 2 + lane);
         for (int l0 = m + 2; l0 <= L; l0 += 32) {
             const int nl = min(32, L - l0 + 1);
             __syncwarp();
             if (lane < nl) {
-                const int l = l0 + lane;
-                sm.ab[warp][lane] = abm[l - m - 2];
+                sm.ab[warp][lane] = ab_n;
 #pragma unroll
                 for (int b = 0; b < NB; ++b) {
-                    sm.ap[warp][b][lane] = colp[(l - m) + albs * b];
-                    double2 am = m > 0 ? colm[(l - m) + albs * b] : zero2;
-                    am.x *= sgn;
-                    am.y *= sgn;
-                    sm.am[warp][b][lane] = am;
+                    sm.ap[warp][b][lane] = ap_n[b];
+                    sm.am[warp][b][lane] = make_double2(am_n[b].x * sgn, am_n[b].y * sgn);
                 }
             }
             __syncwarp();
+            fetch(l0 + 32 + lane);
             const int nblk = nl >> 3;
             for (int blk = 0; blk < nblk; ++blk) {
 #pragma unroll
@@ -458,11 +470,18 @@ ring_fwd_kernel(RingTables t, RingOut o, const RingItem* __restrict__ items, int
 // ---------------------------------------------------------------------------------------
 // adjoint: ring columns -> alm
 // ---------------------------------------------------------------------------------------
-// Two warps per block: each warp double-buffers its reduction area, so one block's partial
-// sums are reduced while the next block's degrees are computed.
+// Two warps per block. With kAdjPipelined each warp double-buffers its reduction area, so
+// one block's partial sums are reduced while the next block's degrees are computed; without
+// it a block is reduced as soon as it is staged (half the shared memory per warp).
 static constexpr int kAdjWarps = 2;
+static constexpr bool kAdjPipelined = false;
+#ifdef PF_ADJ_MIN_BLOCKS
+#define PF_ADJ_BOUNDS __launch_bounds__(kAdjWarps * 32, PF_ADJ_MIN_BLOCKS)
+#else
+#define PF_ADJ_BOUNDS __launch_bounds__(kAdjWarps * 32)
+#endif
 struct AdjSmem {
-    double red[kAdjWarps][2][32][33];
+    double red[kAdjWarps][kAdjPipelined ? 2 : 1][32][33];
     double2 ab[kAdjWarps][32];
 };
 
@@ -557,7 +576,7 @@ __device__ __forceinline__ void ring_adj_item(const RingTables& t, const RingOut
             }
         }
 #pragma unroll
-        for (int v = 0; v < NV; ++v) sm.red[warp][cur][slot * NV + v][lane] = part[v];
+        for (int v = 0; v < NV; ++v) sm.red[warp][kAdjPipelined ? cur : 0][slot * NV + v][lane] = part[v];
     };
     // lane's output (degree lfirst + lane / NV, component lane % NV) of a reduced block
     auto write_out = [&](int lfirst, double s) {
@@ -579,10 +598,10 @@ __device__ __forceinline__ void ring_adj_item(const RingTables& t, const RingOut
             double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
 #pragma unroll
             for (int q = 0; q < 32; q += 4) {
-                s0 += sm.red[warp][cur][lane][q];
-                s1 += sm.red[warp][cur][lane][q + 1];
-                s2 += sm.red[warp][cur][lane][q + 2];
-                s3 += sm.red[warp][cur][lane][q + 3];
+                s0 += sm.red[warp][kAdjPipelined ? cur : 0][lane][q];
+                s1 += sm.red[warp][kAdjPipelined ? cur : 0][lane][q + 1];
+                s2 += sm.red[warp][kAdjPipelined ? cur : 0][lane][q + 2];
+                s3 += sm.red[warp][kAdjPipelined ? cur : 0][lane][q + 3];
             }
             write_out(lfirst, (s0 + s1) + (s2 + s3));
         }
@@ -592,7 +611,7 @@ __device__ __forceinline__ void ring_adj_item(const RingTables& t, const RingOut
     auto drain = [&](int i) {
 #pragma unroll
         for (int k = 0; k < NV; k += 4) {
-            const double* rowp = &sm.red[warp][cur ^ 1][lane][i * NV + k];
+            const double* rowp = &sm.red[warp][kAdjPipelined ? cur ^ 1 : 0][lane][i * NV + k];
             a0 += rowp[0];
             a1 += rowp[1];
             a2 += rowp[2];
@@ -630,14 +649,25 @@ __device__ __forceinline__ void ring_adj_item(const RingTables& t, const RingOut
         };
         // segments start on the renormalisation schedule, so the count restarts at 0
         int steps = 0;
+        // the coefficients of the next 32 degrees are loaded while this chunk runs
+        double2 ab_next = make_double2(0.0, 0.0);
+        if (lstart <= item.lend && lane <= item.lend - lstart) ab_next = abm[lstart + lane - m - 2];
         for (int l0 = lstart; l0 <= item.lend; l0 += 32) {
             const int nl = min(32, item.lend - l0 + 1);
             __syncwarp();
-            if (lane < nl) sm.ab[warp][lane] = abm[l0 + lane - m - 2];
+            if (lane < nl) sm.ab[warp][lane] = ab_next;
             __syncwarp();
+            if (l0 + 32 + lane <= item.lend) ab_next = abm[l0 + 32 + lane - m - 2];
             const int nblk = nl / LB;
             for (int blk = 0; blk < nblk; ++blk) {
-                if (pend >= 0) {
+                if (!kAdjPipelined) {
+#pragma unroll
+                    for (int i = 0; i < LB; ++i) {
+                        rec(blk * LB + i);
+                        stage(p1, i);
+                    }
+                    flush(l0 + blk * LB, LB);
+                } else if (pend >= 0) {
 #pragma unroll
                     for (int i = 0; i < LB; ++i) {
                         rec(blk * LB + i);
@@ -651,11 +681,13 @@ __device__ __forceinline__ void ring_adj_item(const RingTables& t, const RingOut
                         stage(p1, i);
                     }
                 }
-                // this block's sums are visible, and every lane is done with the other buffer
-                __syncwarp();
-                if (pend >= 0) finish();
-                pend = l0 + blk * LB;
-                cur ^= 1;
+                if (kAdjPipelined) {
+                    // this block's sums are visible, and every lane is done with the other buffer
+                    __syncwarp();
+                    if (pend >= 0) finish();
+                    pend = l0 + blk * LB;
+                    cur ^= 1;
+                }
                 steps += LB;
                 if (steps == kStride) {
                     steps = 0;
@@ -714,7 +746,7 @@ __device__ __forceinline__ void ring_adj_item(const RingTables& t, const RingOut
 }
 
 template <int RMAX, int NB>
-__global__ void __launch_bounds__(kAdjWarps * 32)
+__global__ void PF_ADJ_BOUNDS
 ring_adj_kernel(RingTables t, RingOut o, const RingItem* __restrict__ items, int nitems,
                 const double2* __restrict__ in, double* __restrict__ almd, int b0, int allow_sole) {
     __shared__ AdjSmem sm;

@@ -153,20 +153,35 @@ def test_direct_leaf_matches_ylm(pf, O, cuda):
         assert np.abs(_fwd(pd, e)[:20] - y).max() < 1e-13
 
 
-def test_host_buffers_equal_device_applies(pf, O, cuda):
-    # pfsht_forward_host / pfsht_adjoint_host copy in, apply and copy out
+@pytest.mark.parametrize("L,B", [(256, 1), (700, 1), (300, 3)])
+def test_host_buffers_equal_device_applies(pf, O, cuda, L, B):
+    # pfsht_forward_host / pfsht_adjoint_host move the sph_mode staircase in blocks of orders:
+    # what the padding slots hold on input is ignored, and the adjoint leaves them zero
     rng = np.random.default_rng(40)
-    L = 256
     th, ph = cap_points(20000, rng=rng)
-    ps = pf.Plan(th, ph, lmax=L, tol=1e-8)
-    alm = np.asfortranarray(O.rand_alm(L, rng=rng)[:, :, 0])
-    f_host = pf.zeros_field(len(th), device="cpu")
-    ps.mul(f_host, alm)
-    assert np.array_equal(f_host, _fwd(ps, alm[:, :, None]))
-    g = cn(rng, len(th))
-    a_host = pf.zeros_alm(L, device="cpu")
+    ps = pf.Plan(th, ph, lmax=L, tol=1e-8, ntrans=B)
+    alm = O.rand_alm(L, ntrans=B, rng=rng)
+    pad = ~O.valid_mask(L)
+    dirty = alm.copy(order="F")
+    dirty[pad] = np.nan
+    a_in = np.asfortranarray(dirty if B > 1 else dirty[:, :, 0])
+    f_host = pf.zeros_field(len(th), ntrans=B, device="cpu")
+    ps.mul(f_host, a_in)
+    f_dev = _fwd(ps, alm)
+    assert np.array_equal(f_host, f_dev)
+    g = np.asfortranarray(cn(rng, len(th), B)) if B > 1 else cn(rng, len(th))
+    a_host = pf.zeros_alm(L, ntrans=B, device="cpu")
+    a_host[...] = np.nan
     ps.mul_adjoint(a_host, g)
-    assert O.alm_reldiff(a_host, _adj(ps, g), L) < 1e-14
+    a_dev = _adj(ps, g)
+    a3 = a_host if B > 1 else a_host[:, :, None]
+    assert np.all(a3[pad] == 0)
+    # the adjoint adds some partial sums atomically: equal up to the order of those additions
+    assert O.alm_reldiff(a_host, a_dev, L) < 1e-14
+    hb = ps.host_bytes()
+    valid = (L + 1) ** 2 * 16 * B
+    assert valid <= hb["h2d_forward"] < 1.15 * valid
+    assert hb["d2h_forward"] == hb["h2d_adjoint"] == len(th) * 16 * B
 
 
 def test_forward_is_deterministic(pf, O, cuda):
