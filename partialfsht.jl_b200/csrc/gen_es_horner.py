@@ -57,6 +57,7 @@ def main():
     out.append("// Generated by gen_es_horner.py; do not edit. Per-tap Horner coefficients of the")
     out.append("// ES NUFFT kernel exp(beta (sqrt(1 - z^2) - 1)), beta = 2.30 w, degree w + 2, in")
     out.append("// v = s - 1/2 where s = i0 - g + w/2 in [0, 1) is the point's offset to its first cell.")
+    out.append("// The float copies (rounded to 9 digits) serve the single-precision NUFFT.")
     out.append("#pragma once")
     out.append("")
     out.append("namespace pf {")
@@ -68,10 +69,14 @@ def main():
         rows = [tap_coeffs(w, a, beta, d) for a in range(w)]
         vals = ", ".join(mp.nstr(c, 17, min_fixed=-1, max_fixed=-1) if abs(c) > mp.mpf(10) ** -40
                          else "0.0" for r in rows for c in r)
+        fvals = ", ".join((mp.nstr(c, 9, min_fixed=-1, max_fixed=-1) + "f") if abs(c) > mp.mpf(10) ** -30
+                          else "0.0f" for r in rows for c in r)
         out.append(f"__constant__ double kEsHorner{w}[{w * (d + 1)}] = {{{vals}}};")
+        out.append(f"__constant__ float kEsHornerF{w}[{w * (d + 1)}] = {{{fvals}}};")
         out.append(f"template <> struct EsHorner<{w}> {{")
         out.append(f"    static constexpr int NC = {d + 1};")
         out.append(f"    __device__ static const double* coef() {{ return kEsHorner{w}; }}")
+        out.append(f"    __device__ static const float* coef_f() {{ return kEsHornerF{w}; }}")
         out.append("};")
     out.append("")
     out.append("}  // namespace pf")

@@ -185,6 +185,7 @@ struct NufftGrid {
     int ncols = 0;             // mode columns
     int bin_rows = 16, bin_cols = 16, nbr = 0, nbc = 0;
     int nbusy = 0;             // bins holding at least one point
+    int fp32 = 0;              // fine grids, FFTs, spreading and interpolation in FP32
     int64_t M = 0;
 };
 

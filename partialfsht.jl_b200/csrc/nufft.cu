@@ -265,27 +265,55 @@ int nufft_setpts(NufftGrid& g, NufftDev& d, const double* x, const double* y, cu
 }
 
 int nufft_alloc(NufftGrid& g, NufftDev& d, int B) {
-    PF_TRY(d.pad.alloc(sizeof(double2) * (size_t)g.nf1 * g.ncols * B));
-    PF_TRY(d.U.alloc(sizeof(double2) * (size_t)g.nrows * g.nf2 * B));
+    const size_t el = g.fp32 ? sizeof(float2) : sizeof(double2);
+    const cufftType ty = g.fp32 ? CUFFT_C2C : CUFFT_Z2Z;
+    PF_TRY(d.pad.alloc(el * (size_t)g.nf1 * g.ncols * B));
+    PF_TRY(d.U.alloc(el * (size_t)g.nrows * g.nf2 * B));
     int n1[1] = {g.nf1};
-    PF_CUFFT(cufftPlanMany(&d.f1, 1, n1, n1, 1, g.nf1, n1, 1, g.nf1, CUFFT_Z2Z, g.ncols * B));
+    PF_CUFFT(cufftPlanMany(&d.f1, 1, n1, n1, 1, g.nf1, n1, 1, g.nf1, ty, g.ncols * B));
     d.have_f1 = true;
     int n2[1] = {g.nf2};
-    PF_CUFFT(cufftPlanMany(&d.f2, 1, n2, n2, 1, g.nf2, n2, 1, g.nf2, CUFFT_Z2Z, g.nrows * B));
+    PF_CUFFT(cufftPlanMany(&d.f2, 1, n2, n2, 1, g.nf2, n2, 1, g.nf2, ty, g.nrows * B));
     d.have_f2 = true;
     return 0;
 }
 
+// in-place fine-grid FFT of either element type
+static int fine_fft(cufftHandle h, void* data, bool fp32, int dir) {
+    if (fp32)
+        PF_CUFFT(cufftExecC2C(h, static_cast<cufftComplex*>(data), static_cast<cufftComplex*>(data), dir));
+    else
+        PF_CUFFT(cufftExecZ2Z(h, static_cast<cufftDoubleComplex*>(data),
+                              static_cast<cufftDoubleComplex*>(data), dir));
+    return 0;
+}
+
+// ---------------------------------------------------------------------------------------
+// complex element of the fine grids: double2 in the FP64 form, float2 in the mixed form (whose
+// mode columns, points and per-mode factors stay FP64)
+// ---------------------------------------------------------------------------------------
+template <class T> struct Cx;
+template <> struct Cx<double> {
+    using t = double2;
+    __device__ static double2 make(double x, double y) { return make_double2(x, y); }
+};
+template <> struct Cx<float> {
+    using t = float2;
+    __device__ static float2 make(float x, float y) { return make_float2(x, y); }
+};
+template <class T> using cx = typename Cx<T>::t;
+
 // ---------------------------------------------------------------------------------------
 // pad / unpad along dim 1
 // ---------------------------------------------------------------------------------------
+template <class T>
 __global__ void pad_kernel(const double2* __restrict__ in, int n1, int ncols, int nf1,
                            const double2* __restrict__ mult1, const double* __restrict__ dec2,
-                           double2* __restrict__ pad) {
+                           cx<T>* __restrict__ pad) {
     const int c = blockIdx.y, b = blockIdx.z;
     const int pos = (n1 + 1) / 2, neg = n1 / 2;
     const double2* ic = in + (int64_t)n1 * c + (int64_t)n1 * ncols * b;
-    double2* oc = pad + (int64_t)nf1 * c + (int64_t)nf1 * ncols * b;
+    cx<T>* oc = pad + (int64_t)nf1 * c + (int64_t)nf1 * ncols * b;
     const double d2 = dec2[c];
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < nf1; p += gridDim.x * blockDim.x) {
         int i1 = -1;
@@ -298,21 +326,23 @@ __global__ void pad_kernel(const double2* __restrict__ in, int n1, int ncols, in
             v.x = (a.x * f.x - a.y * f.y) * d2;
             v.y = (a.x * f.y + a.y * f.x) * d2;
         }
-        oc[p] = v;
+        oc[p] = Cx<T>::make((T)v.x, (T)v.y);
     }
 }
 
-__global__ void unpad_kernel(const double2* __restrict__ pad, int n1, int ncols, int nf1,
+template <class T>
+__global__ void unpad_kernel(const cx<T>* __restrict__ pad, int n1, int ncols, int nf1,
                              const double2* __restrict__ mult1, const double* __restrict__ dec2,
                              double2* __restrict__ out) {
     const int c = blockIdx.y, b = blockIdx.z;
-    const double2* ic = pad + (int64_t)nf1 * c + (int64_t)nf1 * ncols * b;
+    const cx<T>* ic = pad + (int64_t)nf1 * c + (int64_t)nf1 * ncols * b;
     double2* oc = out + (int64_t)n1 * c + (int64_t)n1 * ncols * b;
     const double d2 = dec2[c];
     for (int i1 = blockIdx.x * blockDim.x + threadIdx.x; i1 < n1; i1 += gridDim.x * blockDim.x) {
         const int k1 = i1 < (n1 + 1) / 2 ? i1 : i1 - n1;
         const int p = k1 >= 0 ? k1 : nf1 + k1;
-        const double2 a = ic[p];
+        const cx<T> a0 = ic[p];
+        const double2 a = make_double2((double)a0.x, (double)a0.y);
         const double2 f = mult1[i1];  // conj(f)
         double2 v;
         v.x = (a.x * f.x + a.y * f.y) * d2;
@@ -325,18 +355,19 @@ __global__ void unpad_kernel(const double2* __restrict__ pad, int n1, int ncols,
 // fine rows <-> fine columns (tile transpose through shared memory)
 // ---------------------------------------------------------------------------------------
 // U[r, p2] = pad[(row0 + r) mod nf1, p2col[p2]] (or 0)
-__global__ void rows_fwd_kernel(const double2* __restrict__ pad, int nf1, int ncols, int row0,
+template <class T>
+__global__ void rows_fwd_kernel(const cx<T>* __restrict__ pad, int nf1, int ncols, int row0,
                                 int nrows, int nf2, const int* __restrict__ p2col,
-                                double2* __restrict__ U) {
-    __shared__ double2 tile[32][33];
+                                cx<T>* __restrict__ U) {
+    __shared__ cx<T> tile[32][33];
     const int b = blockIdx.z;
     const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;  // c0 indexes p2
-    const double2* pb = pad + (int64_t)nf1 * ncols * b;
-    double2* ub = U + (int64_t)nrows * nf2 * b;
+    const cx<T>* pb = pad + (int64_t)nf1 * ncols * b;
+    cx<T>* ub = U + (int64_t)nrows * nf2 * b;
     for (int k = threadIdx.y; k < 32; k += blockDim.y) {
         const int p2 = c0 + k;
         const int r = r0 + threadIdx.x;
-        double2 v = make_double2(0.0, 0.0);
+        cx<T> v = Cx<T>::make(0, 0);
         if (p2 < nf2 && r < nrows) {
             const int c = p2col[p2];
             if (c >= 0) {
@@ -357,18 +388,19 @@ __global__ void rows_fwd_kernel(const double2* __restrict__ pad, int nf1, int nc
 }
 
 // pad[p1, c] = U[(p1 - row0) mod nf1, colp2[c]] when that row is kept, else 0
-__global__ void rows_adj_kernel(const double2* __restrict__ U, int nf1, int ncols, int row0,
+template <class T>
+__global__ void rows_adj_kernel(const cx<T>* __restrict__ U, int nf1, int ncols, int row0,
                                 int nrows, int nf2, const int* __restrict__ colp2,
-                                double2* __restrict__ pad) {
-    __shared__ double2 tile[32][33];
+                                cx<T>* __restrict__ pad) {
+    __shared__ cx<T> tile[32][33];
     const int b = blockIdx.z;
     const int p0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
-    const double2* ub = U + (int64_t)nrows * nf2 * b;
-    double2* pb = pad + (int64_t)nf1 * ncols * b;
+    const cx<T>* ub = U + (int64_t)nrows * nf2 * b;
+    cx<T>* pb = pad + (int64_t)nf1 * ncols * b;
     for (int k = threadIdx.y; k < 32; k += blockDim.y) {
         const int p1 = p0 + k;
         const int c = c0 + threadIdx.x;
-        double2 v = make_double2(0.0, 0.0);
+        cx<T> v = Cx<T>::make(0, 0);
         if (p1 < nf1 && c < ncols) {
             int r = (p1 - row0) % nf1;
             if (r < 0) r += nf1;
@@ -437,11 +469,20 @@ __device__ __forceinline__ void local_origin(double2 g, const TileGeom& tg, int 
     c0 = c - tg.tc0;
 }
 
-template <int W>
-__device__ __forceinline__ double es_poly(int a, double v) {
+template <int W, class T> struct EsCoef;
+template <int W> struct EsCoef<W, double> {
+    __device__ static const double* get() { return EsHorner<W>::coef(); }
+};
+template <int W> struct EsCoef<W, float> {
+    __device__ static const float* get() { return EsHorner<W>::coef_f(); }
+};
+
+// weight of tap a at offset v, in the grid's precision
+template <int W, class T = double>
+__device__ __forceinline__ T es_poly(int a, T v) {
     constexpr int NC = EsHorner<W>::NC;
-    const double* cf = EsHorner<W>::coef();
-    double p = cf[a * NC + NC - 1];
+    const T* cf = EsCoef<W, T>::get();
+    T p = cf[a * NC + NC - 1];
 #pragma unroll
     for (int q = NC - 2; q >= 0; --q) p = fma(p, v, cf[a * NC + q]);
     return p;
@@ -450,22 +491,23 @@ __device__ __forceinline__ double es_poly(int a, double v) {
 // Type-2 interpolation: one CTA per bin copies the bin's tile of U into shared memory, then
 // each thread interpolates points of the bin from it. The row weights are evaluated row by
 // row inside the tap loop so only the column weights are held in registers.
-template <int W>
+template <int W, class T>
 __global__ void __launch_bounds__(128, 5)
 interp_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
               const int* __restrict__ binstart, const int* __restrict__ binorder, int nbc,
-              int BR, int BC, int64_t M, const double2* __restrict__ U, int nrows, int nf2,
+              int BR, int BC, int64_t M, const cx<T>* __restrict__ U, int nrows, int nf2,
               int row_wrap, int B, double2* __restrict__ f) {
-    extern __shared__ double2 tile[];
+    extern __shared__ __align__(16) unsigned char interp_smem[];
+    cx<T>* tile = reinterpret_cast<cx<T>*>(interp_smem);
     const int bin = binorder[blockIdx.x];
     const int s = binstart[bin], e = binstart[bin + 1];
     const TileGeom tg = tile_geom<W>(bin, nbc, BR, BC);
     for (int b = 0; b < B; ++b) {
-        const double2* ub = U + (int64_t)nrows * nf2 * b;
+        const cx<T>* ub = U + (int64_t)nrows * nf2 * b;
         for (int t = threadIdx.x; t < tg.TR * tg.TC; t += blockDim.x) {
             int r = tg.tr0 + t / tg.TC;
             if (row_wrap) r = wrap(r, nrows);
-            double2 v = make_double2(0.0, 0.0);
+            cx<T> v = Cx<T>::make(0, 0);
             if (r >= 0 && r < nrows) v = ub[(int64_t)r * nf2 + wrap(tg.tc0 + t % tg.TC, nf2)];
             tile[t] = v;
         }
@@ -476,19 +518,19 @@ interp_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
             int r0, c0;
             double v1, v2;
             local_origin<W>(g, tg, nrows, nf2, row_wrap, r0, c0, v1, v2);
-            double k2[W];
+            T k2[W];
 #pragma unroll
-            for (int c = 0; c < W; ++c) k2[c] = es_poly<W>(c, v2);
-            double2 acc = make_double2(0.0, 0.0);
+            for (int c = 0; c < W; ++c) k2[c] = es_poly<W, T>(c, (T)v2);
+            cx<T> acc = Cx<T>::make(0, 0);
             if (r0 >= 0 && r0 + W <= tg.TR && c0 >= 0 && c0 + W <= tg.TC) {
 #pragma unroll
                 for (int a = 0; a < W; ++a) {
-                    const double k1 = es_poly<W>(a, v1);
-                    const double2* row = tile + (r0 + a) * tg.TC + c0;
-                    double2 sr = make_double2(0.0, 0.0);
+                    const T k1 = es_poly<W, T>(a, (T)v1);
+                    const cx<T>* row = tile + (r0 + a) * tg.TC + c0;
+                    cx<T> sr = Cx<T>::make(0, 0);
 #pragma unroll
                     for (int c = 0; c < W; ++c) {
-                        const double2 u = row[c];
+                        const cx<T> u = row[c];
                         sr.x = fma(u.x, k2[c], sr.x);
                         sr.y = fma(u.y, k2[c], sr.y);
                     }
@@ -496,7 +538,7 @@ interp_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
                     acc.y = fma(sr.y, k1, acc.y);
                 }
             }
-            f[j + M * b] = acc;
+            f[j + M * b] = make_double2((double)acc.x, (double)acc.y);
         }
         __syncthreads();
     }
@@ -510,53 +552,53 @@ interp_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
 // point's row weights and its value times the column weights into a per-warp staging area;
 // the points are then applied one by one from it, the next point's operands loaded while the
 // current one's W complex FMA pairs run, with no shared-memory read-modify-write.
-template <int W>
+template <int W, class T>
 struct SpreadStage {
     static constexpr int KP = (W + 1) / 2;  // row weights as pairs
-    double2 k1[32][KP];        // row weights (pairs; the odd tail padded with 0)
-    double2 vk[32][W + 1];     // value x column weight; slot W is 0 for lanes off the point
+    cx<T> k1[32][KP];          // row weights (pairs; the odd tail padded with 0)
+    cx<T> vk[32][W + 1];       // value x column weight; slot W is 0 for lanes off the point
     int2 org[32];              // origin row (or -1: skip) and column inside the tile
 };
 
 // warps (bins) per block: the staging area of the wide kernels needs more shared memory
 template <int W> struct SpreadWarps { static constexpr int N = W > 12 ? 2 : 4; };
 
-template <int W>
+template <int W, class T>
 __global__ void __launch_bounds__(SpreadWarps<W>::N * 32)
 spread_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
               const int* __restrict__ binstart, const int* __restrict__ binorder, int nbusy,
               int nbc, int BR, int BC, int64_t M, const double2* __restrict__ fin, int b,
-              int nrows, int nf2, int row_wrap, double2* __restrict__ U) {
-    constexpr int KP = SpreadStage<W>::KP;
+              int nrows, int nf2, int row_wrap, cx<T>* __restrict__ U) {
+    constexpr int KP = SpreadStage<W, T>::KP;
     constexpr int NW = SpreadWarps<W>::N;
-    __shared__ SpreadStage<W> stg[NW];
+    __shared__ SpreadStage<W, T> stg[NW];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int slot = blockIdx.x * NW + warp;
     if (slot >= nbusy) return;
     const int bin = binorder[slot];
     const int s = binstart[bin], e = binstart[bin + 1];
     const TileGeom tg = tile_geom<W>(bin, nbc, BR, BC);
-    SpreadStage<W>& st = stg[warp];
-    double2* ub = U + (int64_t)nrows * nf2 * b;
+    SpreadStage<W, T>& st = stg[warp];
+    cx<T>* ub = U + (int64_t)nrows * nf2 * b;
     const bool col_ok = lane < tg.TC;
     const int gcol = wrap(tg.tc0 + lane, nf2);
-    double2 acc[W];
+    cx<T> acc[W];
 #pragma unroll
-    for (int a = 0; a < W; ++a) acc[a] = make_double2(0.0, 0.0);
+    for (int a = 0; a < W; ++a) acc[a] = Cx<T>::make(0, 0);
     int rbase = -1;
     // add tile row r (a local row) held in acc[a] to U
-    auto flush = [&](int r, const double2& v) {
+    auto flush = [&](int r, const cx<T>& v) {
         int gr = tg.tr0 + r;
         if (row_wrap) gr = wrap(gr, nrows);
         if (col_ok && gr >= 0 && gr < nrows && (v.x != 0.0 || v.y != 0.0)) {
-            double* qd = reinterpret_cast<double*>(ub + (int64_t)gr * nf2 + gcol);
+            T* qd = reinterpret_cast<T*>(ub + (int64_t)gr * nf2 + gcol);
             atomicAdd(qd, v.x);
             atomicAdd(qd + 1, v.y);
         }
     };
     if (lane == 0) {
 #pragma unroll
-        for (int q = 0; q < 32; ++q) st.vk[q][W] = make_double2(0.0, 0.0);
+        for (int q = 0; q < 32; ++q) st.vk[q][W] = Cx<T>::make(0, 0);
     }
     for (int base = s; base < e; base += 32) {
         const int nb = min(32, e - base);
@@ -569,19 +611,19 @@ spread_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
             local_origin<W>(g, tg, nrows, nf2, row_wrap, r0, c0, v1, v2);
 #pragma unroll
             for (int q = 0; q < KP; ++q)
-                st.k1[lane][q] = make_double2(es_poly<W>(2 * q, v1),
-                                              2 * q + 1 < W ? es_poly<W>(2 * q + 1, v1) : 0.0);
+                st.k1[lane][q] = Cx<T>::make(es_poly<W, T>(2 * q, (T)v1),
+                                             2 * q + 1 < W ? es_poly<W, T>(2 * q + 1, (T)v1) : (T)0);
 #pragma unroll
             for (int q = 0; q < W; ++q) {
-                const double k2 = es_poly<W>(q, v2);
-                st.vk[lane][q] = make_double2(v.x * k2, v.y * k2);
+                const T k2 = es_poly<W, T>(q, (T)v2);
+                st.vk[lane][q] = Cx<T>::make((T)v.x * k2, (T)v.y * k2);
             }
             const bool inside = r0 >= 0 && r0 + W <= tg.TR && c0 >= 0 && c0 + W <= tg.TC;
             st.org[lane] = make_int2(inside ? r0 : -1, c0);
         }
         __syncwarp();
         // operands of point q for this lane
-        auto fetch = [&](int q, int2& o, double2& vk, double2 (&k1)[KP]) {
+        auto fetch = [&](int q, int2& o, cx<T>& vk, cx<T> (&k1)[KP]) {
             o = st.org[q];
             const unsigned dc = (unsigned)(lane - o.y);
             vk = st.vk[q][dc < (unsigned)W ? dc : W];
@@ -589,12 +631,12 @@ spread_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
             for (int a2 = 0; a2 < KP; ++a2) k1[a2] = st.k1[q][a2];
         };
         int2 o_n;
-        double2 vk_n, k1_n[KP];
+        cx<T> vk_n, k1_n[KP];
         fetch(0, o_n, vk_n, k1_n);
         for (int q = 0; q < nb; ++q) {
             const int2 o = o_n;
-            const double2 vk = vk_n;
-            double2 k1[KP];
+            const cx<T> vk = vk_n;
+            cx<T> k1[KP];
 #pragma unroll
             for (int a2 = 0; a2 < KP; ++a2) k1[a2] = k1_n[a2];
             if (q + 1 < nb) fetch(q + 1, o_n, vk_n, k1_n);
@@ -607,7 +649,7 @@ spread_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
 #pragma unroll
                     for (int a = 0; a < W; ++a) {
                         flush(rbase + a, acc[a]);
-                        acc[a] = make_double2(0.0, 0.0);
+                        acc[a] = Cx<T>::make(0, 0);
                     }
                     rbase = r0;
                     d = 0;
@@ -616,7 +658,7 @@ spread_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
                     flush(rbase, acc[0]);
 #pragma unroll
                     for (int a = 0; a < W - 1; ++a) acc[a] = acc[a + 1];
-                    acc[W - 1] = make_double2(0.0, 0.0);
+                    acc[W - 1] = Cx<T>::make(0, 0);
                     ++rbase;
                 }
             }
@@ -645,24 +687,24 @@ spread_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
 // so each lane does RH complex FMA pairs per point where the 32-column layout does W. When the
 // origin row advances past a row, the half holding it adds it to U and slides its window by
 // one register; the other half is untouched.
-template <int W>
+template <int W, class T>
 struct Spread16Stage {
     static constexpr int RH = (W + 1) / 2;
     static constexpr int RP = (RH + 1) / 2;  // row weights of one parity, as pairs
-    double2 k1[32][2][RP];     // [point][parity][pair]: even / odd offset row weights, 0-padded
-    double2 vk[32][W + 1];     // value x column weight; slot W is 0 for lanes off the point
+    cx<T> k1[32][2][RP];       // [point][parity][pair]: even / odd offset row weights, 0-padded
+    cx<T> vk[32][W + 1];       // value x column weight; slot W is 0 for lanes off the point
     int2 org[32];              // origin row (or -1: skip) and column inside the tile
 };
 
-template <int W>
+template <int W, class T>
 __global__ void __launch_bounds__(128)
 spread16_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
                 const int* __restrict__ binstart, const int* __restrict__ binorder, int nbusy,
                 int nbc, int BR, int BC, int64_t M, const double2* __restrict__ fin, int b,
-                int nrows, int nf2, int row_wrap, double2* __restrict__ U) {
-    constexpr int RH = Spread16Stage<W>::RH;
-    constexpr int RP = Spread16Stage<W>::RP;
-    __shared__ Spread16Stage<W> stg[4];
+                int nrows, int nf2, int row_wrap, cx<T>* __restrict__ U) {
+    constexpr int RH = Spread16Stage<W, T>::RH;
+    constexpr int RP = Spread16Stage<W, T>::RP;
+    __shared__ Spread16Stage<W, T> stg[4];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int h = lane >> 4, c = lane & 15;
     const int slot = blockIdx.x * 4 + warp;
@@ -670,19 +712,19 @@ spread16_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
     const int bin = binorder[slot];
     const int s = binstart[bin], e = binstart[bin + 1];
     const TileGeom tg = tile_geom<W>(bin, nbc, BR, BC);
-    Spread16Stage<W>& st = stg[warp];
-    double2* ub = U + (int64_t)nrows * nf2 * b;
+    Spread16Stage<W, T>& st = stg[warp];
+    cx<T>* ub = U + (int64_t)nrows * nf2 * b;
     const bool col_ok = c < tg.TC;
     const int gcol = wrap(tg.tc0 + c, nf2);
-    double2 acc[RH];
+    cx<T> acc[RH];
 #pragma unroll
-    for (int i = 0; i < RH; ++i) acc[i] = make_double2(0.0, 0.0);
+    for (int i = 0; i < RH; ++i) acc[i] = Cx<T>::make(0, 0);
     int rbase = -1;  // current origin row (local); this half holds rows base_h + 2 i
-    auto flush = [&](int r, const double2& v) {
+    auto flush = [&](int r, const cx<T>& v) {
         int gr = tg.tr0 + r;
         if (row_wrap) gr = wrap(gr, nrows);
         if (col_ok && gr >= 0 && gr < nrows && (v.x != 0.0 || v.y != 0.0)) {
-            double* qd = reinterpret_cast<double*>(ub + (int64_t)gr * nf2 + gcol);
+            T* qd = reinterpret_cast<T*>(ub + (int64_t)gr * nf2 + gcol);
             atomicAdd(qd, v.x);
             atomicAdd(qd + 1, v.y);
         }
@@ -693,12 +735,12 @@ spread16_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
 #pragma unroll
         for (int i = 0; i < RH; ++i) {
             flush(base_h + 2 * i, acc[i]);
-            acc[i] = make_double2(0.0, 0.0);
+            acc[i] = Cx<T>::make(0, 0);
         }
     };
     if (lane == 0) {
 #pragma unroll
-        for (int q = 0; q < 32; ++q) st.vk[q][W] = make_double2(0.0, 0.0);
+        for (int q = 0; q < 32; ++q) st.vk[q][W] = Cx<T>::make(0, 0);
     }
     for (int base = s; base < e; base += 32) {
         const int nb = min(32, e - base);
@@ -714,14 +756,14 @@ spread16_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
 #pragma unroll
                 for (int p = 0; p < RP; ++p) {
                     const int a0 = par + 4 * p, a1 = par + 4 * p + 2;
-                    st.k1[lane][par][p] = make_double2(a0 < W ? es_poly<W>(a0, v1) : 0.0,
-                                                       a1 < W ? es_poly<W>(a1, v1) : 0.0);
+                    st.k1[lane][par][p] = Cx<T>::make(a0 < W ? es_poly<W, T>(a0, (T)v1) : (T)0,
+                                                      a1 < W ? es_poly<W, T>(a1, (T)v1) : (T)0);
                 }
             }
 #pragma unroll
             for (int q = 0; q < W; ++q) {
-                const double k2 = es_poly<W>(q, v2);
-                st.vk[lane][q] = make_double2(v.x * k2, v.y * k2);
+                const T k2 = es_poly<W, T>(q, (T)v2);
+                st.vk[lane][q] = Cx<T>::make((T)v.x * k2, (T)v.y * k2);
             }
             const bool inside = r0 >= 0 && r0 + W <= tg.TR && c0 >= 0 && c0 + W <= tg.TC;
             st.org[lane] = make_int2(inside ? r0 : -1, c0);
@@ -743,17 +785,17 @@ spread16_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
                             flush(rbase, acc[0]);
 #pragma unroll
                             for (int i = 0; i < RH - 1; ++i) acc[i] = acc[i + 1];
-                            acc[RH - 1] = make_double2(0.0, 0.0);
+                            acc[RH - 1] = Cx<T>::make(0, 0);
                         }
                     }
                 }
             }
             const unsigned dc = (unsigned)(c - o.y);
-            const double2 vk = st.vk[q][dc < (unsigned)W ? dc : W];
+            const cx<T> vk = st.vk[q][dc < (unsigned)W ? dc : W];
             const int par = (h ^ r0) & 1;  // 0: this half holds the even-offset rows
 #pragma unroll
             for (int p = 0; p < RP; ++p) {
-                const double2 kk = st.k1[q][par][p];
+                const cx<T> kk = st.k1[q][par][p];
                 acc[2 * p].x = fma(vk.x, kk.x, acc[2 * p].x);
                 acc[2 * p].y = fma(vk.y, kk.x, acc[2 * p].y);
                 if (2 * p + 1 < RH) {
@@ -766,123 +808,145 @@ spread16_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
     if (rbase >= 0) flush_all();
 }
 
-template <int W>
+template <int W, class T>
 static int launch_interp(const NufftGrid& g, NufftDev& d, double2* f, int B, cudaStream_t s) {
-    const size_t smem = sizeof(double2) * (g.bin_rows + W - 1) * (g.bin_cols + W - 1);
+    const size_t smem = sizeof(cx<T>) * (g.bin_rows + W - 1) * (g.bin_cols + W - 1);
     if (smem > 48 * 1024)
-        PF_CUDA(cudaFuncSetAttribute(interp_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    interp_kernel<W><<<g.nbusy, 128, smem, s>>>(
+        PF_CUDA(cudaFuncSetAttribute(interp_kernel<W, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    interp_kernel<W, T><<<g.nbusy, 128, smem, s>>>(
         d.pts.as<double2>(), d.perm.as<int>(), d.binstart.as<int>(), d.binorder.as<int>(), g.nbc,
-        g.bin_rows, g.bin_cols, g.M, d.U.as<double2>(), g.nrows, g.nf2, g.row_wrap, B, f);
+        g.bin_rows, g.bin_cols, g.M, d.U.as<cx<T>>(), g.nrows, g.nf2, g.row_wrap, B, f);
     return check_launch("interp_kernel");
 }
 
-template <int W>
+template <int W, class T>
 static int launch_spread(const NufftGrid& g, NufftDev& d, const double2* f, int B, cudaStream_t s) {
     if (W <= 10 && g.bin_cols + W - 1 <= 16) {
         for (int b = 0; b < B; ++b) {
-            spread16_kernel<(W <= 10 ? W : 2)><<<(g.nbusy + 3) / 4, 128, 0, s>>>(
+            spread16_kernel<(W <= 10 ? W : 2), T><<<(g.nbusy + 3) / 4, 128, 0, s>>>(
                 d.pts.as<double2>(), d.perm.as<int>(), d.binstart.as<int>(), d.binorder.as<int>(),
                 g.nbusy, g.nbc, g.bin_rows, g.bin_cols, g.M, f, b, g.nrows, g.nf2, g.row_wrap,
-                d.U.as<double2>());
+                d.U.as<cx<T>>());
             PF_TRY(check_launch("spread16_kernel"));
         }
         return 0;
     }
     for (int b = 0; b < B; ++b) {
         constexpr int NW = SpreadWarps<W>::N;
-        spread_kernel<W><<<(g.nbusy + NW - 1) / NW, NW * 32, 0, s>>>(
+        spread_kernel<W, T><<<(g.nbusy + NW - 1) / NW, NW * 32, 0, s>>>(
             d.pts.as<double2>(), d.perm.as<int>(), d.binstart.as<int>(), d.binorder.as<int>(),
             g.nbusy, g.nbc, g.bin_rows, g.bin_cols, g.M, f, b, g.nrows, g.nf2, g.row_wrap,
-            d.U.as<double2>());
+            d.U.as<cx<T>>());
         PF_TRY(check_launch("spread_kernel"));
     }
     return 0;
 }
 
+// kernel widths: 2..16 in FP64; the mixed form runs at tol >= 1e-6, so w <= 8 there
+#define PF_WIDTH_SWITCH(CALL)                                                               \
+    switch (g.w) {                                                                          \
+        case 2: return CALL(2); case 3: return CALL(3); case 4: return CALL(4);             \
+        case 5: return CALL(5); case 6: return CALL(6); case 7: return CALL(7);             \
+        case 8: return CALL(8);                                                             \
+        default: break;                                                                     \
+    }                                                                                       \
+    if constexpr (sizeof(T) == sizeof(double)) {                                            \
+        switch (g.w) {                                                                      \
+            case 9: return CALL(9); case 10: return CALL(10); case 11: return CALL(11);     \
+            case 12: return CALL(12); case 13: return CALL(13); case 14: return CALL(14);   \
+            case 15: return CALL(15); case 16: return CALL(16);                             \
+            default: break;                                                                 \
+        }                                                                                   \
+    }                                                                                       \
+    set_error("unsupported NUFFT kernel width");                                            \
+    return 7;
+
+template <class T>
 static int interp_any(const NufftGrid& g, NufftDev& d, double2* f, int B, cudaStream_t s) {
-#define PF_CALL(WW) launch_interp<WW>(g, d, f, B, s)
-    switch (g.w) {
-        case 2: return PF_CALL(2); case 3: return PF_CALL(3); case 4: return PF_CALL(4);
-        case 5: return PF_CALL(5); case 6: return PF_CALL(6); case 7: return PF_CALL(7);
-        case 8: return PF_CALL(8); case 9: return PF_CALL(9); case 10: return PF_CALL(10);
-        case 11: return PF_CALL(11); case 12: return PF_CALL(12); case 13: return PF_CALL(13);
-        case 14: return PF_CALL(14); case 15: return PF_CALL(15); case 16: return PF_CALL(16);
-        default: set_error("unsupported NUFFT kernel width"); return 7;
-    }
+#define PF_CALL(WW) launch_interp<WW, T>(g, d, f, B, s)
+    PF_WIDTH_SWITCH(PF_CALL)
 #undef PF_CALL
 }
 
+template <class T>
 static int spread_any(const NufftGrid& g, NufftDev& d, const double2* f, int B, cudaStream_t s) {
-#define PF_CALL(WW) launch_spread<WW>(g, d, f, B, s)
-    switch (g.w) {
-        case 2: return PF_CALL(2); case 3: return PF_CALL(3); case 4: return PF_CALL(4);
-        case 5: return PF_CALL(5); case 6: return PF_CALL(6); case 7: return PF_CALL(7);
-        case 8: return PF_CALL(8); case 9: return PF_CALL(9); case 10: return PF_CALL(10);
-        case 11: return PF_CALL(11); case 12: return PF_CALL(12); case 13: return PF_CALL(13);
-        case 14: return PF_CALL(14); case 15: return PF_CALL(15); case 16: return PF_CALL(16);
-        default: set_error("unsupported NUFFT kernel width"); return 7;
-    }
+#define PF_CALL(WW) launch_spread<WW, T>(g, d, f, B, s)
+    PF_WIDTH_SWITCH(PF_CALL)
 #undef PF_CALL
+}
+#undef PF_WIDTH_SWITCH
+
+template <class T>
+static int type2_impl(const NufftGrid& g, NufftDev& d, const double2* modes, double2* f, int B,
+                      int dir, cudaStream_t s, StageClock* clk) {
+    {
+        dim3 grid(nblk(g.nf1, 256), g.ncols, B);
+        pad_kernel<T><<<grid, 256, 0, s>>>(modes, g.n1, g.ncols, g.nf1, d.mult1.as<double2>(),
+                                           d.dec2.as<double>(), d.pad.as<cx<T>>());
+        PF_TRY(check_launch("pad_kernel"));
+    }
+    clock_mark(clk, kStPad, s);
+    PF_CUFFT(cufftSetStream(d.f1, s));
+    PF_TRY(fine_fft(d.f1, d.pad.p, g.fp32, dir));
+    clock_mark(clk, kStFft1Fwd, s);
+    {
+        dim3 grid((g.nf2 + 31) / 32, (g.nrows + 31) / 32, B);
+        rows_fwd_kernel<T><<<grid, dim3(32, 8), 0, s>>>(d.pad.as<cx<T>>(), g.nf1, g.ncols, g.row0,
+                                                        g.nrows, g.nf2, d.p2col.as<int>(),
+                                                        d.U.as<cx<T>>());
+        PF_TRY(check_launch("rows_fwd_kernel"));
+    }
+    clock_mark(clk, kStRowsFwd, s);
+    PF_CUFFT(cufftSetStream(d.f2, s));
+    PF_TRY(fine_fft(d.f2, d.U.p, g.fp32, dir));
+    clock_mark(clk, kStFft2Fwd, s);
+    PF_TRY(interp_any<T>(g, d, f, B, s));
+    clock_mark(clk, kStInterp, s);
+    return 0;
+}
+
+template <class T>
+static int type1_impl(const NufftGrid& g, NufftDev& d, const double2* f, double2* modes, int B,
+                      int dir, cudaStream_t s, StageClock* clk) {
+    PF_CUDA(cudaMemsetAsync(d.U.p, 0, sizeof(cx<T>) * (size_t)g.nrows * g.nf2 * B, s));
+    PF_TRY(spread_any<T>(g, d, f, B, s));
+    clock_mark(clk, kStSpread, s);
+    PF_CUFFT(cufftSetStream(d.f2, s));
+    PF_TRY(fine_fft(d.f2, d.U.p, g.fp32, dir));
+    clock_mark(clk, kStFft2Adj, s);
+    {
+        dim3 grid((g.ncols + 31) / 32, (g.nf1 + 31) / 32, B);
+        rows_adj_kernel<T><<<grid, dim3(32, 8), 0, s>>>(d.U.as<cx<T>>(), g.nf1, g.ncols, g.row0,
+                                                        g.nrows, g.nf2, d.colp2.as<int>(),
+                                                        d.pad.as<cx<T>>());
+        PF_TRY(check_launch("rows_adj_kernel"));
+    }
+    clock_mark(clk, kStRowsAdj, s);
+    PF_CUFFT(cufftSetStream(d.f1, s));
+    PF_TRY(fine_fft(d.f1, d.pad.p, g.fp32, dir));
+    clock_mark(clk, kStFft1Adj, s);
+    {
+        dim3 grid(nblk(g.n1, 256), g.ncols, B);
+        unpad_kernel<T><<<grid, 256, 0, s>>>(d.pad.as<cx<T>>(), g.n1, g.ncols, g.nf1,
+                                             d.mult1.as<double2>(), d.dec2.as<double>(), modes);
+        PF_TRY(check_launch("unpad_kernel"));
+    }
+    clock_mark(clk, kStUnpad, s);
+    return 0;
 }
 
 int nufft_type2(const NufftGrid& g, NufftDev& d, const double2* modes, double2* f, int B,
                 int iflag, cudaStream_t s, StageClock* clk) {
     const int dir = iflag > 0 ? CUFFT_INVERSE : CUFFT_FORWARD;
-    {
-        dim3 grid(nblk(g.nf1, 256), g.ncols, B);
-        pad_kernel<<<grid, 256, 0, s>>>(modes, g.n1, g.ncols, g.nf1, d.mult1.as<double2>(),
-                                        d.dec2.as<double>(), d.pad.as<double2>());
-        PF_TRY(check_launch("pad_kernel"));
-    }
-    clock_mark(clk, kStPad, s);
-    PF_CUFFT(cufftSetStream(d.f1, s));
-    PF_CUFFT(cufftExecZ2Z(d.f1, d.pad.as<cufftDoubleComplex>(), d.pad.as<cufftDoubleComplex>(), dir));
-    clock_mark(clk, kStFft1Fwd, s);
-    {
-        dim3 grid((g.nf2 + 31) / 32, (g.nrows + 31) / 32, B);
-        rows_fwd_kernel<<<grid, dim3(32, 8), 0, s>>>(d.pad.as<double2>(), g.nf1, g.ncols, g.row0,
-                                                     g.nrows, g.nf2, d.p2col.as<int>(),
-                                                     d.U.as<double2>());
-        PF_TRY(check_launch("rows_fwd_kernel"));
-    }
-    clock_mark(clk, kStRowsFwd, s);
-    PF_CUFFT(cufftSetStream(d.f2, s));
-    PF_CUFFT(cufftExecZ2Z(d.f2, d.U.as<cufftDoubleComplex>(), d.U.as<cufftDoubleComplex>(), dir));
-    clock_mark(clk, kStFft2Fwd, s);
-    PF_TRY(interp_any(g, d, f, B, s));
-    clock_mark(clk, kStInterp, s);
-    return 0;
+    return g.fp32 ? type2_impl<float>(g, d, modes, f, B, dir, s, clk)
+                  : type2_impl<double>(g, d, modes, f, B, dir, s, clk);
 }
 
 int nufft_type1(const NufftGrid& g, NufftDev& d, const double2* f, double2* modes, int B,
                 int iflag, cudaStream_t s, StageClock* clk) {
     const int dir = iflag > 0 ? CUFFT_INVERSE : CUFFT_FORWARD;
-    PF_CUDA(cudaMemsetAsync(d.U.p, 0, sizeof(double2) * (size_t)g.nrows * g.nf2 * B, s));
-    PF_TRY(spread_any(g, d, f, B, s));
-    clock_mark(clk, kStSpread, s);
-    PF_CUFFT(cufftSetStream(d.f2, s));
-    PF_CUFFT(cufftExecZ2Z(d.f2, d.U.as<cufftDoubleComplex>(), d.U.as<cufftDoubleComplex>(), dir));
-    clock_mark(clk, kStFft2Adj, s);
-    {
-        dim3 grid((g.ncols + 31) / 32, (g.nf1 + 31) / 32, B);
-        rows_adj_kernel<<<grid, dim3(32, 8), 0, s>>>(d.U.as<double2>(), g.nf1, g.ncols, g.row0,
-                                                     g.nrows, g.nf2, d.colp2.as<int>(),
-                                                     d.pad.as<double2>());
-        PF_TRY(check_launch("rows_adj_kernel"));
-    }
-    clock_mark(clk, kStRowsAdj, s);
-    PF_CUFFT(cufftSetStream(d.f1, s));
-    PF_CUFFT(cufftExecZ2Z(d.f1, d.pad.as<cufftDoubleComplex>(), d.pad.as<cufftDoubleComplex>(), dir));
-    clock_mark(clk, kStFft1Adj, s);
-    {
-        dim3 grid(nblk(g.n1, 256), g.ncols, B);
-        unpad_kernel<<<grid, 256, 0, s>>>(d.pad.as<double2>(), g.n1, g.ncols, g.nf1,
-                                          d.mult1.as<double2>(), d.dec2.as<double>(), modes);
-        PF_TRY(check_launch("unpad_kernel"));
-    }
-    clock_mark(clk, kStUnpad, s);
-    return 0;
+    return g.fp32 ? type1_impl<float>(g, d, f, modes, B, dir, s, clk)
+                  : type1_impl<double>(g, d, f, modes, B, dir, s, clk);
 }
 
 // ---------------------------------------------------------------------------------------
