@@ -41,7 +41,9 @@ typedef enum { PFSHT_METHOD_AUTO = 0, PFSHT_METHOD_STRETCH = 1, PFSHT_METHOD_DIR
 
 typedef enum {
     PFSHT_PRECISION_FP64 = 0,   /* plain form: FP64 everywhere */
-    PFSHT_PRECISION_MIXED = 1   /* FP64 recurrence + exponents; FP32 compensated ring sums and FP32 NUFFT */
+    PFSHT_PRECISION_MIXED = 1   /* FP64 recurrence + exponents; FP32 compensated ring sums and FP32 NUFFT.
+                                   Applies when tol >= 1e-6; a plan asked for it at a smaller tol runs
+                                   the FP64 form (pfsht_plan_info.precision says which). */
 } pfsht_precision;
 
 typedef enum { PFSHT_KIND_POLE = 0, PFSHT_KIND_INTERIOR = 1, PFSHT_KIND_FULL = 2, PFSHT_KIND_DIRECT = 3 } pfsht_kind;

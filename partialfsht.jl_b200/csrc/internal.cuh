@@ -77,12 +77,14 @@ struct RingTables {
     const double* log2sin = nullptr;  // nrings
     const double* log2c = nullptr;    // lmax + 1
     const double* w = nullptr;        // nrings window, or null for 1
-    const double2* ab = nullptr;      // recurrence coefficients, per m from l = m + 2
+    const double2* ab = nullptr;      // (beta_l, g_l) of the monic recurrence, per m from l = m + 2
     const int64_t* aboff = nullptr;   // lmax + 1 offsets into ab
-    const double2* ck_p = nullptr;    // saved recurrence state (P_{l-1}, P_{l-2}) at segment starts
+    const double2* ck_p = nullptr;    // saved monic state (q_{l-1}, q_{l-2}) at segment starts
     const int* ck_E = nullptr;        // and its block exponent
     int lmax = 0;
     int nrings = 0;
+    int mix = 0;       // FP32 accumulation (mixed form)
+    int stride = 64;   // renormalisation block in degrees: 64 (FP64), 16 (mixed)
 };
 
 // Degree segments of the ring pass: order m is walked as nseg[m] pieces that start on the
@@ -130,8 +132,8 @@ struct RingItemsOwner {
     RingItems view;
 };
 
-int build_ab_table(int lmax, int mmax, DevBuf& ab, DevBuf& aboff, cudaStream_t s);
-int launch_ab_table(int lmax, int mmax, const int64_t* aboff, double2* ab, cudaStream_t s);
+int build_ab_table(int lmax, int mmax, int stride, DevBuf& ab, DevBuf& aboff, cudaStream_t s);
+int launch_ab_table(int lmax, int mmax, int stride, const int64_t* aboff, double2* ab, cudaStream_t s);
 // items over the retained (m, ring) set, tiles of `tile` rings, split into the degree
 // segments of `seg` when given, heaviest first
 std::vector<RingItem> make_ring_items(const std::vector<int>& jlo, const std::vector<int>& jhi,

@@ -155,7 +155,7 @@ static int direct_forward_noalloc(const double* theta, const double* phi, int64_
     const unsigned grid = (unsigned)std::min<int64_t>((work + 255) / 256, 4096);
     noalloc_prep_kernel<<<grid, 256, 0, s>>>(theta, M, L, cos_t, log2sin, log2c, aboff, items, ntile);
     PF_TRY(check_launch("noalloc_prep_kernel"));
-    if (L >= 2) PF_TRY(launch_ab_table(L, L, aboff, ab, s));
+    if (L >= 2) PF_TRY(launch_ab_table(L, L, 64, aboff, ab, s));
     RingTables t;
     t.cos_t = cos_t;
     t.log2sin = log2sin;

@@ -259,7 +259,10 @@ int build_stretch(pfsht_plan* p, const double* d_theta, const double* d_phi, con
     PF_TRY(upload(p->log2sin, lf.log2sin, s));
     PF_TRY(upload(p->log2c, lf.log2c, s));
     PF_TRY(upload(p->w, lf.w, s));
-    PF_TRY(build_ab_table(L, lf.mmax, p->ab, p->aboff, s));
+    const bool mix = p->precision == PFSHT_PRECISION_MIXED;
+    PF_TRY(build_ab_table(L, lf.mmax, mix ? 16 : 64, p->ab, p->aboff, s));
+    p->rt.mix = mix;
+    p->rt.stride = mix ? 16 : 64;
     p->rt.cos_t = p->cos_t.as<double>();
     p->rt.log2sin = p->log2sin.as<double>();
     p->rt.log2c = p->log2c.as<double>();
@@ -306,6 +309,7 @@ int build_stretch(pfsht_plan* p, const double* d_theta, const double* d_phi, con
     for (int c = 0; c < p->ncols; ++c) colk2[c] = c - lf.mmax;
     PF_TRY(setup_nufft_grid(p->ng, p->nd, lf.nth, lf.nph, colk2, phase, p->tol, p->M, Tmin, Tmax,
                             false, o.nufft_bin_rows, o.nufft_bin_cols, s));
+    p->ng.fp32 = p->precision == PFSHT_PRECISION_MIXED;
     PF_TRY(nufft_setpts(p->ng, p->nd, Th.as<double>(), ph.as<double>(), s));
     PF_TRY(nufft_alloc(p->ng, p->nd, B));
     return 0;
@@ -331,7 +335,10 @@ int build_direct(pfsht_plan* p, const double* h_theta, const double* h_phi, cuda
     PF_TRY(upload(p->log2sin, l2s, s));
     PF_TRY(upload(p->log2c, l2c, s));
     PF_TRY(upload(p->phi_pts, ph, s));
-    PF_TRY(build_ab_table(L, L, p->ab, p->aboff, s));
+    const bool mix = p->precision == PFSHT_PRECISION_MIXED;
+    PF_TRY(build_ab_table(L, L, mix ? 16 : 64, p->ab, p->aboff, s));
+    p->rt.mix = mix;
+    p->rt.stride = mix ? 16 : 64;
     p->rt.cos_t = p->cos_t.as<double>();
     p->rt.log2sin = p->log2sin.as<double>();
     p->rt.log2c = p->log2c.as<double>();
@@ -378,7 +385,10 @@ int plan_create(const double* theta, const double* phi, int64_t npts, int lmax, 
 
     std::unique_ptr<pfsht_plan> p(new pfsht_plan());
     p->device = dev;
-    p->precision = precision;
+    // the mixed form applies where the tolerance allows FP32 (tol >= 1e-6); below that the
+    // plan runs the FP64 form and reports so in its info
+    p->precision = (precision == PFSHT_PRECISION_MIXED && tol >= 1e-6) ? PFSHT_PRECISION_MIXED
+                                                                        : PFSHT_PRECISION_FP64;
     p->L = lmax;
     p->B = ntrans;
     p->M = npts;

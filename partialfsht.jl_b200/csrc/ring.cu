@@ -2,81 +2,105 @@
 // alm_from_rings! (PartialFSHT.jl src/Legendre.jl:310-542; device analogue of
 // ext/PartialFSHTKernelAbstractionsExt.jl:86-230).
 //
-// Work decomposition: one warp per item (order m, tile of consecutive retained rings); a
-// lane owns R rings (ring j0 + lane + 32 r, R = ceil(tile / 32) chosen per item) and keeps
-// their two-term recurrence state and block-scaling exponent in registers. The recurrence
-// is the reference's
+// Work decomposition: one warp per item (order m, tile of consecutive retained rings, range of
+// degrees); a lane owns R rings (ring j0 + lane + 32 r) and keeps their two-term recurrence
+// state and block-scaling exponent in registers. The recurrence is the reference's
 //     P_m^m = (-1)^m 2^(m log2 sin + log2 c_m),   P_{m+1}^m = sqrt(2m+3) cos P_m^m,
-//     P_l^m = a_l^m cos P_{l-1}^m - b_l^m P_{l-2}^m
-// renormalised every 64 degrees (src/Legendre.jl:16,455-459). Each ring keeps its own
-// exponent (as the KernelAbstractions kernel does), so no chunk headroom rule is needed.
-// a_l^m, b_l^m come from a plan-time table built on the device with the reference's exact
-// expressions. Per chunk of 32 degrees a warp stages them and the coefficients a_{l,+-m}
-// in shared memory; the chunk is walked in fixed, fully unrolled blocks of degrees with no
-// branch inside a block, so successive degrees overlap in the pipeline; renormalisation
-// falls on block boundaries because 64 is a multiple of the block.
+//     P_l^m = a_l^m cos P_{l-1}^m - b_l^m P_{l-2}^m,
+// run in monic form inside blocks of `stride` degrees from l = m + 2: P_l = g_l q_l with
+// g_l = a_lb ... a_l over the block's degrees so far, and
+//     q_l = cos q_{l-1} - beta_l q_{l-2},   beta_l = b_l / (a_l a_{l-1})   (a_{m+1} = sqrt(2m+3)),
+// two FP64 operations per (ring, degree) instead of three. The per-degree g_l multiplies the
+// coefficients (forward) or the reduced sums (adjoint), shared by all rings. A block enters with
+// (q_{lb-1}, q_{lb-2}) = (P_{lb-1}, a_{lb-1} P_{lb-2}) and leaves multiplied by g of its last
+// degree, at which point the state is renormalised by a power of two (src/Legendre.jl:16,
+// 455-459: every 64 degrees in the FP64 form; every 16 in the mixed form, so the values stay
+// inside the FP32 range). Each ring keeps its own exponent, as the KernelAbstractions kernel
+// does (ext/PartialFSHTKernelAbstractionsExt.jl:96-99).
 //
-// Forward: acc(ring, +-m) += a_{l,+-m} P_l^m, written once per ring, windowed and, for a
+// Forward: acc(ring, +-m) += a_{l,+-m} P_l, written once per ring, windowed and, for a
 // pole/full periodisation, mirrored into the DFS row with sign (-1)^m (src/DFS.jl:26). The
 // first tile of each order also writes the zeros of the rings the order does not retain.
 // Adjoint: each lane sums P_l^m g_j over its R rings; per block of degrees the lanes' partial
 // sums are transposed through shared memory and each lane reduces one (degree, component)
 // over the 32 lanes. An order covered by a single tile stores its coefficients; an order
 // split over several tiles adds them atomically (into zeros).
+//
+// Mixed form (MIX): the recurrence and exponents stay FP64; the forward accumulates in FP32
+// with paired (float2) FMAs over blocks of 8 degrees and adds each block into a compensated
+// (two-sum) FP32 total; the adjoint keeps the ring data in FP32 and reduces in FP32.
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 
 #include "internal.cuh"
 
 namespace pf {
 
-static constexpr int kWarpsPerBlock = 4;
-static constexpr int kStride = 64;  // _RESCALE_STRIDE (src/Legendre.jl:16)
+static constexpr int kWarpsPerBlock = 4;  // forward
+static constexpr int kAdjWarps = 2;       // adjoint
 
 // ---------------------------------------------------------------------------------------
-// recurrence coefficient table, exact expressions of src/Legendre.jl:406-408
+// recurrence coefficient table (beta_l, g_l), from the exact expressions of
+// src/Legendre.jl:406-408
 // ---------------------------------------------------------------------------------------
-__global__ void ab_table_kernel(int L, int mmax, const int64_t* __restrict__ aboff,
+__device__ __forceinline__ double rec_a(int l, int m) {
+    if (l == m + 1) return sqrt((double)(2 * m + 3));
+    return sqrt((double)(2 * l - 1) * (double)(2 * l + 1) / ((double)(l - m) * (double)(l + m)));
+}
+__device__ __forceinline__ double rec_b(int l, int m) {
+    return sqrt((double)(2 * l + 1) / (double)(2 * l - 3) * (double)(l - m - 1) / (double)(l - m) *
+                (double)(l + m - 1) / (double)(l + m));
+}
+
+// one thread per (order, block of `stride` degrees)
+__global__ void ab_table_kernel(int L, int mmax, int stride, const int64_t* __restrict__ aboff,
                                 double2* __restrict__ ab) {
     const int m = blockIdx.y;
-    if (m > mmax) return;
-    const int n = L - m - 1;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int l = m + 2 + i;
-        const double a = sqrt((double)(2 * l - 1) * (double)(2 * l + 1) /
-                              ((double)(l - m) * (double)(l + m)));
-        const double b = sqrt((double)(2 * l + 1) / (double)(2 * l - 3) * (double)(l - m - 1) /
-                              (double)(l - m) * (double)(l + m - 1) / (double)(l + m));
-        ab[aboff[m] + i] = make_double2(a, b);
+    if (m > mmax || L < m + 2) return;
+    const int nblk = (L - m - 1 + stride - 1) / stride;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nblk; k += gridDim.x * blockDim.x) {
+        const int lb = m + 2 + k * stride;
+        const int le = min(L, lb + stride - 1);
+        double aprev = rec_a(lb - 1, m);
+        double g = 1.0;
+        for (int l = lb; l <= le; ++l) {
+            const double a = rec_a(l, m), b = rec_b(l, m);
+            g *= a;
+            ab[aboff[m] + (l - m - 2)] = make_double2(b / (a * aprev), g);
+            aprev = a;
+        }
     }
 }
 
-int build_ab_table(int L, int mmax, DevBuf& ab, DevBuf& aboff, cudaStream_t s) {
-    std::vector<int64_t> off(L + 1, 0);
-    int64_t tot = 0;
+static void ab_offsets(int L, int mmax, std::vector<int64_t>& off, int64_t& tot) {
+    off.assign(L + 1, 0);
+    tot = 0;
     for (int m = 0; m <= L; ++m) {
         off[m] = tot;
         if (m <= mmax) tot += std::max(0, L - m - 1);
     }
+}
+
+int launch_ab_table(int L, int mmax, int stride, const int64_t* aboff, double2* ab, cudaStream_t s) {
+    const int nblk = (L + stride) / stride + 1;
+    dim3 grid((unsigned)((nblk + 31) / 32), (unsigned)(mmax + 1));
+    ab_table_kernel<<<grid, 32, 0, s>>>(L, mmax, stride, aboff, ab);
+    return check_launch("ab_table_kernel");
+}
+
+int build_ab_table(int L, int mmax, int stride, DevBuf& ab, DevBuf& aboff, cudaStream_t s) {
+    std::vector<int64_t> off;
+    int64_t tot;
+    ab_offsets(L, mmax, off, tot);
     PF_TRY(aboff.alloc(sizeof(int64_t) * (L + 1)));
     PF_TRY(ab.alloc(sizeof(double2) * std::max<int64_t>(tot, 1)));
     PF_CUDA(cudaMemcpyAsync(aboff.p, off.data(), sizeof(int64_t) * (L + 1),
                             cudaMemcpyHostToDevice, s));
-    if (tot > 0) {
-        dim3 grid((unsigned)std::min(64, (L + 255) / 256 + 1), (unsigned)(mmax + 1));
-        ab_table_kernel<<<grid, 256, 0, s>>>(L, mmax, aboff.as<int64_t>(), ab.as<double2>());
-        PF_TRY(check_launch("ab_table_kernel"));
-    }
+    if (tot > 0) PF_TRY(launch_ab_table(L, mmax, stride, aboff.as<int64_t>(), ab.as<double2>(), s));
     // the host vector must outlive the async copy
     PF_CUDA(cudaStreamSynchronize(s));
     return 0;
-}
-
-// the coefficient-table kernel on caller-provided offsets and storage (no allocation)
-int launch_ab_table(int L, int mmax, const int64_t* aboff, double2* ab, cudaStream_t s) {
-    dim3 grid((unsigned)std::min(64, (L + 255) / 256 + 1), (unsigned)(mmax + 1));
-    ab_table_kernel<<<grid, 256, 0, s>>>(L, mmax, aboff, ab);
-    return check_launch("ab_table_kernel");
 }
 
 std::vector<RingItem> make_ring_items(const std::vector<int>& jlo, const std::vector<int>& jhi,
@@ -121,12 +145,6 @@ __device__ __forceinline__ int ceil_log2(double mx) {
     return f == 0.5 ? e - 1 : e;
 }
 
-__device__ __forceinline__ double2 cmad(double2 acc, double2 a, double p) {
-    acc.x = fma(a.x, p, acc.x);
-    acc.y = fma(a.y, p, acc.y);
-    return acc;
-}
-
 // seed of ring j for order m (src/Legendre.jl:379-382, exponent per ring as in
 // ext/PartialFSHTKernelAbstractionsExt.jl:96-99)
 __device__ __forceinline__ void ring_seed(const RingTables& t, int m, int j, double sgn,
@@ -142,23 +160,16 @@ __device__ __forceinline__ void ring_seed(const RingTables& t, int m, int j, dou
     }
 }
 
-__device__ __forceinline__ void ring_renorm(double& p1, double& p2, int& E) {
-    const double mx = fmax(fabs(p1), fabs(p2));
-    if (mx > 0.0 && isfinite(mx)) {
-        const int s = ceil_log2(mx);
-        if (s != 0) {
-            const double f = scalbn(1.0, -s);
-            p1 *= f;
-            p2 *= f;
-            E += s;
-        }
-    }
+// power-of-two exponent that brings max(|q1|, |q2|) into (1/2, 1]; 0 when nothing to do
+__device__ __forceinline__ int renorm_shift(double q1, double q2) {
+    const double mx = fmax(fabs(q1), fabs(q2));
+    return (mx > 0.0 && isfinite(mx)) ? ceil_log2(mx) : 0;
 }
 
 // ---------------------------------------------------------------------------------------
-// plan-time recurrence checkpoints: one thread per (order, ring) walks the same recurrence
-// and renormalisation schedule as the apply kernels and saves (P_{l-1}, P_{l-2}, E) at the
-// first degree l of every later segment
+// plan-time recurrence checkpoints: one thread per (order, ring) walks the same monic
+// recurrence, block conversions and renormalisations as the apply kernels and saves
+// (q_{l-1}, q_{l-2}, E) at the first degree l of every later segment
 // ---------------------------------------------------------------------------------------
 struct CkptJob {
     int m, j0, n, nseg, nblk;
@@ -174,10 +185,11 @@ __global__ void ring_ckpt_kernel(RingTables t, const CkptJob* __restrict__ jobs,
     if (k >= jb.n) return;
     const int m = jb.m, L = t.lmax, j = jb.j0 + k;
     const double sgn = (m & 1) ? -1.0 : 1.0;
-    double x, p1, p2;
+    double x, p2;
     int E;
     ring_seed(t, m, j, sgn, x, p2, E);
-    p1 = sqrt((double)(2 * m + 3)) * x * p2;
+    const double s23 = sqrt((double)(2 * m + 3));
+    double q1 = s23 * x * p2, q2 = s23 * p2;
     const double2* abm = t.ab + t.aboff[m];
     int s = 1;
     int lnext = m + 2 + 64 * (int)(((int64_t)jb.nblk) / jb.nseg);
@@ -185,18 +197,28 @@ __global__ void ring_ckpt_kernel(RingTables t, const CkptJob* __restrict__ jobs,
     for (int l = m + 2; l <= L; ++l) {
         if (l == lnext) {
             const int64_t idx = jb.ck + (int64_t)(s - 1) * jb.stride + k;
-            ckp[idx] = make_double2(p1, p2);
+            ckp[idx] = make_double2(q1, q2);
             ckE[idx] = E;
             if (++s == jb.nseg) break;
             lnext = m + 2 + 64 * (int)(((int64_t)s * jb.nblk) / jb.nseg);
         }
-        const double2 ab = abm[l - m - 2];
-        const double p = fma(ab.x * x, p1, -(ab.y * p2));
-        p2 = p1;
-        p1 = p;
-        if (++steps == kStride) {
+        const double2 bg = abm[l - m - 2];
+        const double qn = fma(x, q1, -(bg.x * q2));
+        q2 = q1;
+        q1 = qn;
+        if (++steps == t.stride) {
             steps = 0;
-            if (l < L) ring_renorm(p1, p2, E);
+            if (l < L) {
+                q1 *= bg.y;
+                q2 *= bg.y;
+                const int sh = renorm_shift(q1, q2);
+                if (sh != 0) {
+                    const double f = scalbn(1.0, -sh);
+                    q1 *= f;
+                    q2 *= f;
+                    E += sh;
+                }
+            }
         }
     }
 }
@@ -250,18 +272,74 @@ int build_ring_segments(const RingTables& t, const std::vector<int>& jlo,
 // ---------------------------------------------------------------------------------------
 // forward: alm -> ring columns
 // ---------------------------------------------------------------------------------------
-template <int NB>
+template <bool MIX> using CoefT = std::conditional_t<MIX, float2, double2>;
+
+template <int NB, bool MIX>
 struct FwdSmem {
-    double2 ab[kWarpsPerBlock][32];
-    double2 ap[kWarpsPerBlock][NB][32];
-    double2 am[kWarpsPerBlock][NB][32];
+    double2 bg[kWarpsPerBlock][32];               // (beta_l, g_l) of the chunk's degrees
+    CoefT<MIX> ap[kWarpsPerBlock][NB][32];        // g_l a_{l,+m}
+    CoefT<MIX> am[kWarpsPerBlock][NB][32];        // g_l (-1)^m a_{l,-m}
 };
 
-template <int R, int NB>
+// accumulator of one (ring, +-m, transform): FP64, or FP32 blocks into a two-sum total
+template <bool MIX> struct FwdAcc;
+template <> struct FwdAcc<false> {
+    double2 a;
+    __device__ __forceinline__ void zero() { a = make_double2(0.0, 0.0); }
+    __device__ __forceinline__ void add(double2 c, double p) {
+        a.x = fma(c.x, p, a.x);
+        a.y = fma(c.y, p, a.y);
+    }
+    __device__ __forceinline__ void fold() {}
+    __device__ __forceinline__ void scale(double f) {
+        a.x *= f;
+        a.y *= f;
+    }
+    __device__ __forceinline__ double2 total() const { return a; }
+};
+template <> struct FwdAcc<true> {
+    float2 blk, s, c;
+    __device__ __forceinline__ void zero() {
+        blk = s = c = make_float2(0.f, 0.f);
+    }
+    __device__ __forceinline__ void add(float2 cf, float p) {
+        blk = __ffma2_rn(cf, make_float2(p, p), blk);
+    }
+    // s + blk as a two-sum: the rounding error of each block's addition is kept in c
+    __device__ __forceinline__ void fold() {
+        const float2 t = __fadd2_rn(s, blk);
+        const float2 bp = __fadd2_rn(t, make_float2(-s.x, -s.y));
+        const float2 sa = __fadd2_rn(t, make_float2(-bp.x, -bp.y));
+        const float2 e = __fadd2_rn(__fadd2_rn(s, make_float2(-sa.x, -sa.y)),
+                                    __fadd2_rn(blk, make_float2(-bp.x, -bp.y)));
+        c = __fadd2_rn(c, e);
+        s = t;
+        blk = make_float2(0.f, 0.f);
+    }
+    __device__ __forceinline__ void scale(double f) {
+        const float2 ff = make_float2((float)f, (float)f);
+        blk = __fmul2_rn(blk, ff);
+        s = __fmul2_rn(s, ff);
+        c = __fmul2_rn(c, ff);
+    }
+    __device__ __forceinline__ double2 total() const {
+        return make_double2((double)s.x + ((double)c.x + (double)blk.x),
+                            (double)s.y + ((double)c.y + (double)blk.y));
+    }
+};
+
+template <bool MIX>
+__device__ __forceinline__ CoefT<MIX> to_coef(double2 v) {
+    if constexpr (MIX) return make_float2((float)v.x, (float)v.y);
+    else return v;
+}
+
+template <int R, int NB, bool MIX>
 __device__ __forceinline__ void ring_fwd_item(const RingTables& t, const RingOut& o,
                                               const RingItem& item, const double2* __restrict__ alm,
-                                              double2* __restrict__ out, int b0, FwdSmem<NB>& sm,
-                                              int warp, int lane) {
+                                              double2* __restrict__ out, int b0,
+                                              FwdSmem<NB, MIX>& sm, int warp, int lane) {
+    constexpr int STRIDE = MIX ? 16 : 64;
     const int m = item.m, L = t.lmax;
     const double sgn = (m & 1) ? -1.0 : 1.0;
     const int64_t albs = (int64_t)(L + 1) * (2 * L + 1);
@@ -270,77 +348,125 @@ __device__ __forceinline__ void ring_fwd_item(const RingTables& t, const RingOut
     const double2* abm = t.ab + t.aboff[m];
     const double2 zero2 = make_double2(0.0, 0.0);
 
-    double x[R], p1[R], p2[R];
+    double x[R], q1[R], q2[R];
     int E[R];
-    double2 accp[R][NB], accm[R][NB];
+    FwdAcc<MIX> accp[R][NB], accm[R][NB];
+    const bool seeded = item.ck < 0;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int k = lane + 32 * r;
         x[r] = 0.0;
-        p1[r] = 0.0;
-        p2[r] = 0.0;
+        q1[r] = 0.0;
+        q2[r] = 0.0;
         E[r] = 0;
-        if (k < item.n) ring_seed(t, m, item.j0 + k, sgn, x[r], p2[r], E[r]);
+        if (k < item.n) {
+            if (seeded) {
+                ring_seed(t, m, item.j0 + k, sgn, x[r], q2[r], E[r]);
+            } else {
+                x[r] = t.cos_t[item.j0 + k];
+                const double2 c = t.ck_p[item.ck + k];
+                q1[r] = c.x;
+                q2[r] = c.y;
+                E[r] = t.ck_E[item.ck + k];
+            }
+        }
 #pragma unroll
         for (int b = 0; b < NB; ++b) {
-            accp[r][b] = zero2;
-            accm[r][b] = zero2;
+            accp[r][b].zero();
+            accm[r][b].zero();
         }
     }
-    // l = m: P = seed
-#pragma unroll
-    for (int b = 0; b < NB; ++b) {
-        const double2 ap = colp[albs * b];
-        double2 am = m > 0 ? colm[albs * b] : zero2;
-        am.x *= sgn;
-        am.y *= sgn;
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            accp[r][b] = cmad(accp[r][b], ap, p2[r]);
-            accm[r][b] = cmad(accm[r][b], am, p2[r]);
-        }
-    }
-    if (m < L) {
-        const double s23 = sqrt((double)(2 * m + 3));
-#pragma unroll
-        for (int r = 0; r < R; ++r) p1[r] = s23 * x[r] * p2[r];
+    // add a_{l,+-m} P for degree l (true P values, the first two degrees)
+    auto add_true = [&](int l, const double (&P)[R]) {
 #pragma unroll
         for (int b = 0; b < NB; ++b) {
-            const double2 ap = colp[1 + albs * b];
-            double2 am = m > 0 ? colm[1 + albs * b] : zero2;
+            const double2 ap = colp[(l - m) + albs * b];
+            double2 am = m > 0 ? colm[(l - m) + albs * b] : zero2;
             am.x *= sgn;
             am.y *= sgn;
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-                accp[r][b] = cmad(accp[r][b], ap, p1[r]);
-                accm[r][b] = cmad(accm[r][b], am, p1[r]);
-            }
-        }
-        auto step = [&](int i) {
-            const double2 ab = sm.ab[warp][i];
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const double p = fma(ab.x * x[r], p1[r], -(ab.y * p2[r]));
-                p2[r] = p1[r];
-                p1[r] = p;
-            }
-#pragma unroll
-            for (int b = 0; b < NB; ++b) {
-                const double2 ap = sm.ap[warp][b][i];
-                const double2 am = sm.am[warp][b][i];
-#pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    accp[r][b] = cmad(accp[r][b], ap, p1[r]);
-                    accm[r][b] = cmad(accm[r][b], am, p1[r]);
+                if constexpr (MIX) {
+                    accp[r][b].add(to_coef<MIX>(ap), (float)P[r]);
+                    accm[r][b].add(to_coef<MIX>(am), (float)P[r]);
+                } else {
+                    accp[r][b].add(ap, P[r]);
+                    accm[r][b].add(am, P[r]);
                 }
             }
-        };
-        int steps = 0;
+        }
+    };
+    int lstart = item.lbeg;
+    if (seeded) {
+        add_true(m, q2);  // l = m
+        if (m < L) {
+            const double s23 = sqrt((double)(2 * m + 3));
+            double p1[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) p1[r] = s23 * x[r] * q2[r];
+            add_true(m + 1, p1);  // l = m + 1
+            // enter the monic form at l = m + 2: (q1, q2) = (P_{m+1}, a_{m+1} P_m)
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                q2[r] = s23 * q2[r];
+                q1[r] = p1[r];
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+#pragma unroll
+            for (int b = 0; b < NB; ++b) {
+                accp[r][b].fold();
+                accm[r][b].fold();
+            }
+        lstart = m + 2;
+    }
+    auto step = [&](int i) {
+        const double beta = sm.bg[warp][i].x;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const double qn = fma(x[r], q1[r], -(beta * q2[r]));
+            q2[r] = q1[r];
+            q1[r] = qn;
+        }
+        float pf[R];
+        if constexpr (MIX) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) pf[r] = (float)q1[r];
+        }
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            const CoefT<MIX> ap = sm.ap[warp][b][i];
+            const CoefT<MIX> am = sm.am[warp][b][i];
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                if constexpr (MIX) {
+                    accp[r][b].add(ap, pf[r]);
+                    accm[r][b].add(am, pf[r]);
+                } else {
+                    accp[r][b].add(ap, q1[r]);
+                    accm[r][b].add(am, q1[r]);
+                }
+            }
+        }
+    };
+    auto fold_all = [&]() {
+        if constexpr (MIX) {
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+#pragma unroll
+                for (int b = 0; b < NB; ++b) {
+                    accp[r][b].fold();
+                    accm[r][b].fold();
+                }
+        }
+    };
+    if (lstart <= item.lend) {
         // the coefficients of the next 32 degrees are loaded while this chunk runs
-        double2 ab_n = zero2, ap_n[NB], am_n[NB];
+        double2 bg_n = zero2, ap_n[NB], am_n[NB];
         auto fetch = [&](int l) {
-            if (l <= L) {
-                ab_n = abm[l - m - 2];
+            if (l <= item.lend) {
+                bg_n = abm[l - m - 2];
 #pragma unroll
                 for (int b = 0; b < NB; ++b) {
                     ap_n[b] = colp[(l - m) + albs * b];
@@ -350,16 +476,19 @@ __device__ __forceinline__ void ring_fwd_item(const RingTables& t, const RingOut
         };
 #pragma unroll
         for (int b = 0; b < NB; ++b) ap_n[b] = am_n[b] = zero2;
-        fetch(m + 2 + lane);
-        for (int l0 = m + 2; l0 <= L; l0 += 32) {
-            const int nl = min(32, L - l0 + 1);
+        fetch(lstart + lane);
+        int steps = 0;
+        for (int l0 = lstart; l0 <= item.lend; l0 += 32) {
+            const int nl = min(32, item.lend - l0 + 1);
             __syncwarp();
             if (lane < nl) {
-                sm.ab[warp][lane] = ab_n;
+                const double g = bg_n.y;
+                sm.bg[warp][lane] = bg_n;
 #pragma unroll
                 for (int b = 0; b < NB; ++b) {
-                    sm.ap[warp][b][lane] = ap_n[b];
-                    sm.am[warp][b][lane] = make_double2(am_n[b].x * sgn, am_n[b].y * sgn);
+                    sm.ap[warp][b][lane] = to_coef<MIX>(make_double2(ap_n[b].x * g, ap_n[b].y * g));
+                    const double gs = g * sgn;
+                    sm.am[warp][b][lane] = to_coef<MIX>(make_double2(am_n[b].x * gs, am_n[b].y * gs));
                 }
             }
             __syncwarp();
@@ -368,34 +497,35 @@ __device__ __forceinline__ void ring_fwd_item(const RingTables& t, const RingOut
             for (int blk = 0; blk < nblk; ++blk) {
 #pragma unroll
                 for (int i = 0; i < 8; ++i) step(blk * 8 + i);
+                fold_all();
                 steps += 8;
-                if (steps == kStride) {
+                if (steps == STRIDE) {
                     steps = 0;
                     if (l0 + blk * 8 + 7 < L) {
+                        // leave the block: scale the state by g of its last degree, renormalise
+                        const double G = sm.bg[warp][blk * 8 + 7].y;
 #pragma unroll
                         for (int r = 0; r < R; ++r) {
-                            const double mx = fmax(fabs(p1[r]), fabs(p2[r]));
-                            if (mx > 0.0 && isfinite(mx)) {
-                                const int s = ceil_log2(mx);
-                                if (s != 0) {
-                                    const double f = scalbn(1.0, -s);
-                                    p1[r] *= f;
-                                    p2[r] *= f;
+                            q1[r] *= G;
+                            q2[r] *= G;
+                            const int sh = renorm_shift(q1[r], q2[r]);
+                            if (sh != 0) {
+                                const double f = scalbn(1.0, -sh);
+                                q1[r] *= f;
+                                q2[r] *= f;
 #pragma unroll
-                                    for (int b = 0; b < NB; ++b) {
-                                        accp[r][b].x *= f;
-                                        accp[r][b].y *= f;
-                                        accm[r][b].x *= f;
-                                        accm[r][b].y *= f;
-                                    }
-                                    E[r] += s;
+                                for (int b = 0; b < NB; ++b) {
+                                    accp[r][b].scale(f);
+                                    accm[r][b].scale(f);
                                 }
+                                E[r] += sh;
                             }
                         }
                     }
                 }
             }
             for (int i = nblk * 8; i < nl; ++i) step(i);
+            fold_all();
         }
     }
     // write the ring columns (window and 2^E folded into one exact scale)
@@ -409,8 +539,9 @@ __device__ __forceinline__ void ring_fwd_item(const RingTables& t, const RingOut
 #pragma unroll
         for (int b = 0; b < NB; ++b) {
             double2* ob = out + o.bstride * (b0 + b);
-            const double2 gp = make_double2(accp[r][b].x * sc, accp[r][b].y * sc);
-            const double2 gm = make_double2(accm[r][b].x * sc, accm[r][b].y * sc);
+            const double2 tp = accp[r][b].total(), tm = accm[r][b].total();
+            const double2 gp = make_double2(tp.x * sc, tp.y * sc);
+            const double2 gm = make_double2(tm.x * sc, tm.y * sc);
             ob[j + o.ld * (o.col_off + m)] = gp;
             if (m > 0) ob[j + o.ld * (o.col_off - m)] = gm;
             if (o.reflect) {
@@ -444,12 +575,12 @@ __device__ __forceinline__ void ring_fwd_zero_rest(const RingOut& o, const RingI
     }
 }
 
-template <int RMAX, int NB>
+template <int RMAX, int NB, bool MIX>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32)
 ring_fwd_kernel(RingTables t, RingOut o, const RingItem* __restrict__ items, int nitems,
                 const int* __restrict__ jlo, const int* __restrict__ jhi,
                 const double2* __restrict__ alm, double2* __restrict__ out, int b0) {
-    __shared__ FwdSmem<NB> sm;
+    __shared__ FwdSmem<NB, MIX> sm;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int it = blockIdx.x * kWarpsPerBlock + warp;
     if (it >= nitems) return;
@@ -460,38 +591,40 @@ ring_fwd_kernel(RingTables t, RingOut o, const RingItem* __restrict__ items, int
         RingItem sub = item;
         sub.j0 = item.j0 + base;
         sub.n = min(32 * RMAX, item.n - base);
+        if (sub.ck >= 0) sub.ck += base;
         const int reff = (sub.n + 31) >> 5;
-        if (RMAX >= 4 && reff >= 3) ring_fwd_item<(RMAX >= 4 ? 4 : 1), NB>(t, o, sub, alm, out, b0, sm, warp, lane);
-        else if (RMAX >= 2 && reff == 2) ring_fwd_item<(RMAX >= 2 ? 2 : 1), NB>(t, o, sub, alm, out, b0, sm, warp, lane);
-        else ring_fwd_item<1, NB>(t, o, sub, alm, out, b0, sm, warp, lane);
+        if (RMAX >= 4 && reff >= 3) ring_fwd_item<(RMAX >= 4 ? 4 : 1), NB, MIX>(t, o, sub, alm, out, b0, sm, warp, lane);
+        else if (RMAX >= 2 && reff == 2) ring_fwd_item<(RMAX >= 2 ? 2 : 1), NB, MIX>(t, o, sub, alm, out, b0, sm, warp, lane);
+        else ring_fwd_item<1, NB, MIX>(t, o, sub, alm, out, b0, sm, warp, lane);
     }
 }
 
 // ---------------------------------------------------------------------------------------
 // adjoint: ring columns -> alm
 // ---------------------------------------------------------------------------------------
-// Two warps per block. With kAdjPipelined each warp double-buffers its reduction area, so
-// one block's partial sums are reduced while the next block's degrees are computed; without
-// it a block is reduced as soon as it is staged (half the shared memory per warp).
-static constexpr int kAdjWarps = 2;
-static constexpr bool kAdjPipelined = false;
-#ifdef PF_ADJ_MIN_BLOCKS
-#define PF_ADJ_BOUNDS __launch_bounds__(kAdjWarps * 32, PF_ADJ_MIN_BLOCKS)
-#else
-#define PF_ADJ_BOUNDS __launch_bounds__(kAdjWarps * 32)
-#endif
+template <bool MIX> using RedT = std::conditional_t<MIX, float, double>;
+template <bool MIX> using RingDataT = std::conditional_t<MIX, float2, double2>;
+
+template <bool MIX>
 struct AdjSmem {
-    double red[kAdjWarps][kAdjPipelined ? 2 : 1][32][33];
-    double2 ab[kAdjWarps][32];
+    RedT<MIX> red[kAdjWarps][32][33];
+    double2 bg[kAdjWarps][32];
 };
 
-template <int R, int NB>
+template <int R, int NB, bool MIX>
 __device__ __forceinline__ void ring_adj_item(const RingTables& t, const RingOut& o,
                                               const RingItem& item, const double2* __restrict__ in,
                                               double* __restrict__ almd, int b0, bool sole,
-                                              AdjSmem& sm, int warp, int lane) {
+                                              AdjSmem<MIX>& sm, int warp, int lane) {
+    constexpr int STRIDE = MIX ? 16 : 64;
     constexpr int NV = 4 * NB;   // (+m re, +m im, -m re, -m im) per transform
     constexpr int LB = 32 / NV;  // degrees per reduction block
+    // the scaled ring data g w 2^E stay normal (exactly rescalable) above kMinE, and round to
+    // zero below kZeroE for any input smaller than 2^9 (mixed) or 2^125 (FP64)
+    constexpr int kMinE = MIX ? -100 : -900;
+    constexpr int kZeroE = MIX ? -160 : -1200;
+    using GD = RingDataT<MIX>;
+    using RT = RedT<MIX>;
     const int m = item.m, L = t.lmax;
     const double sgn = (m & 1) ? -1.0 : 1.0;
     const double smir = o.spin_sgn * sgn;
@@ -500,19 +633,23 @@ __device__ __forceinline__ void ring_adj_item(const RingTables& t, const RingOut
     const int64_t cp = (int64_t)(L + 1) * (2 * m);
     const int64_t cm = (int64_t)(L + 1) * (m > 0 ? 2 * m - 1 : 0);
 
-    double x[R], p1[R], p2[R];
+    double x[R], q1[R], q2[R];
     int E[R];
-    double2 gp[R][NB], gm[R][NB];
+    GD gp[R][NB], gm[R][NB];
+    auto put = [&](double a, double b) -> GD {
+        if constexpr (MIX) return make_float2((float)a, (float)b);
+        else return make_double2(a, b);
+    };
     // ring data for (ring r, transform b): folded, windowed, scaled by 2^E; the -m column
     // carries the (-1)^m of src/Legendre.jl:511
     auto load_g = [&](int r) {
         const int k = lane + 32 * r;
 #pragma unroll
         for (int b = 0; b < NB; ++b) {
-            gp[r][b] = make_double2(0.0, 0.0);
-            gm[r][b] = make_double2(0.0, 0.0);
+            gp[r][b] = put(0.0, 0.0);
+            gm[r][b] = put(0.0, 0.0);
         }
-        if (k >= item.n) return;
+        if (k >= item.n || E[r] < kZeroE) return;
         const int j = item.j0 + k;
         const double sc = scalbn(t.w ? t.w[j] : 1.0, E[r]);
 #pragma unroll
@@ -524,7 +661,7 @@ __device__ __forceinline__ void ring_adj_item(const RingTables& t, const RingOut
                 v.x += smir * u.x;
                 v.y += smir * u.y;
             }
-            gp[r][b] = make_double2(v.x * sc, v.y * sc);
+            gp[r][b] = put(v.x * sc, v.y * sc);
             if (m > 0) {
                 double2 u = ib[j + o.ld * (o.col_off - m)];
                 if (o.reflect) {
@@ -532,7 +669,7 @@ __device__ __forceinline__ void ring_adj_item(const RingTables& t, const RingOut
                     u.x += smir * q.x;
                     u.y += smir * q.y;
                 }
-                gm[r][b] = make_double2(u.x * sc * sgn, u.y * sc * sgn);
+                gm[r][b] = put(u.x * sc * sgn, u.y * sc * sgn);
             }
         }
     };
@@ -541,215 +678,190 @@ __device__ __forceinline__ void ring_adj_item(const RingTables& t, const RingOut
     for (int r = 0; r < R; ++r) {
         const int k = lane + 32 * r;
         x[r] = 0.0;
-        p1[r] = 0.0;
-        p2[r] = 0.0;
+        q1[r] = 0.0;
+        q2[r] = 0.0;
         E[r] = 0;
         if (k < item.n) {
             if (seeded) {
-                ring_seed(t, m, item.j0 + k, sgn, x[r], p2[r], E[r]);
+                ring_seed(t, m, item.j0 + k, sgn, x[r], q2[r], E[r]);
             } else {
                 x[r] = t.cos_t[item.j0 + k];
                 const double2 c = t.ck_p[item.ck + k];
-                p1[r] = c.x;
-                p2[r] = c.y;
+                q1[r] = c.x;
+                q2[r] = c.y;
                 E[r] = t.ck_E[item.ck + k];
             }
         }
         load_g(r);
     }
-    int cur = 0;     // reduction buffer the current block stages into
-    int pend = -1;   // first degree of the block waiting in buffer cur ^ 1 (-1: none)
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;  // this lane's sums of the pending block
     // partial sums over this lane's rings for degree slot `slot`
     auto stage = [&](const double (&P)[R], int slot) {
-        double part[NV];
+        RT part[NV];
+        if constexpr (MIX) {
+            float2 pp[2 * NB];
 #pragma unroll
-        for (int v = 0; v < NV; ++v) part[v] = 0.0;
+            for (int v = 0; v < 2 * NB; ++v) pp[v] = make_float2(0.f, 0.f);
 #pragma unroll
-        for (int r = 0; r < R; ++r) {
+            for (int r = 0; r < R; ++r) {
+                const float pf = (float)P[r];
+                const float2 p2 = make_float2(pf, pf);
 #pragma unroll
-            for (int b = 0; b < NB; ++b) {
-                part[4 * b + 0] = fma(P[r], gp[r][b].x, part[4 * b + 0]);
-                part[4 * b + 1] = fma(P[r], gp[r][b].y, part[4 * b + 1]);
-                part[4 * b + 2] = fma(P[r], gm[r][b].x, part[4 * b + 2]);
-                part[4 * b + 3] = fma(P[r], gm[r][b].y, part[4 * b + 3]);
+                for (int b = 0; b < NB; ++b) {
+                    pp[2 * b] = __ffma2_rn(p2, gp[r][b], pp[2 * b]);
+                    pp[2 * b + 1] = __ffma2_rn(p2, gm[r][b], pp[2 * b + 1]);
+                }
+            }
+#pragma unroll
+            for (int v = 0; v < 2 * NB; ++v) {
+                part[2 * v] = pp[v].x;
+                part[2 * v + 1] = pp[v].y;
+            }
+        } else {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) part[v] = 0.0;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+#pragma unroll
+                for (int b = 0; b < NB; ++b) {
+                    part[4 * b + 0] = fma(P[r], gp[r][b].x, part[4 * b + 0]);
+                    part[4 * b + 1] = fma(P[r], gp[r][b].y, part[4 * b + 1]);
+                    part[4 * b + 2] = fma(P[r], gm[r][b].x, part[4 * b + 2]);
+                    part[4 * b + 3] = fma(P[r], gm[r][b].y, part[4 * b + 3]);
+                }
             }
         }
 #pragma unroll
-        for (int v = 0; v < NV; ++v) sm.red[warp][kAdjPipelined ? cur : 0][slot * NV + v][lane] = part[v];
+        for (int v = 0; v < NV; ++v) sm.red[warp][slot * NV + v][lane] = part[v];
     };
-    // lane's output (degree lfirst + lane / NV, component lane % NV) of a reduced block
-    auto write_out = [&](int lfirst, double s) {
-        const int li = lane / NV, v = lane % NV;
-        const int l = lfirst + li;
-        const int b = v >> 2, comp = v & 3;
-        if (comp < 2 || m > 0) {
-            const int64_t idx = (l - m) + (comp < 2 ? cp : cm) + albs * (b0 + b);
-            double* dst = almd + 2 * idx + (comp & 1);
-            if (sole) *dst = s;
-            else atomicAdd(dst, s);
-        }
-    };
-    // reduce the staged degrees [lfirst, lfirst + cnt) of buffer cur over the lanes at once
-    auto flush = [&](int lfirst, int cnt) {
+    // reduce the staged degrees [lfirst, lfirst + cnt) over the lanes and write alm; degree
+    // lfirst + i carries the factor g of its chunk slot gslot0 + i (1 for the seed degrees)
+    auto flush = [&](int lfirst, int cnt, int gslot0) {
         __syncwarp();
         if (lane < cnt * NV) {
+            const int li = lane / NV, v = lane % NV;
             // four independent partial sums: the chain of dependent adds is 8 long, not 32
-            double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+            RT s0 = 0, s1 = 0, s2 = 0, s3 = 0;
 #pragma unroll
             for (int q = 0; q < 32; q += 4) {
-                s0 += sm.red[warp][kAdjPipelined ? cur : 0][lane][q];
-                s1 += sm.red[warp][kAdjPipelined ? cur : 0][lane][q + 1];
-                s2 += sm.red[warp][kAdjPipelined ? cur : 0][lane][q + 2];
-                s3 += sm.red[warp][kAdjPipelined ? cur : 0][lane][q + 3];
+                s0 += sm.red[warp][lane][q];
+                s1 += sm.red[warp][lane][q + 1];
+                s2 += sm.red[warp][lane][q + 2];
+                s3 += sm.red[warp][lane][q + 3];
             }
-            write_out(lfirst, (s0 + s1) + (s2 + s3));
+            double s = (double)((s0 + s1) + (s2 + s3));
+            if (gslot0 >= 0) s *= sm.bg[warp][gslot0 + li].y;
+            const int l = lfirst + li;
+            const int b = v >> 2, comp = v & 3;
+            if (comp < 2 || m > 0) {
+                const int64_t idx = (l - m) + (comp < 2 ? cp : cm) + albs * (b0 + b);
+                double* dst = almd + 2 * idx + (comp & 1);
+                if (sole) *dst = s;
+                else atomicAdd(dst, s);
+            }
         }
         __syncwarp();
-    };
-    // NV of the pending block's 32 values, read while degree slot i of the next block runs
-    auto drain = [&](int i) {
-#pragma unroll
-        for (int k = 0; k < NV; k += 4) {
-            const double* rowp = &sm.red[warp][kAdjPipelined ? cur ^ 1 : 0][lane][i * NV + k];
-            a0 += rowp[0];
-            a1 += rowp[1];
-            a2 += rowp[2];
-            a3 += rowp[3];
-        }
-    };
-    auto finish = [&]() {
-        write_out(pend, (a0 + a1) + (a2 + a3));
-        a0 = a1 = a2 = a3 = 0.0;
-        pend = -1;
     };
     int lstart = item.lbeg;
     if (seeded) {
-        stage(p2, 0);  // l = m
+        stage(q2, 0);  // l = m
         if (m == L) {
-            flush(m, 1);
+            flush(m, 1, -1);
             return;
         }
         const double s23 = sqrt((double)(2 * m + 3));
+        double p1[R];
 #pragma unroll
-        for (int r = 0; r < R; ++r) p1[r] = s23 * x[r] * p2[r];
+        for (int r = 0; r < R; ++r) p1[r] = s23 * x[r] * q2[r];
         stage(p1, 1);  // l = m + 1
-        flush(m, 2);
+        flush(m, 2, -1);
+        // enter the monic form at l = m + 2: (q1, q2) = (P_{m+1}, a_{m+1} P_m)
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            q2[r] = s23 * q2[r];
+            q1[r] = p1[r];
+        }
         lstart = m + 2;
     }
-    {
-        auto rec = [&](int i) {
-            const double2 ab = sm.ab[warp][i];
+    auto rec = [&](int i) {
+        const double beta = sm.bg[warp][i].x;
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const double p = fma(ab.x * x[r], p1[r], -(ab.y * p2[r]));
-                p2[r] = p1[r];
-                p1[r] = p;
+        for (int r = 0; r < R; ++r) {
+            const double qn = fma(x[r], q1[r], -(beta * q2[r]));
+            q2[r] = q1[r];
+            q1[r] = qn;
+        }
+    };
+    // the coefficients of the next 32 degrees are loaded while this chunk runs
+    double2 bg_next = make_double2(0.0, 0.0);
+    if (lstart <= item.lend && lane <= item.lend - lstart) bg_next = abm[lstart + lane - m - 2];
+    // segments start on the renormalisation schedule, so the count restarts at 0
+    int steps = 0;
+    for (int l0 = lstart; l0 <= item.lend; l0 += 32) {
+        const int nl = min(32, item.lend - l0 + 1);
+        __syncwarp();
+        if (lane < nl) sm.bg[warp][lane] = bg_next;
+        __syncwarp();
+        if (l0 + 32 + lane <= item.lend) bg_next = abm[l0 + 32 + lane - m - 2];
+        const int nblk = nl / LB;
+        for (int blk = 0; blk < nblk; ++blk) {
+#pragma unroll
+            for (int i = 0; i < LB; ++i) {
+                rec(blk * LB + i);
+                stage(q1, i);
             }
-        };
-        // segments start on the renormalisation schedule, so the count restarts at 0
-        int steps = 0;
-        // the coefficients of the next 32 degrees are loaded while this chunk runs
-        double2 ab_next = make_double2(0.0, 0.0);
-        if (lstart <= item.lend && lane <= item.lend - lstart) ab_next = abm[lstart + lane - m - 2];
-        for (int l0 = lstart; l0 <= item.lend; l0 += 32) {
-            const int nl = min(32, item.lend - l0 + 1);
-            __syncwarp();
-            if (lane < nl) sm.ab[warp][lane] = ab_next;
-            __syncwarp();
-            if (l0 + 32 + lane <= item.lend) ab_next = abm[l0 + 32 + lane - m - 2];
-            const int nblk = nl / LB;
-            for (int blk = 0; blk < nblk; ++blk) {
-                if (!kAdjPipelined) {
+            flush(l0 + blk * LB, LB, blk * LB);
+            steps += LB;
+            if (steps == STRIDE) {
+                steps = 0;
+                if (l0 + blk * LB + LB - 1 < L) {
+                    // leave the block: scale the state by g of its last degree, renormalise
+                    const double G = sm.bg[warp][blk * LB + LB - 1].y;
 #pragma unroll
-                    for (int i = 0; i < LB; ++i) {
-                        rec(blk * LB + i);
-                        stage(p1, i);
-                    }
-                    flush(l0 + blk * LB, LB);
-                } else if (pend >= 0) {
+                    for (int r = 0; r < R; ++r) {
+                        q1[r] *= G;
+                        q2[r] *= G;
+                        const int sh = renorm_shift(q1[r], q2[r]);
+                        if (sh != 0) {
+                            const double f = scalbn(1.0, -sh);
+                            q1[r] *= f;
+                            q2[r] *= f;
+                            const int Eold = E[r];
+                            E[r] += sh;
+                            if (Eold >= kMinE) {
+                                // the scaled ring data were normal: 2^sh keeps them exactly
+                                // what a reload would give
+                                const double u = scalbn(1.0, sh);
 #pragma unroll
-                    for (int i = 0; i < LB; ++i) {
-                        rec(blk * LB + i);
-                        stage(p1, i);
-                        drain(i);
-                    }
-                } else {
-#pragma unroll
-                    for (int i = 0; i < LB; ++i) {
-                        rec(blk * LB + i);
-                        stage(p1, i);
-                    }
-                }
-                if (kAdjPipelined) {
-                    // this block's sums are visible, and every lane is done with the other buffer
-                    __syncwarp();
-                    if (pend >= 0) finish();
-                    pend = l0 + blk * LB;
-                    cur ^= 1;
-                }
-                steps += LB;
-                if (steps == kStride) {
-                    steps = 0;
-                    if (l0 + blk * LB + LB - 1 < L) {
-#pragma unroll
-                        for (int r = 0; r < R; ++r) {
-                            const double mx = fmax(fabs(p1[r]), fabs(p2[r]));
-                            if (mx > 0.0 && isfinite(mx)) {
-                                const int s = ceil_log2(mx);
-                                if (s != 0) {
-                                    const double f = scalbn(1.0, -s);
-                                    p1[r] *= f;
-                                    p2[r] *= f;
-                                    const int Eold = E[r];
-                                    E[r] += s;
-                                    if (Eold >= -900) {
-                                        // the scaled ring data were normal: 2^s keeps them
-                                        // exactly what a reload would give
-                                        const double u = scalbn(1.0, s);
-#pragma unroll
-                                        for (int b = 0; b < NB; ++b) {
-                                            gp[r][b].x *= u;
-                                            gp[r][b].y *= u;
-                                            gm[r][b].x *= u;
-                                            gm[r][b].y *= u;
-                                        }
-                                    } else {
-                                        load_g(r);
-                                    }
+                                for (int b = 0; b < NB; ++b) {
+                                    gp[r][b].x *= u;
+                                    gp[r][b].y *= u;
+                                    gm[r][b].x *= u;
+                                    gm[r][b].y *= u;
                                 }
+                            } else {
+                                load_g(r);
                             }
                         }
                     }
                 }
             }
-            const int rem = nl - nblk * LB;
-            if (rem > 0) {
-                if (pend >= 0) {
-#pragma unroll
-                    for (int i = 0; i < LB; ++i) drain(i);
-                    finish();
-                }
-                for (int i = 0; i < rem; ++i) {
-                    rec(nblk * LB + i);
-                    stage(p1, i);
-                }
-                flush(l0 + nblk * LB, rem);
-            }
         }
-        if (pend >= 0) {
-#pragma unroll
-            for (int i = 0; i < LB; ++i) drain(i);
-            finish();
+        const int rem = nl - nblk * LB;
+        if (rem > 0) {
+            for (int i = 0; i < rem; ++i) {
+                rec(nblk * LB + i);
+                stage(q1, i);
+            }
+            flush(l0 + nblk * LB, rem, nblk * LB);
         }
     }
 }
 
-template <int RMAX, int NB>
-__global__ void PF_ADJ_BOUNDS
+template <int RMAX, int NB, bool MIX>
+__global__ void __launch_bounds__(kAdjWarps * 32)
 ring_adj_kernel(RingTables t, RingOut o, const RingItem* __restrict__ items, int nitems,
                 const double2* __restrict__ in, double* __restrict__ almd, int b0, int allow_sole) {
-    __shared__ AdjSmem sm;
+    __shared__ AdjSmem<MIX> sm;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int it = blockIdx.x * kAdjWarps + warp;
     if (it >= nitems) return;
@@ -762,10 +874,10 @@ ring_adj_kernel(RingTables t, RingOut o, const RingItem* __restrict__ items, int
         sub.n = min(32 * RMAX, item.n - base);
         if (sub.ck >= 0) sub.ck += base;
         const int reff = (sub.n + 31) >> 5;
-        if (RMAX >= 8 && reff >= 5) ring_adj_item<(RMAX >= 8 ? 8 : 1), NB>(t, o, sub, in, almd, b0, sole, sm, warp, lane);
-        else if (RMAX >= 4 && reff >= 3) ring_adj_item<(RMAX >= 4 ? 4 : 1), NB>(t, o, sub, in, almd, b0, sole, sm, warp, lane);
-        else if (RMAX >= 2 && reff == 2) ring_adj_item<(RMAX >= 2 ? 2 : 1), NB>(t, o, sub, in, almd, b0, sole, sm, warp, lane);
-        else ring_adj_item<1, NB>(t, o, sub, in, almd, b0, sole, sm, warp, lane);
+        if (RMAX >= 8 && reff >= 5) ring_adj_item<(RMAX >= 8 ? 8 : 1), NB, MIX>(t, o, sub, in, almd, b0, sole, sm, warp, lane);
+        else if (RMAX >= 4 && reff >= 3) ring_adj_item<(RMAX >= 4 ? 4 : 1), NB, MIX>(t, o, sub, in, almd, b0, sole, sm, warp, lane);
+        else if (RMAX >= 2 && reff == 2) ring_adj_item<(RMAX >= 2 ? 2 : 1), NB, MIX>(t, o, sub, in, almd, b0, sole, sm, warp, lane);
+        else ring_adj_item<1, NB, MIX>(t, o, sub, in, almd, b0, sole, sm, warp, lane);
     }
 }
 
@@ -784,44 +896,51 @@ __global__ void alm_prepare_kernel(double2* __restrict__ alm, int L, int B,
 // ---------------------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------------------
-template <int RMAX, int NB>
+template <int RMAX, int NB, bool MIX>
 static int launch_fwd(const RingTables& t, const RingOut& o, const RingItem* items, int nitems,
                       const int* jlo, const int* jhi, const double2* alm, double2* out, int b0,
                       cudaStream_t s) {
     const int grid = (nitems + kWarpsPerBlock - 1) / kWarpsPerBlock;
-    ring_fwd_kernel<RMAX, NB><<<grid, kWarpsPerBlock * 32, 0, s>>>(t, o, items, nitems, jlo, jhi,
-                                                                  alm, out, b0);
+    ring_fwd_kernel<RMAX, NB, MIX><<<grid, kWarpsPerBlock * 32, 0, s>>>(t, o, items, nitems, jlo, jhi,
+                                                                       alm, out, b0);
     return check_launch("ring_fwd_kernel");
 }
 
-template <int RMAX, int NB>
+template <int RMAX, int NB, bool MIX>
 static int launch_adj(const RingTables& t, const RingOut& o, const RingItem* items, int nitems,
                       const double2* in, double2* alm, int b0, int allow_sole, cudaStream_t s) {
     const int grid = (nitems + kAdjWarps - 1) / kAdjWarps;
-    ring_adj_kernel<RMAX, NB><<<grid, kAdjWarps * 32, 0, s>>>(
+    ring_adj_kernel<RMAX, NB, MIX><<<grid, kAdjWarps * 32, 0, s>>>(
         t, o, items, nitems, in, reinterpret_cast<double*>(alm), b0, allow_sole);
     return check_launch("ring_adj_kernel");
+}
+
+template <bool MIX>
+static int ring_forward_t(const RingTables& t, const RingOut& o, const RingItems& it,
+                          const double2* alm, double2* out, int B, cudaStream_t s) {
+    int b0 = 0;
+    while (b0 < B) {
+        const int rem = B - b0;
+        if (rem >= 4) {
+            PF_TRY((launch_fwd<1, 4, MIX>(t, o, it.items, it.nitems, it.jlo, it.jhi, alm, out, b0, s)));
+            b0 += 4;
+        } else if (rem >= 2) {
+            PF_TRY((launch_fwd<2, 2, MIX>(t, o, it.items, it.nitems, it.jlo, it.jhi, alm, out, b0, s)));
+            b0 += 2;
+        } else {
+            if (it.rmax >= 4) PF_TRY((launch_fwd<4, 1, MIX>(t, o, it.items, it.nitems, it.jlo, it.jhi, alm, out, b0, s)));
+            else PF_TRY((launch_fwd<2, 1, MIX>(t, o, it.items, it.nitems, it.jlo, it.jhi, alm, out, b0, s)));
+            b0 += 1;
+        }
+    }
+    return 0;
 }
 
 int ring_forward(const RingTables& t, const RingOut& o, const RingItems& it, const double2* alm,
                  double2* out, int B, cudaStream_t s) {
     if (it.nitems <= 0) return 0;
-    int b0 = 0;
-    while (b0 < B) {
-        const int rem = B - b0;
-        if (rem >= 4) {
-            PF_TRY((launch_fwd<1, 4>(t, o, it.items, it.nitems, it.jlo, it.jhi, alm, out, b0, s)));
-            b0 += 4;
-        } else if (rem >= 2) {
-            PF_TRY((launch_fwd<2, 2>(t, o, it.items, it.nitems, it.jlo, it.jhi, alm, out, b0, s)));
-            b0 += 2;
-        } else {
-            if (it.rmax >= 4) PF_TRY((launch_fwd<4, 1>(t, o, it.items, it.nitems, it.jlo, it.jhi, alm, out, b0, s)));
-            else PF_TRY((launch_fwd<2, 1>(t, o, it.items, it.nitems, it.jlo, it.jhi, alm, out, b0, s)));
-            b0 += 1;
-        }
-    }
-    return 0;
+    return t.mix ? ring_forward_t<true>(t, o, it, alm, out, B, s)
+                 : ring_forward_t<false>(t, o, it, alm, out, B, s);
 }
 
 int alm_prepare(double2* alm, int L, int B, const unsigned char* sole_m, int allow_sole,
@@ -831,6 +950,28 @@ int alm_prepare(double2* alm, int L, int B, const unsigned char* sole_m, int all
     return check_launch("alm_prepare_kernel");
 }
 
+template <bool MIX>
+static int ring_adjoint_t(const RingTables& t, const RingOut& o, const RingItems& it,
+                          const double2* in, double2* alm, int B, int allow_sole, cudaStream_t s) {
+    int b0 = 0;
+    while (b0 < B) {
+        const int rem = B - b0;
+        if (rem >= 4) {
+            PF_TRY((launch_adj<1, 4, MIX>(t, o, it.items, it.nitems, in, alm, b0, allow_sole, s)));
+            b0 += 4;
+        } else if (rem >= 2) {
+            PF_TRY((launch_adj<2, 2, MIX>(t, o, it.items, it.nitems, in, alm, b0, allow_sole, s)));
+            b0 += 2;
+        } else {
+            if (it.rmax >= 8) PF_TRY((launch_adj<8, 1, MIX>(t, o, it.items, it.nitems, in, alm, b0, allow_sole, s)));
+            else if (it.rmax >= 4) PF_TRY((launch_adj<4, 1, MIX>(t, o, it.items, it.nitems, in, alm, b0, allow_sole, s)));
+            else PF_TRY((launch_adj<2, 1, MIX>(t, o, it.items, it.nitems, in, alm, b0, allow_sole, s)));
+            b0 += 1;
+        }
+    }
+    return 0;
+}
+
 int ring_adjoint(const RingTables& t, const RingOut& o, const RingItems& it, const double2* in,
                  double2* alm, int B, cudaStream_t s) {
     // a single transform with the item's own tile shape stores sole orders directly; the
@@ -838,23 +979,8 @@ int ring_adjoint(const RingTables& t, const RingOut& o, const RingItems& it, con
     const int allow_sole = (B == 1 && it.rmax >= 2) ? 1 : 0;
     PF_TRY(alm_prepare(alm, t.lmax, B, it.sole_m, allow_sole, s));
     if (it.nitems <= 0) return 0;
-    int b0 = 0;
-    while (b0 < B) {
-        const int rem = B - b0;
-        if (rem >= 4) {
-            PF_TRY((launch_adj<1, 4>(t, o, it.items, it.nitems, in, alm, b0, allow_sole, s)));
-            b0 += 4;
-        } else if (rem >= 2) {
-            PF_TRY((launch_adj<2, 2>(t, o, it.items, it.nitems, in, alm, b0, allow_sole, s)));
-            b0 += 2;
-        } else {
-            if (it.rmax >= 8) PF_TRY((launch_adj<8, 1>(t, o, it.items, it.nitems, in, alm, b0, allow_sole, s)));
-            else if (it.rmax >= 4) PF_TRY((launch_adj<4, 1>(t, o, it.items, it.nitems, in, alm, b0, allow_sole, s)));
-            else PF_TRY((launch_adj<2, 1>(t, o, it.items, it.nitems, in, alm, b0, allow_sole, s)));
-            b0 += 1;
-        }
-    }
-    return 0;
+    return t.mix ? ring_adjoint_t<true>(t, o, it, in, alm, B, allow_sole, s)
+                 : ring_adjoint_t<false>(t, o, it, in, alm, B, allow_sole, s);
 }
 
 // item lists of one ring set: tiles of 32 * rmax rings, the order flags, the device tables
