@@ -271,9 +271,11 @@ int build_stretch(pfsht_plan* p, const double* d_theta, const double* d_phi, con
     p->rt.aboff = p->aboff.as<int64_t>();
     p->rt.lmax = L;
     p->rt.nrings = lf.nth_half;
-    // forward tiles of 64 rings (more warps), adjoint tiles of 128 (amortises its reduction)
-    // split along the degree axis when the tiles alone leave the GPU under-filled
-    PF_TRY(build_ring_items(lf.jlo, lf.jhi, L, lf.mmax, p->R > 0 ? p->R : 2, p->fwd_items, s));
+    // forward tiles of 64 rings in the FP64 form (more warps) and of 128 in the mixed form
+    // (measured faster), adjoint tiles of 128 (amortises its reduction), split along the degree
+    // axis when the tiles alone leave the GPU under-filled
+    PF_TRY(build_ring_items(lf.jlo, lf.jhi, L, lf.mmax, p->R > 0 ? p->R : (mix ? 4 : 2),
+                            p->fwd_items, s));
     PF_TRY(build_adjoint_items(p, lf.jlo, lf.jhi, lf.mmax, s));
     p->ncols = 2 * lf.mmax + 1;
     p->ro_cols.ld = lf.nth;

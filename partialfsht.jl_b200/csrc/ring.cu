@@ -27,7 +27,7 @@
 // split over several tiles adds them atomically (into zeros).
 //
 // Mixed form (MIX): the recurrence and exponents stay FP64; the forward accumulates in FP32
-// with paired (float2) FMAs over blocks of 8 degrees and adds each block into a compensated
+// with paired (float2) FMAs over each 32-degree chunk and adds the chunk into a compensated
 // (two-sum) FP32 total; the adjoint keeps the ring data in FP32 and reduces in FP32.
 #include <algorithm>
 #include <cmath>
@@ -138,13 +138,6 @@ std::vector<RingItem> make_ring_items(const std::vector<int>& jlo, const std::ve
     return out;
 }
 
-// ceil(log2(mx)) for finite mx > 0, exact (no transcendental)
-__device__ __forceinline__ int ceil_log2(double mx) {
-    int e;
-    double f = frexp(mx, &e);
-    return f == 0.5 ? e - 1 : e;
-}
-
 // seed of ring j for order m (src/Legendre.jl:379-382, exponent per ring as in
 // ext/PartialFSHTKernelAbstractionsExt.jl:96-99)
 __device__ __forceinline__ void ring_seed(const RingTables& t, int m, int j, double sgn,
@@ -160,11 +153,16 @@ __device__ __forceinline__ void ring_seed(const RingTables& t, int m, int j, dou
     }
 }
 
-// power-of-two exponent that brings max(|q1|, |q2|) into (1/2, 1]; 0 when nothing to do
+// power-of-two exponent that brings max(|q1|, |q2|) into [1/2, 1), read from the exponent
+// field (any power of two keeps the scaling exact); 0 for zero, subnormal or non-finite
 __device__ __forceinline__ int renorm_shift(double q1, double q2) {
     const double mx = fmax(fabs(q1), fabs(q2));
-    return (mx > 0.0 && isfinite(mx)) ? ceil_log2(mx) : 0;
+    const int e = (__double2hiint(mx) >> 20) & 0x7ff;
+    return (e == 0 || e == 0x7ff) ? 0 : e - 1022;
 }
+
+// 2^k for -1022 <= k <= 1023, built from its exponent field
+__device__ __forceinline__ double pow2i(int k) { return __hiloint2double((k + 1023) << 20, 0); }
 
 // ---------------------------------------------------------------------------------------
 // plan-time recurrence checkpoints: one thread per (order, ring) walks the same monic
@@ -213,7 +211,7 @@ __global__ void ring_ckpt_kernel(RingTables t, const CkptJob* __restrict__ jobs,
                 q2 *= bg.y;
                 const int sh = renorm_shift(q1, q2);
                 if (sh != 0) {
-                    const double f = scalbn(1.0, -sh);
+                    const double f = pow2i(-sh);
                     q1 *= f;
                     q2 *= f;
                     E += sh;
@@ -497,7 +495,6 @@ __device__ __forceinline__ void ring_fwd_item(const RingTables& t, const RingOut
             for (int blk = 0; blk < nblk; ++blk) {
 #pragma unroll
                 for (int i = 0; i < 8; ++i) step(blk * 8 + i);
-                fold_all();
                 steps += 8;
                 if (steps == STRIDE) {
                     steps = 0;
@@ -510,7 +507,7 @@ __device__ __forceinline__ void ring_fwd_item(const RingTables& t, const RingOut
                             q2[r] *= G;
                             const int sh = renorm_shift(q1[r], q2[r]);
                             if (sh != 0) {
-                                const double f = scalbn(1.0, -sh);
+                                const double f = pow2i(-sh);
                                 q1[r] *= f;
                                 q2[r] *= f;
 #pragma unroll
@@ -822,7 +819,7 @@ __device__ __forceinline__ void ring_adj_item(const RingTables& t, const RingOut
                         q2[r] *= G;
                         const int sh = renorm_shift(q1[r], q2[r]);
                         if (sh != 0) {
-                            const double f = scalbn(1.0, -sh);
+                            const double f = pow2i(-sh);
                             q1[r] *= f;
                             q2[r] *= f;
                             const int Eold = E[r];
@@ -830,7 +827,7 @@ __device__ __forceinline__ void ring_adj_item(const RingTables& t, const RingOut
                             if (Eold >= kMinE) {
                                 // the scaled ring data were normal: 2^sh keeps them exactly
                                 // what a reload would give
-                                const double u = scalbn(1.0, sh);
+                                const double u = pow2i(sh);
 #pragma unroll
                                 for (int b = 0; b < NB; ++b) {
                                     gp[r][b].x *= u;
