@@ -142,6 +142,28 @@ pfsht_status pfsht_nufft_create(int32_t type, int32_t n1, int32_t n2, int32_t if
 pfsht_status pfsht_nufft_exec(pfsht_nufft* p, const void* in, void* out, void* stream);
 pfsht_status pfsht_nufft_destroy(pfsht_nufft* p);
 
+/* Many plans applied together (the farmed mul! over independent plans,
+ * ext/PartialFSHTOhMyThreadsExt.jl:151-159, on one GPU). A batch holds borrowed plans of one
+ * device, which must outlive it and must not be applied elsewhere while a batch apply runs.
+ * Each direction is one CUDA graph, captured at its first call and replayed by one
+ * cudaGraphLaunch: the ring passes of all plans run as one launch per kernel shape (at most a
+ * few), the remaining stages of the plans concurrently on nstreams internal streams (0 = 8).
+ * alms[i] and fs[i] are plan i's device arrays, in the layouts of pfsht_forward / pfsht_adjoint;
+ * they may change from call to call. A call returns once the graph is enqueued on `stream`;
+ * it first waits for the batch's previous call to finish on the device. */
+typedef struct pfsht_batch pfsht_batch;
+pfsht_status pfsht_batch_create(pfsht_plan* const* plans, int32_t nplans, int32_t nstreams,
+                                pfsht_batch** out);
+pfsht_status pfsht_batch_forward(pfsht_batch* batch, const void* const* alms, void* const* fs,
+                                 void* stream);
+pfsht_status pfsht_batch_adjoint(pfsht_batch* batch, const void* const* fs, void* const* alms,
+                                 void* stream);
+/* ring-pass launches per direction and nodes of the captured graphs (0 before the first call) */
+pfsht_status pfsht_batch_info(const pfsht_batch* batch, int32_t* ring_launches_fwd,
+                              int32_t* ring_launches_adj, int64_t* graph_nodes_fwd,
+                              int64_t* graph_nodes_adj);
+pfsht_status pfsht_batch_destroy(pfsht_batch* batch);
+
 /* FMA-throughput microbenchmark on the current device (no reference counterpart): runs a
  * grid of independent FP64 (fp64 = 1) or FP32 FMA chains and reports FLOP/s (2 per FMA).
  * These are the denominators of the ring-pass and NUFFT FLOP rooflines. */

@@ -23,7 +23,7 @@ import numpy as np
 from . import _lib
 from ._lib import DimensionMismatch, PFSHTError, RefusedGeometry  # noqa: F401
 
-__all__ = ["Plan", "AdjointPlan", "mul", "coeff_size", "sph_mode", "zeros_alm", "zeros_field",
+__all__ = ["Plan", "AdjointPlan", "Batch", "mul", "coeff_size", "sph_mode", "zeros_alm", "zeros_field",
            "plan_geometry", "ring_forward", "ring_adjoint", "NUFFT", "DimensionMismatch",
            "RefusedGeometry", "PFSHTError", "version"]
 
@@ -385,6 +385,62 @@ def plan_geometry(theta, phi, *, lmax, tol=1e-10, ntrans=1, method="auto",
     d = {k: getattr(inf, k) for k, _ in _lib.PlanInfo._fields_}
     d["kind"] = _lib.KINDS[inf.kind]
     return d
+
+
+class Batch:
+    """Many plans applied together (pfsht_batch_*): one captured CUDA graph per direction, the
+    ring passes of all plans in a few launches, the other stages on ``nstreams`` streams. The
+    batch borrows the plans: keep them alive and do not apply them elsewhere meanwhile."""
+
+    def __init__(self, plans, nstreams=0):
+        self._h = None
+        self.plans = list(plans)
+        if not self.plans:
+            raise ValueError("a batch needs at least one plan")
+        arr = (C.c_void_p * len(self.plans))(*[p._h for p in self.plans])
+        h = C.c_void_p()
+        _lib.check(_lib.load().pfsht_batch_create(arr, len(self.plans), int(nstreams), C.byref(h)),
+                   "batch")
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _lib is not None and _lib._lib is not None:
+            _lib._lib.pfsht_batch_destroy(h)
+        self._h = None
+
+    def _ptrs(self, arrays, shapes, what):
+        if len(arrays) != len(self.plans):
+            raise DimensionMismatch(f"{len(arrays)} {what} arrays for {len(self.plans)} plans")
+        for a, shp in zip(arrays, shapes):
+            _check_array(a, shp, what)
+            if not (_is_torch(a) and a.is_cuda):
+                raise ValueError("batch applies take CUDA tensors")
+        return (C.c_void_p * len(arrays))(*[_ptr(a) for a in arrays])
+
+    def forward(self, fs, alms, stream=None):
+        """mul!(f_i, plan_i, alm_i) for every plan of the batch."""
+        pa = self._ptrs(alms, [_coeff_shapes(p.lmax, p.ntrans) for p in self.plans], "coefficient")
+        pf_ = self._ptrs(fs, [_field_shapes(p.npts, p.ntrans) for p in self.plans], "field")
+        _lib.check(_lib.load().pfsht_batch_forward(self._h, pa, pf_, _stream_of(alms[0], stream)),
+                   "batch forward")
+        return fs
+
+    def adjoint(self, alms, fs, stream=None):
+        """mul!(alm_i, plan_i', f_i) for every plan of the batch."""
+        pa = self._ptrs(alms, [_coeff_shapes(p.lmax, p.ntrans) for p in self.plans], "coefficient")
+        pf_ = self._ptrs(fs, [_field_shapes(p.npts, p.ntrans) for p in self.plans], "field")
+        _lib.check(_lib.load().pfsht_batch_adjoint(self._h, pf_, pa, _stream_of(fs[0], stream)),
+                   "batch adjoint")
+        return alms
+
+    def info(self) -> dict:
+        a, b = C.c_int32(), C.c_int32()
+        c, d = C.c_int64(), C.c_int64()
+        _lib.check(_lib.load().pfsht_batch_info(self._h, C.byref(a), C.byref(b), C.byref(c),
+                                                C.byref(d)), "batch info")
+        return {"ring_launches_fwd": a.value, "ring_launches_adj": b.value,
+                "graph_nodes_fwd": c.value, "graph_nodes_adj": d.value}
 
 
 class NUFFT:

@@ -70,6 +70,12 @@ SIGNATURES = {
     "pfsht_fma_peak": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "pfsht_launch_count": (C.c_int64, []),
     "pfsht_direct_forward_noalloc": (C.c_int, [_vp, _vp, C.c_int64, C.c_int32, _vp, _vp, _vp]),
+    "pfsht_batch_create": (C.c_int, [C.POINTER(_vp), C.c_int32, C.c_int32, C.POINTER(_vp)]),
+    "pfsht_batch_forward": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(_vp), _vp]),
+    "pfsht_batch_adjoint": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(_vp), _vp]),
+    "pfsht_batch_info": (C.c_int, [_vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                   C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "pfsht_batch_destroy": (C.c_int, [_vp]),
     "pfsht_profile_start": (C.c_int, [_vp, C.c_int32]),
     "pfsht_profile_stop": (C.c_int, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
     "pfsht_num_stages": (C.c_int32, []),

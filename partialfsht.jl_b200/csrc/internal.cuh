@@ -4,6 +4,7 @@
 #include <cufft.h>
 
 #include <cstdint>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -130,7 +131,46 @@ struct RingItems {
 struct RingItemsOwner {
     DevBuf items, sole, jlo, jhi;
     RingItems view;
+    std::vector<RingItem> host;  // the items, in launch order
 };
+
+// one plan of a batched ring pass, as the batched kernels read it from device memory
+struct RingSlot {
+    RingTables t;
+    RingOut o;
+    const int* jlo = nullptr;
+    const int* jhi = nullptr;
+    double2* H = nullptr;     // the plan's column array
+    int allow_sole = 0;       // adjoint: orders covered by one tile store instead of adding
+    int ptr = 0;              // index of the plan's coefficient array in the pointer table
+};
+struct BatchItem {
+    RingItem it;
+    int slot;   // plan
+    int b0;     // first transform of the pass
+};
+// the items of one kernel shape: rings per lane (rmax), transforms per pass (nb), mixed
+struct RingBatchGroup {
+    int rmax = 1, nb = 1, mix = 0;
+    DevBuf items;
+    int nitems = 0;
+};
+// what the grouping needs of one plan
+struct RingBatchPlan {
+    const std::vector<RingItem>* items;
+    int B, rmax, mix;
+};
+// one group per kernel shape, items of all plans heaviest first
+int build_ring_batch(const std::vector<RingBatchPlan>& plans, bool adjoint,
+                     std::vector<std::unique_ptr<RingBatchGroup>>& groups, cudaStream_t s);
+// the ring passes of all plans: one launch per group; coefficient arrays through ptrs
+int ring_forward_batch(const RingSlot* slots, const std::vector<std::unique_ptr<RingBatchGroup>>& groups,
+                       void* const* ptrs, cudaStream_t s);
+int ring_adjoint_batch(const RingSlot* slots, const std::vector<std::unique_ptr<RingBatchGroup>>& groups,
+                       void* const* ptrs, cudaStream_t s);
+// alm_prepare of one plan whose coefficient array is ptrs[ptr]
+int alm_prepare_ptr(void* const* ptrs, int ptr, int L, int B, const unsigned char* sole_m,
+                    int allow_sole, cudaStream_t s);
 
 int build_ab_table(int lmax, int mmax, int stride, DevBuf& ab, DevBuf& aboff, cudaStream_t s);
 int launch_ab_table(int lmax, int mmax, int stride, const int64_t* aboff, double2* ab, cudaStream_t s);

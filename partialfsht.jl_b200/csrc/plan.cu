@@ -23,6 +23,7 @@
 
 #include "../../include/pfsht_b200.h"
 #include "internal.cuh"
+#include "plan_internal.hpp"
 
 namespace pf {
 
@@ -33,45 +34,6 @@ const std::string& get_error() { return g_err; }
 }  // namespace pf
 
 using namespace pf;
-
-struct pfsht_plan {
-    int device = 0;
-    int precision = 0;
-    int kind = kPole;
-    int L = 0, B = 1;
-    int64_t M = 0;
-    double tol = 0;
-    int R = 0;  // ring tile rings-per-lane override (0 = defaults)
-    Leaf leaf;
-    int ncols = 0;
-    int nrings = 0;
-    // ring pass
-    DevBuf cos_t, log2sin, log2c, w, ab, aboff;
-    RingItemsOwner fwd_items, adj_items;
-    RingSegments adj_seg;  // degree segments of the adjoint items
-    int seg_degrees = 0;   // requested segment length (0 = auto, < 0 = none)
-    RingTables rt;
-    RingOut ro_cols;  // the apply's column array H (or G for the direct leaf)
-    // column array: nth x ncols x B (stretch) or M x (2L+1) x B (direct)
-    DevBuf H;
-    cufftHandle fth = 0;
-    bool have_fth = false;
-    // NUFFT
-    NufftGrid ng;
-    NufftDev nd;
-    // direct leaf
-    DevBuf phi_pts;
-    // host-buffer staging
-    DevBuf st_alm, st_f;
-    cudaStream_t st_stream = nullptr;
-    pfsht_plan_info info{};
-    StageClock clk;
-    ~pfsht_plan() {
-        if (have_fth) cufftDestroy(fth);
-        if (st_stream) cudaStreamDestroy(st_stream);
-        for (cudaEvent_t e : clk.ev) cudaEventDestroy(e);
-    }
-};
 
 struct pfsht_nufft {
     int device = 0;
@@ -88,17 +50,6 @@ int fail(int code, const std::string& msg) {
     set_error(msg);
     return code;
 }
-
-struct DeviceGuard {
-    int prev = -1;
-    explicit DeviceGuard(int dev) {
-        cudaGetDevice(&prev);
-        if (dev >= 0 && dev != prev) cudaSetDevice(dev);
-    }
-    ~DeviceGuard() {
-        if (prev >= 0) cudaSetDevice(prev);
-    }
-};
 
 template <class T>
 int upload(DevBuf& d, const std::vector<T>& h, cudaStream_t s) {
@@ -463,42 +414,51 @@ int plan_create(const double* theta, const double* phi, int64_t npts, int lmax, 
 }
 
 int apply_forward(pfsht_plan* p, const double2* alm, double2* f, cudaStream_t s) {
-    const int B = p->B;
-    StageClock* clk = &p->clk;
-    clock_begin(clk, s);
-    PF_TRY(ring_forward(p->rt, p->ro_cols, p->fwd_items.view, alm, p->H.as<double2>(), B, s));
-    if (p->kind == kDirect) {
-        PF_TRY(direct_phase_sum(p->H.as<double2>(), p->phi_pts.as<double>(), p->M, p->L, B, f, s));
-        clock_mark(clk, kStDirect, s);
-        return 0;
-    }
-    clock_mark(clk, kStRingFwd, s);
-    PF_CUFFT(cufftSetStream(p->fth, s));
-    PF_CUFFT(cufftExecZ2Z(p->fth, p->H.as<cufftDoubleComplex>(), p->H.as<cufftDoubleComplex>(),
-                          CUFFT_FORWARD));
-    clock_mark(clk, kStFftThetaFwd, s);
-    return nufft_type2(p->ng, p->nd, p->H.as<double2>(), f, B, +1, s, clk);
+    clock_begin(&p->clk, s);
+    PF_TRY(ring_forward(p->rt, p->ro_cols, p->fwd_items.view, alm, p->H.as<double2>(), p->B, s));
+    if (p->kind != kDirect) clock_mark(&p->clk, kStRingFwd, s);
+    return plan_forward_after_ring(p, f, s);
 }
 
 int apply_adjoint(pfsht_plan* p, const double2* f, double2* alm, cudaStream_t s) {
-    const int B = p->B;
-    StageClock* clk = &p->clk;
-    clock_begin(clk, s);
-    if (p->kind == kDirect) {
-        PF_TRY(direct_phase_spread(f, p->phi_pts.as<double>(), p->M, p->L, B, p->H.as<double2>(), s));
-    } else {
-        PF_TRY(nufft_type1(p->ng, p->nd, f, p->H.as<double2>(), B, -1, s, clk));
-        PF_CUFFT(cufftSetStream(p->fth, s));
-        PF_CUFFT(cufftExecZ2Z(p->fth, p->H.as<cufftDoubleComplex>(), p->H.as<cufftDoubleComplex>(),
-                              CUFFT_INVERSE));
-        clock_mark(clk, kStFftThetaAdj, s);
-    }
-    PF_TRY(ring_adjoint(p->rt, p->ro_cols, p->adj_items.view, p->H.as<double2>(), alm, B, s));
-    clock_mark(clk, p->kind == kDirect ? kStDirect : kStRingAdj, s);
+    clock_begin(&p->clk, s);
+    PF_TRY(plan_adjoint_before_ring(p, f, s));
+    PF_TRY(ring_adjoint(p->rt, p->ro_cols, p->adj_items.view, p->H.as<double2>(), alm, p->B, s));
+    clock_mark(&p->clk, p->kind == kDirect ? kStDirect : kStRingAdj, s);
     return 0;
 }
 
 }  // namespace
+
+namespace pf {
+
+int plan_forward_after_ring(pfsht_plan* p, double2* f, cudaStream_t s) {
+    StageClock* clk = &p->clk;
+    if (p->kind == kDirect) {
+        PF_TRY(direct_phase_sum(p->H.as<double2>(), p->phi_pts.as<double>(), p->M, p->L, p->B, f, s));
+        clock_mark(clk, kStDirect, s);
+        return 0;
+    }
+    PF_CUFFT(cufftSetStream(p->fth, s));
+    PF_CUFFT(cufftExecZ2Z(p->fth, p->H.as<cufftDoubleComplex>(), p->H.as<cufftDoubleComplex>(),
+                          CUFFT_FORWARD));
+    clock_mark(clk, kStFftThetaFwd, s);
+    return nufft_type2(p->ng, p->nd, p->H.as<double2>(), f, p->B, +1, s, clk);
+}
+
+int plan_adjoint_before_ring(pfsht_plan* p, const double2* f, cudaStream_t s) {
+    StageClock* clk = &p->clk;
+    if (p->kind == kDirect)
+        return direct_phase_spread(f, p->phi_pts.as<double>(), p->M, p->L, p->B, p->H.as<double2>(), s);
+    PF_TRY(nufft_type1(p->ng, p->nd, f, p->H.as<double2>(), p->B, -1, s, clk));
+    PF_CUFFT(cufftSetStream(p->fth, s));
+    PF_CUFFT(cufftExecZ2Z(p->fth, p->H.as<cufftDoubleComplex>(), p->H.as<cufftDoubleComplex>(),
+                          CUFFT_INVERSE));
+    clock_mark(clk, kStFftThetaAdj, s);
+    return 0;
+}
+
+}  // namespace pf
 
 extern "C" {
 

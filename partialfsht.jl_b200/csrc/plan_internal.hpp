@@ -1,0 +1,69 @@
+// The plan object behind the C ABI's opaque pfsht_plan, shared by plan.cu (construction and
+// single-plan applies) and batch.cu (many plans in one captured graph).
+#pragma once
+#include <cufft.h>
+
+#include "../../include/pfsht_b200.h"
+#include "internal.cuh"
+
+using namespace pf;
+
+struct pfsht_plan {
+    int device = 0;
+    int precision = 0;
+    int kind = kPole;
+    int L = 0, B = 1;
+    int64_t M = 0;
+    double tol = 0;
+    int R = 0;  // ring tile rings-per-lane override (0 = defaults)
+    pf::Leaf leaf;
+    int ncols = 0;
+    int nrings = 0;
+    // ring pass
+    DevBuf cos_t, log2sin, log2c, w, ab, aboff;
+    RingItemsOwner fwd_items, adj_items;
+    RingSegments adj_seg;  // degree segments of the adjoint items
+    int seg_degrees = 0;   // requested segment length (0 = auto, < 0 = none)
+    RingTables rt;
+    RingOut ro_cols;  // the apply's column array H (or G for the direct leaf)
+    // column array: nth x ncols x B (stretch) or M x (2L+1) x B (direct)
+    DevBuf H;
+    cufftHandle fth = 0;
+    bool have_fth = false;
+    // NUFFT
+    NufftGrid ng;
+    NufftDev nd;
+    // direct leaf
+    DevBuf phi_pts;
+    // host-buffer staging
+    DevBuf st_alm, st_f;
+    cudaStream_t st_stream = nullptr;
+    pfsht_plan_info info{};
+    StageClock clk;
+    ~pfsht_plan() {
+        if (have_fth) cufftDestroy(fth);
+        if (st_stream) cudaStreamDestroy(st_stream);
+        for (cudaEvent_t e : clk.ev) cudaEventDestroy(e);
+    }
+};
+
+namespace pf {
+
+// selects a device for the lifetime of a call and restores the caller's
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (dev >= 0 && dev != prev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+// The pieces of one apply around its ring pass: the forward after the ring pass (FFT along
+// Theta and NUFFT type 2, or the Direct leaf's phase sum) and the adjoint before it.
+int plan_forward_after_ring(pfsht_plan* p, double2* f, cudaStream_t s);
+int plan_adjoint_before_ring(pfsht_plan* p, const double2* f, cudaStream_t s);
+
+}  // namespace pf

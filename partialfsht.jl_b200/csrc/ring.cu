@@ -31,6 +31,7 @@
 // (two-sum) FP32 total; the adjoint keeps the ring data in FP32 and reduces in FP32.
 #include <algorithm>
 #include <cmath>
+#include <map>
 #include <type_traits>
 
 #include "internal.cuh"
@@ -573,15 +574,12 @@ __device__ __forceinline__ void ring_fwd_zero_rest(const RingOut& o, const RingI
 }
 
 template <int RMAX, int NB, bool MIX>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32)
-ring_fwd_kernel(RingTables t, RingOut o, const RingItem* __restrict__ items, int nitems,
-                const int* __restrict__ jlo, const int* __restrict__ jhi,
-                const double2* __restrict__ alm, double2* __restrict__ out, int b0) {
-    __shared__ FwdSmem<NB, MIX> sm;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int it = blockIdx.x * kWarpsPerBlock + warp;
-    if (it >= nitems) return;
-    const RingItem item = items[it];
+__device__ __forceinline__ void ring_fwd_body(const RingTables& t, const RingOut& o,
+                                              const RingItem& item, const int* __restrict__ jlo,
+                                              const int* __restrict__ jhi,
+                                              const double2* __restrict__ alm,
+                                              double2* __restrict__ out, int b0,
+                                              FwdSmem<NB, MIX>& sm, int warp, int lane) {
     if ((item.flags & kItemFirst) && o.zero_rest)
         ring_fwd_zero_rest<NB>(o, item, jlo[item.m], jhi[item.m], out, b0, lane);
     for (int base = 0; base < item.n; base += 32 * RMAX) {
@@ -594,6 +592,36 @@ ring_fwd_kernel(RingTables t, RingOut o, const RingItem* __restrict__ items, int
         else if (RMAX >= 2 && reff == 2) ring_fwd_item<(RMAX >= 2 ? 2 : 1), NB, MIX>(t, o, sub, alm, out, b0, sm, warp, lane);
         else ring_fwd_item<1, NB, MIX>(t, o, sub, alm, out, b0, sm, warp, lane);
     }
+}
+
+template <int RMAX, int NB, bool MIX>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+ring_fwd_kernel(RingTables t, RingOut o, const RingItem* __restrict__ items, int nitems,
+                const int* __restrict__ jlo, const int* __restrict__ jhi,
+                const double2* __restrict__ alm, double2* __restrict__ out, int b0) {
+    __shared__ FwdSmem<NB, MIX> sm;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int it = blockIdx.x * kWarpsPerBlock + warp;
+    if (it >= nitems) return;
+    ring_fwd_body<RMAX, NB, MIX>(t, o, items[it], jlo, jhi, alm, out, b0, sm, warp, lane);
+}
+
+// the forward ring passes of many plans: item i belongs to plan items[i].slot
+template <int RMAX, int NB, bool MIX>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+ring_fwd_batch_kernel(const RingSlot* __restrict__ slots, const BatchItem* __restrict__ items,
+                      int nitems, void* const* __restrict__ ptrs) {
+    __shared__ FwdSmem<NB, MIX> sm;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int it = blockIdx.x * kWarpsPerBlock + warp;
+    if (it >= nitems) return;
+    const BatchItem bi = items[it];
+    const RingSlot& sl = slots[bi.slot];
+    const RingTables t = sl.t;
+    const RingOut o = sl.o;
+    ring_fwd_body<RMAX, NB, MIX>(t, o, bi.it, sl.jlo, sl.jhi,
+                                 static_cast<const double2*>(ptrs[sl.ptr]), sl.H, bi.b0, sm, warp,
+                                 lane);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -855,14 +883,10 @@ __device__ __forceinline__ void ring_adj_item(const RingTables& t, const RingOut
 }
 
 template <int RMAX, int NB, bool MIX>
-__global__ void __launch_bounds__(kAdjWarps * 32)
-ring_adj_kernel(RingTables t, RingOut o, const RingItem* __restrict__ items, int nitems,
-                const double2* __restrict__ in, double* __restrict__ almd, int b0, int allow_sole) {
-    __shared__ AdjSmem<MIX> sm;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int it = blockIdx.x * kAdjWarps + warp;
-    if (it >= nitems) return;
-    const RingItem item = items[it];
+__device__ __forceinline__ void ring_adj_body(const RingTables& t, const RingOut& o,
+                                              const RingItem& item, const double2* __restrict__ in,
+                                              double* __restrict__ almd, int b0, int allow_sole,
+                                              AdjSmem<MIX>& sm, int warp, int lane) {
     const bool multi = item.n > 32 * RMAX;
     const bool sole = allow_sole && (item.flags & kItemSole) && !multi;
     for (int base = 0; base < item.n; base += 32 * RMAX) {
@@ -876,6 +900,34 @@ ring_adj_kernel(RingTables t, RingOut o, const RingItem* __restrict__ items, int
         else if (RMAX >= 2 && reff == 2) ring_adj_item<(RMAX >= 2 ? 2 : 1), NB, MIX>(t, o, sub, in, almd, b0, sole, sm, warp, lane);
         else ring_adj_item<1, NB, MIX>(t, o, sub, in, almd, b0, sole, sm, warp, lane);
     }
+}
+
+template <int RMAX, int NB, bool MIX>
+__global__ void __launch_bounds__(kAdjWarps * 32)
+ring_adj_kernel(RingTables t, RingOut o, const RingItem* __restrict__ items, int nitems,
+                const double2* __restrict__ in, double* __restrict__ almd, int b0, int allow_sole) {
+    __shared__ AdjSmem<MIX> sm;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int it = blockIdx.x * kAdjWarps + warp;
+    if (it >= nitems) return;
+    ring_adj_body<RMAX, NB, MIX>(t, o, items[it], in, almd, b0, allow_sole, sm, warp, lane);
+}
+
+// the adjoint ring passes of many plans: item i belongs to plan items[i].slot
+template <int RMAX, int NB, bool MIX>
+__global__ void __launch_bounds__(kAdjWarps * 32)
+ring_adj_batch_kernel(const RingSlot* __restrict__ slots, const BatchItem* __restrict__ items,
+                      int nitems, void* const* __restrict__ ptrs) {
+    __shared__ AdjSmem<MIX> sm;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int it = blockIdx.x * kAdjWarps + warp;
+    if (it >= nitems) return;
+    const BatchItem bi = items[it];
+    const RingSlot& sl = slots[bi.slot];
+    const RingTables t = sl.t;
+    const RingOut o = sl.o;
+    ring_adj_body<RMAX, NB, MIX>(t, o, bi.it, sl.H, static_cast<double*>(ptrs[sl.ptr]), bi.b0,
+                                 sl.allow_sole, sm, warp, lane);
 }
 
 // zero what the adjoint does not overwrite: padding rows of every column, the orders the
@@ -1000,10 +1052,155 @@ int build_ring_items(const std::vector<int>& jlo, const std::vector<int>& jhi, i
     PF_CUDA(cudaStreamSynchronize(s));
     own.view.items = own.items.as<RingItem>();
     own.view.nitems = (int)items.size();
+    own.host = items;
     own.view.rmax = rmax;
     own.view.sole_m = own.sole.as<unsigned char>();
     own.view.jlo = own.jlo.as<int>();
     own.view.jhi = own.jhi.as<int>();
+    return 0;
+}
+
+// ---------------------------------------------------------------------------------------
+// batched ring passes: the items of many plans, grouped by kernel shape
+// ---------------------------------------------------------------------------------------
+__global__ void alm_prepare_ptr_kernel(void* const* __restrict__ ptrs, int ptr, int L, int B,
+                                       const unsigned char* __restrict__ sole_m, int allow_sole) {
+    double2* alm = static_cast<double2*>(ptrs[ptr]);
+    const int c = blockIdx.x, b = blockIdx.y;
+    const int am = (c + 1) / 2;
+    double2* col = alm + (int64_t)(L + 1) * c + (int64_t)(L + 1) * (2 * L + 1) * b;
+    const int first = (allow_sole && sole_m[am]) ? L - am + 1 : 0;
+    for (int r = first + threadIdx.x; r <= L; r += blockDim.x) col[r] = make_double2(0.0, 0.0);
+}
+
+int alm_prepare_ptr(void* const* ptrs, int ptr, int L, int B, const unsigned char* sole_m,
+                    int allow_sole, cudaStream_t s) {
+    dim3 grid(2 * L + 1, B);
+    alm_prepare_ptr_kernel<<<grid, 128, 0, s>>>(ptrs, ptr, L, B, sole_m, allow_sole);
+    return check_launch("alm_prepare_ptr_kernel");
+}
+
+// the passes a single-plan launch would make over B transforms: (rings per lane, transforms)
+static std::vector<std::pair<int, int>> ring_passes(int B, int rmax, bool adjoint, std::vector<int>& b0s) {
+    std::vector<std::pair<int, int>> v;
+    b0s.clear();
+    int b0 = 0;
+    while (b0 < B) {
+        const int rem = B - b0;
+        b0s.push_back(b0);
+        if (rem >= 4) {
+            v.push_back({1, 4});
+            b0 += 4;
+        } else if (rem >= 2) {
+            v.push_back({2, 2});
+            b0 += 2;
+        } else {
+            const int r = adjoint ? (rmax >= 8 ? 8 : rmax >= 4 ? 4 : 2) : (rmax >= 4 ? 4 : 2);
+            v.push_back({r, 1});
+            b0 += 1;
+        }
+    }
+    return v;
+}
+
+int build_ring_batch(const std::vector<RingBatchPlan>& plans, bool adjoint,
+                     std::vector<std::unique_ptr<RingBatchGroup>>& groups, cudaStream_t s) {
+    groups.clear();
+    struct Key {
+        int rmax, nb, mix;
+        bool operator<(const Key& o) const {
+            return rmax != o.rmax ? rmax < o.rmax : nb != o.nb ? nb < o.nb : mix < o.mix;
+        }
+    };
+    std::map<Key, std::vector<std::pair<int64_t, BatchItem>>> by;
+    std::vector<int> b0s;
+    for (size_t p = 0; p < plans.size(); ++p) {
+        const RingBatchPlan& pl = plans[p];
+        const auto passes = ring_passes(pl.B, pl.rmax, adjoint, b0s);
+        for (size_t k = 0; k < passes.size(); ++k) {
+            auto& vec = by[Key{passes[k].first, passes[k].second, pl.mix}];
+            for (const RingItem& it : *pl.items) {
+                const int64_t cost = (int64_t)((it.n + 31) / 32) * (it.lend - it.lbeg + 1) *
+                                     passes[k].second;
+                vec.push_back({cost, BatchItem{it, (int)p, b0s[k]}});
+            }
+        }
+    }
+    for (auto& kv : by) {
+        auto& vec = kv.second;
+        std::stable_sort(vec.begin(), vec.end(),
+                         [](const auto& a, const auto& b) { return a.first > b.first; });
+        std::vector<BatchItem> items(vec.size());
+        for (size_t i = 0; i < vec.size(); ++i) items[i] = vec[i].second;
+        auto g = std::make_unique<RingBatchGroup>();
+        g->rmax = kv.first.rmax;
+        g->nb = kv.first.nb;
+        g->mix = kv.first.mix;
+        g->nitems = (int)items.size();
+        PF_TRY(g->items.alloc(sizeof(BatchItem) * std::max<size_t>(items.size(), 1)));
+        if (!items.empty())
+            PF_CUDA(cudaMemcpyAsync(g->items.p, items.data(), sizeof(BatchItem) * items.size(),
+                                    cudaMemcpyHostToDevice, s));
+        PF_CUDA(cudaStreamSynchronize(s));
+        groups.push_back(std::move(g));
+    }
+    return 0;
+}
+
+template <int RMAX, int NB, bool MIX>
+static int launch_fwd_batch(const RingSlot* slots, const RingBatchGroup& g, void* const* ptrs,
+                            cudaStream_t s) {
+    const int grid = (g.nitems + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    ring_fwd_batch_kernel<RMAX, NB, MIX><<<grid, kWarpsPerBlock * 32, 0, s>>>(
+        slots, g.items.as<BatchItem>(), g.nitems, ptrs);
+    return check_launch("ring_fwd_batch_kernel");
+}
+
+template <int RMAX, int NB, bool MIX>
+static int launch_adj_batch(const RingSlot* slots, const RingBatchGroup& g, void* const* ptrs,
+                            cudaStream_t s) {
+    const int grid = (g.nitems + kAdjWarps - 1) / kAdjWarps;
+    ring_adj_batch_kernel<RMAX, NB, MIX><<<grid, kAdjWarps * 32, 0, s>>>(
+        slots, g.items.as<BatchItem>(), g.nitems, ptrs);
+    return check_launch("ring_adj_batch_kernel");
+}
+
+template <bool MIX>
+static int fwd_batch_shape(const RingSlot* slots, const RingBatchGroup& g, void* const* ptrs,
+                           cudaStream_t s) {
+    if (g.nb == 4) return launch_fwd_batch<1, 4, MIX>(slots, g, ptrs, s);
+    if (g.nb == 2) return launch_fwd_batch<2, 2, MIX>(slots, g, ptrs, s);
+    if (g.rmax >= 4) return launch_fwd_batch<4, 1, MIX>(slots, g, ptrs, s);
+    return launch_fwd_batch<2, 1, MIX>(slots, g, ptrs, s);
+}
+
+template <bool MIX>
+static int adj_batch_shape(const RingSlot* slots, const RingBatchGroup& g, void* const* ptrs,
+                           cudaStream_t s) {
+    if (g.nb == 4) return launch_adj_batch<1, 4, MIX>(slots, g, ptrs, s);
+    if (g.nb == 2) return launch_adj_batch<2, 2, MIX>(slots, g, ptrs, s);
+    if (g.rmax >= 8) return launch_adj_batch<8, 1, MIX>(slots, g, ptrs, s);
+    if (g.rmax >= 4) return launch_adj_batch<4, 1, MIX>(slots, g, ptrs, s);
+    return launch_adj_batch<2, 1, MIX>(slots, g, ptrs, s);
+}
+
+int ring_forward_batch(const RingSlot* slots, const std::vector<std::unique_ptr<RingBatchGroup>>& groups,
+                       void* const* ptrs, cudaStream_t s) {
+    for (const auto& g : groups) {
+        if (g->nitems == 0) continue;
+        PF_TRY(g->mix ? fwd_batch_shape<true>(slots, *g, ptrs, s)
+                      : fwd_batch_shape<false>(slots, *g, ptrs, s));
+    }
+    return 0;
+}
+
+int ring_adjoint_batch(const RingSlot* slots, const std::vector<std::unique_ptr<RingBatchGroup>>& groups,
+                       void* const* ptrs, cudaStream_t s) {
+    for (const auto& g : groups) {
+        if (g->nitems == 0) continue;
+        PF_TRY(g->mix ? adj_batch_shape<true>(slots, *g, ptrs, s)
+                      : adj_batch_shape<false>(slots, *g, ptrs, s));
+    }
     return 0;
 }
 
