@@ -260,6 +260,122 @@ def accuracy(pf, plan, theta, phi, lmax, alm, fin, nsub, rng):
     return err, dot
 
 
+def batch_workload(nplans=64, seed=4):
+    """Plans of the batched configuration: lmax log-uniform in [128, 1024], cap radius uniform
+    in 5-30 degrees, M = round(4 (lmax theta*)^2) points, ntrans uniform in 1..8, tol 1e-6 (the
+    mixed form) or 1e-8 (FP64)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(nplans):
+        L = int(round(np.exp(rng.uniform(np.log(128), np.log(1024)))))
+        cap = np.deg2rad(rng.uniform(5.0, 30.0))
+        M = max(64, int(round(4 * (L * cap) ** 2)))
+        th = np.arccos(1 - (1 - np.cos(cap)) * rng.random(M))
+        ph = 2 * np.pi * rng.random(M)
+        B = int(rng.integers(1, 9))
+        tol = 1e-6 if rng.random() < 0.5 else 1e-8
+        out.append((L, th, ph, B, tol))
+    return out
+
+
+def run_batch(args, world, rank, local):
+    """--config batch: 64 plans, one launch sequence per plan with default tiles vs the
+    autotuned batch graph (both forward + adjoint of every plan per step)."""
+    import torch
+    from __graft_entry__ import load_package
+    pf = load_package()
+    import importlib
+    autotune = importlib.import_module("pfsht_b200.autotune")
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    specs = batch_workload()
+    t0 = time.perf_counter()
+    plain = [pf.Plan(th, ph, lmax=L, tol=tol, ntrans=B, precision="mixed" if tol >= 1e-6 else "fp64")
+             for (L, th, ph, B, tol) in specs]
+    build_plain = time.perf_counter() - t0
+    cache = os.path.join("/tmp", f"pfsht_tiles_{os.getpid()}.json")
+    t0 = time.perf_counter()
+    tuned = [autotune.tuned_plan(th, ph, lmax=L, tol=tol, ntrans=B, cache=cache,
+                                 precision="mixed" if tol >= 1e-6 else "fp64")
+             for (L, th, ph, B, tol) in specs]
+    tune_s = time.perf_counter() - t0
+    nclasses = len(json.load(open(cache)))
+    alms, fins, fouts, aouts = [], [], [], []
+    for p in plain:
+        a = pf.zeros_alm(p.lmax, p.ntrans, device=dev)
+        a.real.normal_()
+        a.imag.normal_()
+        f = pf.zeros_field(p.npts, p.ntrans, device=dev)
+        f.real.normal_()
+        f.imag.normal_()
+        alms.append(a)
+        fins.append(f)
+        fouts.append(pf.zeros_field(p.npts, p.ntrans, device=dev))
+        aouts.append(pf.zeros_alm(p.lmax, p.ntrans, device=dev))
+    stream = torch.cuda.current_stream(dev)
+
+    def timed(step, n):
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(n):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n
+
+    def per_plan():
+        for p, a, f, fo, ao in zip(plain, alms, fins, fouts, aouts):
+            p.mul(fo, a)
+            p.mul_adjoint(ao, f)
+
+    batch = pf.Batch(tuned, nstreams=8)
+
+    def batched():
+        batch.forward(fouts, alms)
+        batch.adjoint(aouts, fins)
+
+    batch_default = pf.Batch(plain, nstreams=8)
+
+    def batched_default():
+        batch_default.forward(fouts, alms)
+        batch_default.adjoint(aouts, fins)
+
+    steps = max(3, min(args.steps, 20))
+    ms_plain = timed(per_plan, steps)
+    ms_batch_default = timed(batched_default, steps)
+    ms_batch = timed(batched, steps)
+    del batch_default
+    info = batch.info()
+    triples = sum(p.ring_work() * p.ntrans for p in plain)
+    kinds = [p.info["kind"] for p in plain]
+    line = {
+        "metric": "ms per batch step (fwd+adj of 64 plans)", "value": ms_batch, "unit": "ms",
+        "n_gpus": 1, "steps": steps, "warmup": args.warmup, "higher_is_better": False,
+        "data": "synthetic", "config": {"workload": "batched: 64 plans, lmax log-uniform in "
+                                        "[128, 1024], cap 5-30 deg, M = 4 (lmax theta*)^2, "
+                                        "ntrans 1..8, tol 1e-6 (mixed) or 1e-8 (fp64)",
+                                        "seed": 4},
+        "one_launch_sequence_per_plan_ms": ms_plain, "speedup": ms_plain / ms_batch,
+        "batched_default_tiles_ms": ms_batch_default,
+        "ns_per_triple_batched": ms_batch * 1e6 / triples,
+        "ring_launches": [info["ring_launches_fwd"], info["ring_launches_adj"]],
+        "graph_nodes": [info["graph_nodes_fwd"], info["graph_nodes_adj"]],
+        "direct_plans": kinds.count("direct"), "mixed_plans": sum(p.info["precision"] == 1 for p in plain),
+        "autotune": {"seconds": tune_s, "shape_classes": nclasses}, "plan_build_s": build_plain,
+    }
+    del batch
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_serve(args, world, rank, local):
+    raise NotImplementedError("the serving loop is built in a later step")
+
+
 def run_b200(args, world, rank, local):
     import ctypes as C
 
@@ -446,6 +562,9 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-form measurement")
+    ap.add_argument("--config", default="headline", choices=["headline", "batch", "serve"],
+                    help="headline (default): the lmax 2048 cap; batch: 64 plans in one graph; "
+                         "serve: the request loop")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
@@ -454,6 +573,10 @@ def main():
         return run_reference(args, world, rank)
     world, rank, local = dist_setup(args.gpus)
     try:
+        if args.config == "batch":
+            return run_batch(args, world, rank, local) if rank == 0 else 0
+        if args.config == "serve":
+            return run_serve(args, world, rank, local) if rank == 0 else 0
         return run_b200(args, world, rank, local)
     finally:
         if world > 1:
