@@ -372,8 +372,117 @@ def run_batch(args, world, rank, local):
     return 0
 
 
+def serve_workload(nplans=32, seed=5):
+    """Plans of the serving configuration: lmax cycling through 128..2048, cap radius uniform in
+    5-30 degrees, M = round(4 (lmax theta*)^2), alternately FP64 at tol 1e-8 and mixed at 1e-6."""
+    rng = np.random.default_rng(seed)
+    Ls = (128, 256, 512, 1024, 2048)
+    out = []
+    for i in range(nplans):
+        L = Ls[i % len(Ls)]
+        cap = np.deg2rad(rng.uniform(5.0, 30.0))
+        M = max(64, int(round(4 * (L * cap) ** 2)))
+        th = np.arccos(1 - (1 - np.cos(cap)) * rng.random(M))
+        ph = 2 * np.pi * rng.random(M)
+        tol, prec = (1e-8, "fp64") if i % 2 == 0 else (1e-6, "mixed")
+        out.append((L, th, ph, tol, prec))
+    return out
+
+
+def measure_serving(pf, nreq=160, loads=(0.7, 1.0, 1.5), seed=6):
+    """Poisson arrivals of synthesis/adjoint requests (half each) over 32 resident plans, host
+    buffers in pinned memory: the serving loop against the unbatched path (each request a
+    synchronous host-buffer apply, in arrival order). Loads are multiples of the unbatched
+    path's capacity (1 / mean service time)."""
+    rng = np.random.default_rng(seed)
+    specs = serve_workload()
+    t0 = time.perf_counter()
+    plans = [pf.Plan(th, ph, lmax=L, tol=tol, precision=prec) for (L, th, ph, tol, prec) in specs]
+    build_s = time.perf_counter() - t0
+    bufs = []
+    for p in plans:
+        a = pf.zeros_alm(p.lmax, device="pinned")
+        a.real[...] = rng.standard_normal(a.shape)
+        f = pf.zeros_field(p.npts, device="pinned")
+        f.real[...] = rng.standard_normal(f.shape)
+        bufs.append((a, f, pf.zeros_field(p.npts, device="pinned"), pf.zeros_alm(p.lmax, device="pinned")))
+    reqs = [(int(rng.integers(len(plans))), bool(rng.integers(2))) for _ in range(nreq)]
+
+    def run_unbatched(arrivals):
+        lat = []
+        t_start = time.perf_counter()
+        for (i, fwd), ta in zip(reqs, arrivals):
+            now = time.perf_counter() - t_start
+            if now < ta:
+                time.sleep(ta - now)
+            a, f, fo, ao = bufs[i]
+            if fwd:
+                plans[i].mul(fo, a)
+            else:
+                plans[i].mul_adjoint(ao, f)
+            lat.append(time.perf_counter() - t_start - ta)
+        span = time.perf_counter() - t_start
+        return lat, span
+
+    # warm up, then the service time of the unbatched path (back to back)
+    run_unbatched([0.0] * nreq)
+    lat0, span0 = run_unbatched([0.0] * nreq)
+    service = span0 / nreq
+    srv = pf.Server(hbm_budget_gb=120, nslots=8)
+    ids = [srv.add(p) for p in plans]
+    resident = srv.stats()["bytes_resident"]
+
+    def run_server(arrivals):
+        rids = []
+        t_start = time.perf_counter()
+        for (i, fwd), ta in zip(reqs, arrivals):
+            now = time.perf_counter() - t_start
+            if now < ta:
+                time.sleep(ta - now)
+            a, f, fo, ao = bufs[i]
+            rids.append(srv.submit(ids[i], fwd, a if fwd else f, fo if fwd else ao))
+        lat = [srv.wait(r) for r in rids]
+        times = [srv.times(r) for r in rids]
+        for r in rids:
+            srv.release(r)
+        span = max(t[2] for t in times) - min(t[0] for t in times)
+        return lat, span
+
+    run_server(np.zeros(nreq))
+    out = []
+    for load in loads:
+        rate = load / service
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, nreq))
+        lu, su = run_unbatched(arrivals)
+        ls, ss = run_server(arrivals)
+        pct = lambda v, q: float(np.percentile(np.asarray(v) * 1e3, q))
+        out.append({"load": load, "rate_rps": rate,
+                    "server": {"p50_ms": pct(ls, 50), "p99_ms": pct(ls, 99), "rps": nreq / ss},
+                    "unbatched": {"p50_ms": pct(lu, 50), "p99_ms": pct(lu, 99), "rps": nreq / su}})
+    srv.close()
+    return {"plans": len(plans), "requests_per_rate": nreq, "hbm_budget_gb": 120,
+            "resident_gb": resident / 1e9, "unbatched_service_ms": service * 1e3,
+            "plan_build_s": build_s, "rates": out,
+            "workload": "32 resident plans (lmax 128..2048, cap 5-30 deg, M = 4 (lmax theta*)^2, "
+                        "fp64 at 1e-8 / mixed at 1e-6), Poisson arrivals, half synthesis half "
+                        "adjoint, host buffers in pinned memory; unbatched = synchronous "
+                        "host-buffer applies in arrival order"}
+
+
 def run_serve(args, world, rank, local):
-    raise NotImplementedError("the serving loop is built in a later step")
+    """--config serve: the serving loop alone."""
+    import torch
+    from __graft_entry__ import load_package
+    pf = load_package()
+    torch.cuda.set_device(local)
+    res = measure_serving(pf)
+    mid = res["rates"][1]
+    line = {"metric": "serve p50/p99 latency and requests/s", "value": mid["server"]["p99_ms"],
+            "unit": "ms (p99 at the unbatched path's capacity)", "n_gpus": 1,
+            "higher_is_better": False, "data": "synthetic", "config": {"workload": res["workload"]},
+            "serve": res}
+    print(json.dumps(line), flush=True)
+    return 0
 
 
 def run_b200(args, world, rank, local):
@@ -484,6 +593,9 @@ def run_b200(args, world, rank, local):
                  "note": "FP64 recurrence and exponents, FP32 compensated ring sums, FP32 "
                          "NUFFT (w=7); same points, inputs and timing as the headline"}
         del pm
+    serve = None
+    if not args.no_serve and world == 1:
+        serve = measure_serving(pf)
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
@@ -537,6 +649,7 @@ def run_b200(args, world, rank, local):
         "accuracy": {"tol": args.tol, "l2_rel_vs_direct": err, "dot_rel": dot,
                      "sample": "4096 seeded points, FP64 direct evaluation on the device"},
         "mixed": mixed,
+        "serve": serve,
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_ms / world, "unit": "ms",
                 "h2d_bytes_per_step": hb["h2d_forward"] + hb["h2d_adjoint"],
@@ -562,6 +675,7 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-form measurement")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving measurement")
     ap.add_argument("--config", default="headline", choices=["headline", "batch", "serve"],
                     help="headline (default): the lmax 2048 cap; batch: 64 plans in one graph; "
                          "serve: the request loop")

@@ -164,6 +164,32 @@ pfsht_status pfsht_batch_info(const pfsht_batch* batch, int32_t* ring_launches_f
                               int64_t* graph_nodes_adj);
 pfsht_status pfsht_batch_destroy(pfsht_batch* batch);
 
+/* Serving loop (no reference counterpart): plans resident on one device and a worker thread
+ * that runs synthesis (forward = 1) and adjoint requests on HOST arrays as they arrive. Plans are
+ * registered against hbm_budget_bytes (each counts its device memory plus its staging buffers;
+ * a registration past the budget returns PFSHT_ERR_OUT_OF_MEMORY). A request starts as soon as
+ * one of nslots streams is free and its plan is idle: requests for different plans overlap on
+ * the device, requests for one plan run in arrival order. submit returns at once with an id;
+ * wait blocks until that request is done (timeout_s < 0: no limit; PFSHT_ERR_TIMEOUT when it
+ * runs out) and gives its latency from submission. Host arrays must stay valid until their
+ * request is done; pinned arrays let copies of one request overlap another's kernels.
+ * Registered plans must outlive the server and must not be applied elsewhere meanwhile.
+ * Times are seconds since the server was created; release forgets a finished request. */
+typedef struct pfsht_server pfsht_server;
+pfsht_status pfsht_server_create(int32_t device, int64_t hbm_budget_bytes, int32_t nslots,
+                                 pfsht_server** out);
+pfsht_status pfsht_server_add_plan(pfsht_server* server, pfsht_plan* plan, int32_t* plan_id);
+pfsht_status pfsht_server_submit(pfsht_server* server, int32_t plan_id, int32_t forward,
+                                 const void* in, void* out, int64_t* request_id);
+pfsht_status pfsht_server_wait(pfsht_server* server, int64_t request_id, double timeout_s,
+                               double* latency_s);
+pfsht_status pfsht_server_request_times(pfsht_server* server, int64_t request_id,
+                                        double* t_submit, double* t_start, double* t_done);
+pfsht_status pfsht_server_release(pfsht_server* server, int64_t request_id);
+pfsht_status pfsht_server_stats(pfsht_server* server, int64_t* completed, int64_t* queued,
+                                int64_t* running, int64_t* bytes_resident);
+pfsht_status pfsht_server_destroy(pfsht_server* server);
+
 /* FMA-throughput microbenchmark on the current device (no reference counterpart): runs a
  * grid of independent FP64 (fp64 = 1) or FP32 FMA chains and reports FLOP/s (2 per FMA).
  * These are the denominators of the ring-pass and NUFFT FLOP rooflines. */

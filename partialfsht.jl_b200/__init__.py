@@ -23,7 +23,7 @@ import numpy as np
 from . import _lib
 from ._lib import DimensionMismatch, PFSHTError, RefusedGeometry  # noqa: F401
 
-__all__ = ["Plan", "AdjointPlan", "Batch", "mul", "coeff_size", "sph_mode", "zeros_alm", "zeros_field",
+__all__ = ["Plan", "AdjointPlan", "Batch", "Server", "mul", "coeff_size", "sph_mode", "zeros_alm", "zeros_field",
            "plan_geometry", "ring_forward", "ring_adjoint", "NUFFT", "DimensionMismatch",
            "RefusedGeometry", "PFSHTError", "version"]
 
@@ -53,9 +53,19 @@ def _torch():
     return torch
 
 
+def _pinned(shape):
+    """Zero complex128 numpy array of `shape` in page-locked host memory, column-major."""
+    torch = _torch()
+    t = torch.zeros(tuple(reversed(shape)), dtype=torch.complex128).pin_memory()
+    return t.numpy().T  # the array's base keeps the pinned tensor alive
+
+
 def zeros_alm(lmax: int, ntrans: int = 1, device="cuda"):
-    """Zero coefficient array, Julia shape (lmax+1, 2lmax+1[, ntrans]), column-major."""
+    """Zero coefficient array, Julia shape (lmax+1, 2lmax+1[, ntrans]), column-major.
+    ``device`` is a torch device, "cpu" (numpy) or "pinned" (numpy in page-locked memory)."""
     nr, nc = coeff_size(lmax)
+    if device == "pinned":
+        return _pinned((nr, nc) if ntrans == 1 else (nr, nc, ntrans))
     if device in (None, "cpu", "host"):
         shape = (nr, nc) if ntrans == 1 else (nr, nc, ntrans)
         return np.zeros(shape, dtype=np.complex128, order="F")
@@ -65,7 +75,9 @@ def zeros_alm(lmax: int, ntrans: int = 1, device="cuda"):
 
 
 def zeros_field(npts: int, ntrans: int = 1, device="cuda"):
-    """Zero field, Julia shape (npts[, ntrans]), column-major."""
+    """Zero field, Julia shape (npts[, ntrans]), column-major (devices as for zeros_alm)."""
+    if device == "pinned":
+        return _pinned((npts,) if ntrans == 1 else (npts, ntrans))
     if device in (None, "cpu", "host"):
         shape = (npts,) if ntrans == 1 else (npts, ntrans)
         return np.zeros(shape, dtype=np.complex128, order="F")
@@ -441,6 +453,74 @@ class Batch:
                                                 C.byref(d)), "batch info")
         return {"ring_launches_fwd": a.value, "ring_launches_adj": b.value,
                 "graph_nodes_fwd": c.value, "graph_nodes_adj": d.value}
+
+
+class Server:
+    """Serving loop (pfsht_server_*): plans resident on one device, synthesis and adjoint
+    requests on host arrays run as they arrive, concurrently across plans, within an HBM
+    budget for the resident plans. Registered plans must outlive the server."""
+
+    def __init__(self, hbm_budget_gb=120.0, nslots=8, device=None):
+        self._h = None
+        h = C.c_void_p()
+        dev = -1 if device is None else int(device)
+        _lib.check(_lib.load().pfsht_server_create(dev, int(hbm_budget_gb * 1e9), int(nslots),
+                                                   C.byref(h)), "server")
+        self._h = h
+        self.plans = []
+        self._keep = {}
+
+    def add(self, plan) -> int:
+        pid = C.c_int32()
+        _lib.check(_lib.load().pfsht_server_add_plan(self._h, plan._h, C.byref(pid)), "add_plan")
+        self.plans.append(plan)
+        return pid.value
+
+    def submit(self, plan_id, forward, inp, out) -> int:
+        """Queue mul!(out, plan, inp) (forward) or mul!(out, plan', inp); host arrays."""
+        p = self.plans[plan_id]
+        cs, fs = _coeff_shapes(p.lmax, p.ntrans), _field_shapes(p.npts, p.ntrans)
+        _check_array(inp, cs if forward else fs, "input")
+        _check_array(out, fs if forward else cs, "output")
+        if _is_torch(inp) or _is_torch(out):
+            raise ValueError("server requests take host (numpy) arrays")
+        rid = C.c_int64()
+        _lib.check(_lib.load().pfsht_server_submit(self._h, int(plan_id), 1 if forward else 0,
+                                                   _ptr(inp), _ptr(out), C.byref(rid)), "submit")
+        self._keep[rid.value] = (inp, out)
+        return rid.value
+
+    def wait(self, rid, timeout=None) -> float:
+        """Block until request `rid` is done; returns its latency in seconds."""
+        lat = C.c_double()
+        _lib.check(_lib.load().pfsht_server_wait(self._h, int(rid), -1.0 if timeout is None
+                                                 else float(timeout), C.byref(lat)), "wait")
+        return lat.value
+
+    def times(self, rid):
+        """(submitted, started, done) in seconds since the server was created."""
+        a, b, c = C.c_double(), C.c_double(), C.c_double()
+        _lib.check(_lib.load().pfsht_server_request_times(self._h, int(rid), C.byref(a),
+                                                          C.byref(b), C.byref(c)), "times")
+        return a.value, b.value, c.value
+
+    def release(self, rid):
+        _lib.check(_lib.load().pfsht_server_release(self._h, int(rid)), "release")
+        self._keep.pop(rid, None)
+
+    def stats(self) -> dict:
+        v = [C.c_int64() for _ in range(4)]
+        _lib.check(_lib.load().pfsht_server_stats(self._h, *[C.byref(x) for x in v]), "stats")
+        return dict(zip(("completed", "queued", "running", "bytes_resident"), [x.value for x in v]))
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h and _lib is not None and _lib._lib is not None:
+            _lib._lib.pfsht_server_destroy(h)
+        self._h = None
+        self._keep = {}
+
+    __del__ = close
 
 
 class NUFFT:

@@ -76,6 +76,16 @@ SIGNATURES = {
     "pfsht_batch_info": (C.c_int, [_vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                    C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "pfsht_batch_destroy": (C.c_int, [_vp]),
+    "pfsht_server_create": (C.c_int, [C.c_int32, C.c_int64, C.c_int32, C.POINTER(_vp)]),
+    "pfsht_server_add_plan": (C.c_int, [_vp, _vp, C.POINTER(C.c_int32)]),
+    "pfsht_server_submit": (C.c_int, [_vp, C.c_int32, C.c_int32, _vp, _vp, C.POINTER(C.c_int64)]),
+    "pfsht_server_wait": (C.c_int, [_vp, C.c_int64, C.c_double, C.POINTER(C.c_double)]),
+    "pfsht_server_request_times": (C.c_int, [_vp, C.c_int64, C.POINTER(C.c_double),
+                                             C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "pfsht_server_release": (C.c_int, [_vp, C.c_int64]),
+    "pfsht_server_stats": (C.c_int, [_vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                     C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "pfsht_server_destroy": (C.c_int, [_vp]),
     "pfsht_profile_start": (C.c_int, [_vp, C.c_int32]),
     "pfsht_profile_stop": (C.c_int, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
     "pfsht_num_stages": (C.c_int32, []),

@@ -567,13 +567,21 @@ static void alm_zero_host_padding(const pfsht_plan* p, void* host) {
     }
 }
 
-static int host_apply(pfsht_plan* p, const void* in, void* out, bool fwd) {
-    DeviceGuard dg(p->device);
+}  // extern "C"
+
+namespace pf {
+
+int plan_host_staging(pfsht_plan* p) {
     const size_t na = sizeof(double2) * (size_t)(p->L + 1) * (2 * p->L + 1) * p->B;
     const size_t nf = sizeof(double2) * (size_t)p->M * p->B;
     if (!p->st_alm.p) PF_TRY(p->st_alm.alloc(na));
     if (!p->st_f.p) PF_TRY(p->st_f.alloc(nf));
-    cudaStream_t s = p->st_stream;
+    return 0;
+}
+
+int plan_host_enqueue(pfsht_plan* p, const void* in, void* out, bool fwd, cudaStream_t s) {
+    PF_TRY(plan_host_staging(p));
+    const size_t nf = sizeof(double2) * (size_t)p->M * p->B;
     if (fwd) {
         // the forward reads rows 0 .. lmax - m of each order only
         PF_TRY(alm_copy(p, const_cast<void*>(in), true, s));
@@ -585,6 +593,17 @@ static int host_apply(pfsht_plan* p, const void* in, void* out, bool fwd) {
         PF_TRY(alm_copy(p, out, false, s));
         alm_zero_host_padding(p, out);
     }
+    return 0;
+}
+
+}  // namespace pf
+
+extern "C" {
+
+static int host_apply(pfsht_plan* p, const void* in, void* out, bool fwd) {
+    DeviceGuard dg(p->device);
+    cudaStream_t s = p->st_stream;
+    PF_TRY(plan_host_enqueue(p, in, out, fwd, s));
     PF_CUDA(cudaStreamSynchronize(s));
     return 0;
 }

@@ -66,4 +66,12 @@ struct DeviceGuard {
 int plan_forward_after_ring(pfsht_plan* p, double2* f, cudaStream_t s);
 int plan_adjoint_before_ring(pfsht_plan* p, const double2* f, cudaStream_t s);
 
+// The host-buffer apply without its final synchronisation: copies in (the coefficient
+// staircase or the field), applies on the plan's staging buffers and copies out, all on `s`;
+// for the adjoint it also zeroes the host array's padding rows on host threads before it
+// returns. The host arrays must stay valid until `s` reaches this point.
+int plan_host_enqueue(pfsht_plan* p, const void* in, void* out, bool fwd, cudaStream_t s);
+// allocate the plan's staging buffers for host-buffer applies
+int plan_host_staging(pfsht_plan* p);
+
 }  // namespace pf
