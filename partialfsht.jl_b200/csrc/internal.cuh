@@ -227,6 +227,8 @@ struct NufftGrid {
     int ncols = 0;             // mode columns
     int bin_rows = 16, bin_cols = 16, nbr = 0, nbc = 0;
     int nbusy = 0;             // bins holding at least one point
+    int igroup = 1;            // interpolation: consecutive bins of a bin row per block
+    int nsbc = 0, nisb = 0;    // groups per bin row; non-empty groups
     int fp32 = 0;              // fine grids, FFTs, spreading and interpolation in FP32
     int64_t M = 0;
 };
@@ -236,6 +238,7 @@ struct NufftDev {
     DevBuf perm;      // int32 original index, bin order
     DevBuf binstart;  // int32 nbins + 1
     DevBuf binorder;  // int32 nbusy: non-empty bins, most points first
+    DevBuf iorder;    // int32 nisb: non-empty interpolation groups, most points first
     DevBuf colp2;     // int32 ncols: fine column of each mode column
     DevBuf p2col;     // int32 nf2: mode column of each fine column or -1
     DevBuf mult1;     // double2 n1: per-mode complex factor along dim 1 (deconv incl.)

@@ -260,6 +260,21 @@ int nufft_setpts(NufftGrid& g, NufftDev& d, const double* x, const double* y, cu
     if (!order.empty())
         PF_CUDA(cudaMemcpyAsync(d.binorder.p, order.data(), sizeof(int) * order.size(),
                                 cudaMemcpyHostToDevice, s));
+    // interpolation groups igroup consecutive bins of a bin row; non-empty groups, most
+    // points first
+    g.igroup = std::max(1, g.igroup);
+    g.nsbc = (g.nbc + g.igroup - 1) / g.igroup;
+    std::vector<int> gcnt((size_t)g.nbr * g.nsbc, 0);
+    for (int b = 0; b < nbins; ++b) gcnt[(size_t)(b / g.nbc) * g.nsbc + (b % g.nbc) / g.igroup] += cnt[b];
+    std::vector<int> gorder;
+    for (int q = 0; q < (int)gcnt.size(); ++q)
+        if (gcnt[q] > 0) gorder.push_back(q);
+    std::stable_sort(gorder.begin(), gorder.end(), [&](int a, int b) { return gcnt[a] > gcnt[b]; });
+    g.nisb = (int)gorder.size();
+    PF_TRY(d.iorder.alloc(sizeof(int) * std::max<size_t>(gorder.size(), 1)));
+    if (!gorder.empty())
+        PF_CUDA(cudaMemcpyAsync(d.iorder.p, gorder.data(), sizeof(int) * gorder.size(),
+                                cudaMemcpyHostToDevice, s));
     PF_CUDA(cudaStreamSynchronize(s));
     return 0;
 }
@@ -488,20 +503,24 @@ __device__ __forceinline__ T es_poly(int a, T v) {
     return p;
 }
 
-// Type-2 interpolation: one CTA per bin copies the bin's tile of U into shared memory, then
-// each thread interpolates points of the bin from it. The row weights are evaluated row by
+// Type-2 interpolation: one CTA per group of consecutive bins of a bin row copies the group's
+// tile of U (at most 32 columns) into shared memory, then each thread interpolates points of
+// the group from it. The row weights are evaluated row by
 // row inside the tap loop so only the column weights are held in registers.
 template <int W, class T>
-__global__ void __launch_bounds__(128, 5)
+__global__ void __launch_bounds__(128, sizeof(T) == 8 ? 5 : 4)
 interp_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
-              const int* __restrict__ binstart, const int* __restrict__ binorder, int nbc,
-              int BR, int BC, int64_t M, const cx<T>* __restrict__ U, int nrows, int nf2,
-              int row_wrap, int B, double2* __restrict__ f) {
+              const int* __restrict__ binstart, const int* __restrict__ iorder, int nbc, int G,
+              int nsbc, int BR, int BC, int64_t M, const cx<T>* __restrict__ U, int nrows,
+              int nf2, int row_wrap, int B, double2* __restrict__ f) {
     extern __shared__ __align__(16) unsigned char interp_smem[];
     cx<T>* tile = reinterpret_cast<cx<T>*>(interp_smem);
-    const int bin = binorder[blockIdx.x];
-    const int s = binstart[bin], e = binstart[bin + 1];
-    const TileGeom tg = tile_geom<W>(bin, nbc, BR, BC);
+    // a group of G consecutive bins of one bin row: their points are contiguous in bin order
+    const int sb = iorder[blockIdx.x];
+    const int br = sb / nsbc, sg = sb % nsbc;
+    const int s = binstart[br * nbc + sg * G];
+    const int e = binstart[br * nbc + min(nbc, sg * G + G)];
+    const TileGeom tg{br * BR, sg * G * BC, BR + W - 1, G * BC + W - 1};
     for (int b = 0; b < B; ++b) {
         const cx<T>* ub = U + (int64_t)nrows * nf2 * b;
         for (int t = threadIdx.x; t < tg.TR * tg.TC; t += blockDim.x) {
@@ -511,10 +530,32 @@ interp_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
             if (r >= 0 && r < nrows) v = ub[(int64_t)r * nf2 + wrap(tg.tc0 + t % tg.TC, nf2)];
             tile[t] = v;
         }
+        // FP32 grids: the first point's coordinates load while the tile copy completes and
+        // each later point's load is issued one iteration ahead (in FP64 the extra registers
+        // cost more occupancy than the hidden latency gains)
+        constexpr bool kAhead = sizeof(T) == 4;
+        int p = s + threadIdx.x;
+        double2 gn = make_double2(0.0, 0.0);
+        int jn = 0;
+        if (kAhead && p < e) {
+            gn = pts[p];
+            jn = perm[p];
+        }
         __syncthreads();
-        for (int p = s + threadIdx.x; p < e; p += blockDim.x) {
-            const double2 g = pts[p];
-            const int j = perm[p];
+        for (; p < e; p += blockDim.x) {
+            double2 g;
+            int j;
+            if constexpr (kAhead) {
+                g = gn;
+                j = jn;
+                if (p + (int)blockDim.x < e) {
+                    gn = pts[p + blockDim.x];
+                    jn = perm[p + blockDim.x];
+                }
+            } else {
+                g = pts[p];
+                j = perm[p];
+            }
             int r0, c0;
             double v1, v2;
             local_origin<W>(g, tg, nrows, nf2, row_wrap, r0, c0, v1, v2);
@@ -810,12 +851,13 @@ spread16_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
 
 template <int W, class T>
 static int launch_interp(const NufftGrid& g, NufftDev& d, double2* f, int B, cudaStream_t s) {
-    const size_t smem = sizeof(cx<T>) * (g.bin_rows + W - 1) * (g.bin_cols + W - 1);
+    const size_t smem = sizeof(cx<T>) * (g.bin_rows + W - 1) * (g.igroup * g.bin_cols + W - 1);
     if (smem > 48 * 1024)
         PF_CUDA(cudaFuncSetAttribute(interp_kernel<W, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    interp_kernel<W, T><<<g.nbusy, 128, smem, s>>>(
-        d.pts.as<double2>(), d.perm.as<int>(), d.binstart.as<int>(), d.binorder.as<int>(), g.nbc,
-        g.bin_rows, g.bin_cols, g.M, d.U.as<cx<T>>(), g.nrows, g.nf2, g.row_wrap, B, f);
+    interp_kernel<W, T><<<g.nisb, 128, smem, s>>>(
+        d.pts.as<double2>(), d.perm.as<int>(), d.binstart.as<int>(), d.iorder.as<int>(), g.nbc,
+        g.igroup, g.nsbc, g.bin_rows, g.bin_cols, g.M, d.U.as<cx<T>>(), g.nrows, g.nf2,
+        g.row_wrap, B, f);
     return check_launch("interp_kernel");
 }
 

@@ -78,6 +78,8 @@ int setup_nufft_grid(NufftGrid& g, NufftDev& d, int n1, int nmodes2, const std::
     g.bin_rows = bin_rows > 0 ? bin_rows : (half ? 24 : 12);
     g.bin_cols = (half ? 17 : 33) - g.w;
     if (bin_cols > 0 && bin_cols < g.bin_cols) g.bin_cols = bin_cols;
+    // interpolation tiles of up to 32 columns: as many whole bins as fit
+    g.igroup = std::max(1, (33 - g.w) / g.bin_cols);
     if (full_rows) {
         g.row0 = 0;
         g.nrows = g.nf1;
