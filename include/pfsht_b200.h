@@ -63,7 +63,11 @@ typedef struct pfsht_opts {
     int32_t ring_segment_degrees; /* adjoint ring pass: split each order into degree segments of
                                      about this length, started from recurrence states saved at
                                      plan time (0 = auto, < 0 = never split) */
-    int32_t reserved[7];
+    int32_t nufft_fft_lengths;  /* NUFFT fine-grid FFT lengths: 0 = the fastest library FFT among
+                                   the 7-smooth lengths within 10% above the minimum (timed at
+                                   plan time, once per process and shape); 1 = the minimum
+                                   2,3,5-smooth lengths >= 2n (deterministic, as FINUFFT) */
+    int32_t reserved[6];
 } pfsht_opts;
 
 typedef struct pfsht_plan pfsht_plan;
@@ -120,7 +124,8 @@ pfsht_status pfsht_plan_get_info(const pfsht_plan* plan, pfsht_plan_info* info);
 int64_t pfsht_workspace_bytes(const pfsht_plan* plan);
 
 /* Host-only plan geometry, no device touched: what pfsht_plan_create would choose for
- * these points (kind, sizes, ring_work). Points are host pointers. */
+ * these points (kind, sizes, ring_work). Points are host pointers. nf1/nf2 are the minimum
+ * fine-grid lengths; a plan built with timed lengths may use longer ones (pfsht_plan_get_info). */
 pfsht_status pfsht_plan_geometry(const double* theta, const double* phi, int64_t npts,
                                  int32_t lmax, int32_t ntrans, double tol,
                                  const pfsht_opts* opts, pfsht_plan_info* info);

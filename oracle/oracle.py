@@ -99,6 +99,8 @@ def lib():
         "orc_esnufft_params": (None, [vp, C.POINTER(C.c_int), C.POINTER(C.c_double),
                                       C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "orc_esnufft_exec": (None, [vp, C.c_int, C.c_int, vp, vp, C.c_int]),
+        "orc_esnufft_set_grid": (C.c_int, [vp, C.c_int, C.c_int]),
+        "orc_stretch_set_nufft_grid": (C.c_int, [vp, C.c_int, C.c_int]),
         "orc_es_kernel": (C.c_double, [C.c_double, C.c_double]),
         "orc_es_deconv": (C.c_double, [C.c_int, C.c_int, C.c_int, C.c_double]),
         "orc_direct_create": (vp, [_dp, _dp, C.c_int64, C.c_int, C.c_int]),
@@ -437,12 +439,14 @@ def nufft_direct(typ, n1, n2, iflag, x, y, inp):
 class ESNufft:
     """CPU ES-kernel NUFFT (published FINUFFT algorithm)."""
 
-    def __init__(self, n1, n2, x, y, tol, ntrans=1, kernel="poly"):
+    def __init__(self, n1, n2, x, y, tol, ntrans=1, kernel="poly", grid=None):
         self.x = _f64(x)
         self.y = _f64(y)
         self.n1, self.n2, self.B = int(n1), int(n2), int(ntrans)
         self._h = lib().orc_esnufft_create_k(self.n1, self.n2, self.B, float(tol), self.x,
                                              self.y, len(self.x), 1 if kernel == "poly" else 0)
+        if grid is not None and lib().orc_esnufft_set_grid(self._h, int(grid[0]), int(grid[1])):
+            raise ValueError("fine-grid lengths below the minimum")
 
     def __del__(self):
         if getattr(self, "_h", None):
@@ -510,10 +514,11 @@ class RefusedGeometry(ValueError):
 class Stretch:
     """StretchLeaf (src/Stretch.jl:94-295) with DirectSum (exact, nufft="direct"), the ES
     NUFFT with FINUFFT's polynomial kernel evaluation (nufft="es") or with the exact kernel
-    (nufft="es_exact")."""
+    (nufft="es_exact"). nufft_grid = (nf1, nf2) sets the ES NUFFT's fine-grid lengths (default:
+    the minimum 2,3,5-smooth lengths), e.g. to those of a device plan."""
 
     def __init__(self, theta, phi, lmax, tol, ntrans=1, nufft="es", eps_apo_max=1.0,
-                 oversample_theta=1.0, oversample_phi=1.0):
+                 oversample_theta=1.0, oversample_phi=1.0, nufft_grid=None):
         self.theta = _f64(theta)
         self.phi = _f64(phi)
         self.M = len(self.theta)
@@ -527,6 +532,9 @@ class Stretch:
             if st.value == 1:
                 raise RefusedGeometry("stretched transform is degenerate at this lmax and tol")
             raise ValueError("bad arguments")
+        if nufft_grid is not None and lib().orc_stretch_set_nufft_grid(
+                self._h, int(nufft_grid[0]), int(nufft_grid[1])):
+            raise ValueError("nufft_grid needs an ES NUFFT and lengths >= the minimum")
         i = _StretchInfo()
         lib().orc_stretch_info_get(self._h, C.byref(i))
         self.info = {name: getattr(i, name) for name, _ in _StretchInfo._fields_}

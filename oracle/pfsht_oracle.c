@@ -1025,6 +1025,19 @@ void orc_esnufft_destroy(orc_esnufft* p) {
     free(p);
 }
 
+/* Fine-grid lengths other than the minimum (any nf1 >= max(2 n1, 2 w), likewise nf2): the
+ * per-mode deconvolution follows the lengths. Used to mirror a device plan's lengths. */
+int orc_esnufft_set_grid(orc_esnufft* p, int nf1, int nf2) {
+    if (nf1 < 2 * p->n1 || nf1 < 2 * p->w || nf2 < 2 * p->n2 || nf2 < 2 * p->w) return 1;
+    p->nf1 = nf1;
+    p->nf2 = nf2;
+    for (int i = 0; i < p->n1; ++i) p->dec1[i] = orc_es_deconv(orc_mode_k(i, p->n1, 1), nf1, p->w, p->beta);
+    for (int i = 0; i < p->n2; ++i) p->dec2[i] = orc_es_deconv(orc_mode_k(i, p->n2, 1), nf2, p->w, p->beta);
+    free(p->grid);
+    p->grid = (cplx*)malloc(sizeof(cplx) * (size_t)nf1 * nf2);
+    return 0;
+}
+
 void orc_esnufft_params(const orc_esnufft* p, int* w, double* beta, int* nf1, int* nf2) {
     if (w) *w = p->w;
     if (beta) *beta = p->beta;
@@ -1397,6 +1410,10 @@ void orc_stretch_destroy(orc_stretch* s) {
 }
 
 void orc_stretch_info_get(const orc_stretch* s, orc_stretch_info* out) { *out = s->info; }
+
+int orc_stretch_set_nufft_grid(orc_stretch* s, int nf1, int nf2) {
+    return s->es ? orc_esnufft_set_grid(s->es, nf1, nf2) : 1;
+}
 const orc_rings* orc_stretch_rings_engine(const orc_stretch* s) { return s->eng; }
 
 void orc_stretch_tables(const orc_stretch* s, double* th_r, double* Th_r, double* w,

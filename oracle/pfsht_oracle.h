@@ -95,6 +95,7 @@ orc_esnufft* orc_esnufft_create_k(int n1, int n2, int ntrans, double tol, const 
                                   const double* y, int64_t M, int kermode);
 void orc_esnufft_destroy(orc_esnufft*);
 void orc_esnufft_params(const orc_esnufft*, int* w, double* beta, int* nf1, int* nf2);
+int orc_esnufft_set_grid(orc_esnufft*, int nf1, int nf2);  /* 0 = ok, 1 = lengths too short */
 void orc_esnufft_exec(orc_esnufft*, int type, int iflag, const double* in, double* out,
                       int nthreads);
 double orc_es_kernel(double z, double beta);
@@ -124,6 +125,7 @@ orc_stretch* orc_stretch_create(const double* theta, const double* phi, int64_t 
                                 double oversample_theta, double oversample_phi, int* status);
 void orc_stretch_destroy(orc_stretch*);
 void orc_stretch_info_get(const orc_stretch*, orc_stretch_info*);
+int orc_stretch_set_nufft_grid(orc_stretch*, int nf1, int nf2);  /* ES NUFFT leaves only */
 void orc_stretch_tables(const orc_stretch*, double* theta_rings, double* Theta_rings,
                         double* window, double* Theta_pts, double* phi_pts);
 void orc_stretch_forward(orc_stretch*, const double* alm, double* f, int nthreads);

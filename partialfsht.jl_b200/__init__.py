@@ -155,12 +155,15 @@ class Plan:
     ``precision`` is "fp64" (plain form) or "mixed". Points may be host arrays or CUDA
     tensors (float64). ``rings_per_lane`` / ``bin_rows`` / ``bin_cols`` are device tile
     shapes (0 = defaults); ``segment_degrees`` splits the adjoint ring pass along the degree
-    axis (0 = auto, negative = never).
+    axis (0 = auto, negative = never). ``fft_lengths`` is "timed" (NUFFT fine-grid lengths
+    picked by timing the library FFT, the default) or "minimal" (the smallest 2,3,5-smooth
+    lengths, deterministic); ``info["nf1"]``, ``info["nf2"]`` give the lengths in use.
     """
 
     def __init__(self, theta, phi, *, lmax, tol=1e-10, ntrans=1, method="auto",
                  precision="fp64", oversample_theta=1.0, oversample_phi=1.0, eps_apo_max=1.0,
-                 device=None, rings_per_lane=0, bin_rows=0, bin_cols=0, segment_degrees=0):
+                 device=None, rings_per_lane=0, bin_rows=0, bin_cols=0, segment_degrees=0,
+                 fft_lengths="timed"):
         self._h = None
         if len(theta) != len(phi):
             raise DimensionMismatch("θ and φ must have the same length")
@@ -181,6 +184,9 @@ class Plan:
         o.nufft_bin_rows = int(bin_rows)
         o.nufft_bin_cols = int(bin_cols)
         o.ring_segment_degrees = int(segment_degrees)
+        if fft_lengths not in ("timed", "minimal"):
+            raise ValueError(f"unknown fft_lengths {fft_lengths!r}")
+        o.nufft_fft_lengths = 0 if fft_lengths == "timed" else 1
         if _is_torch(theta):
             torch = _torch()
             th = theta.to(torch.float64).contiguous()

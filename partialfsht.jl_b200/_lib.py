@@ -23,7 +23,8 @@ class Opts(C.Structure):
                 ("ring_rings_per_lane", C.c_int32), ("nufft_bin_rows", C.c_int32),
                 ("nufft_bin_cols", C.c_int32), ("oversample_theta", C.c_double),
                 ("oversample_phi", C.c_double), ("eps_apo_max", C.c_double),
-                ("ring_segment_degrees", C.c_int32), ("reserved", C.c_int32 * 7)]
+                ("ring_segment_degrees", C.c_int32), ("nufft_fft_lengths", C.c_int32),
+                ("reserved", C.c_int32 * 6)]
 
 
 class PlanInfo(C.Structure):

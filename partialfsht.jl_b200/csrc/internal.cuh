@@ -253,6 +253,10 @@ struct NufftDev {
 // transform points (x = stretched colatitude, y = longitude; both radians) into grid
 // coordinates, sort them into bins, fill pts/perm/binstart. x,y are device arrays.
 int nufft_setpts(NufftGrid& g, NufftDev& d, const double* x, const double* y, cudaStream_t s);
+// fine-grid FFT length for a dimension of minimum length nmin: the fastest batched library FFT
+// (batch sequences, FP32 or FP64) among the 7-smooth lengths in [nmin, 1.1 nmin], timed on the
+// device once per process for each (nmin, batch, type)
+int fine_fft_length(int nmin, int64_t batch, bool fp32, cudaStream_t s, int* out);
 // allocate pad/U and plan the fine-grid FFTs for B transforms
 int nufft_alloc(NufftGrid& g, NufftDev& d, int B);
 // type 2 from mode columns (n1 x ncols x B, FFT order along dim 1) to values f (M x B)

@@ -21,6 +21,10 @@
 #include <atomic>
 #include <cmath>
 
+#include <map>
+#include <mutex>
+#include <tuple>
+
 #include "es_horner_table.h"
 #include "internal.cuh"
 
@@ -276,6 +280,96 @@ int nufft_setpts(NufftGrid& g, NufftDev& d, const double* x, const double* y, cu
         PF_CUDA(cudaMemcpyAsync(d.iorder.p, gorder.data(), sizeof(int) * gorder.size(),
                                 cudaMemcpyHostToDevice, s));
     PF_CUDA(cudaStreamSynchronize(s));
+    return 0;
+}
+
+// ---------------------------------------------------------------------------------------
+// fine-grid FFT lengths: any length >= the minimum serves the NUFFT (the deconvolution uses the
+// actual length), and the library FFT's speed varies by a factor ~3 between neighbouring smooth
+// lengths, so the lengths are picked by timing.
+// ---------------------------------------------------------------------------------------
+namespace {
+
+bool smooth7(int64_t n) {
+    for (int p : {2, 3, 5, 7})
+        while (n % p == 0) n /= p;
+    return n == 1;
+}
+
+struct LenKey {
+    int nmin;
+    int64_t batch;
+    int fp32;
+    bool operator<(const LenKey& o) const {
+        return std::tie(nmin, batch, fp32) < std::tie(o.nmin, o.batch, o.fp32);
+    }
+};
+std::mutex g_len_mu;
+std::map<LenKey, int> g_len_cache;
+
+// device time of one batched in-place FFT of length n (ms), or a large value when the library
+// cannot plan it
+double time_fft(int n, int64_t batch, bool fp32, void* buf, cudaStream_t s) {
+    cufftHandle h;
+    int nn[1] = {n};
+    if (cufftPlanMany(&h, 1, nn, nn, 1, n, nn, 1, n, fp32 ? CUFFT_C2C : CUFFT_Z2Z, (int)batch) !=
+        CUFFT_SUCCESS)
+        return 1e30;
+    cufftSetStream(h, s);
+    auto run = [&] {
+        if (fp32) cufftExecC2C(h, (cufftComplex*)buf, (cufftComplex*)buf, CUFFT_FORWARD);
+        else cufftExecZ2Z(h, (cufftDoubleComplex*)buf, (cufftDoubleComplex*)buf, CUFFT_FORWARD);
+    };
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    run();
+    run();
+    cudaEventRecord(e0, s);
+    for (int k = 0; k < 3; ++k) run();
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cufftDestroy(h);
+    return ms / 3;
+}
+
+}  // namespace
+
+int fine_fft_length(int nmin, int64_t batch, bool fp32, cudaStream_t s, int* out) {
+    *out = nmin;
+    std::vector<int> cand;
+    for (int64_t n = nmin; n <= nmin + nmin / 10 && cand.size() < 12; ++n)
+        if (smooth7(n)) cand.push_back((int)n);
+    if (cand.size() < 2 || batch < 1) return 0;
+    const LenKey key{nmin, batch, fp32 ? 1 : 0};
+    std::lock_guard<std::mutex> lk(g_len_mu);
+    auto it = g_len_cache.find(key);
+    if (it != g_len_cache.end()) {
+        *out = it->second;
+        return 0;
+    }
+    // time on at most 256 MB of scratch (a smaller batch ranks the lengths alike)
+    const size_t el = fp32 ? sizeof(float2) : sizeof(double2);
+    const int64_t bm = std::max<int64_t>(1, std::min<int64_t>(batch, ((int64_t)256 << 20) / ((int64_t)cand.back() * el)));
+    DevBuf scratch;
+    PF_TRY(scratch.alloc(el * (size_t)bm * cand.back()));
+    PF_CUDA(cudaMemsetAsync(scratch.p, 0, el * (size_t)bm * cand.back(), s));
+    std::vector<double> t(cand.size());
+    for (size_t i = 0; i < cand.size(); ++i) t[i] = time_fft(cand[i], bm, fp32, scratch.p, s);
+    PF_CUDA(cudaStreamSynchronize(s));
+    PF_CUDA(cudaGetLastError());
+    // the shortest length within 5% of the fastest (a longer grid costs the other stages more)
+    const double best = *std::min_element(t.begin(), t.end());
+    for (size_t i = 0; i < cand.size(); ++i)
+        if (t[i] <= 1.05 * best) {
+            *out = cand[i];
+            break;
+        }
+    g_len_cache[key] = *out;
     return 0;
 }
 

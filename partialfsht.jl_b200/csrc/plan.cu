@@ -62,15 +62,21 @@ int upload(DevBuf& d, const std::vector<T>& h, cudaStream_t s) {
 int mode_k(int i, int n) { return i < (n + 1) / 2 ? i : i - n; }
 
 // NUFFT grid and per-mode factors; n1 modes along dim 1, columns -> k2 via colk2
+// timed: fine-grid FFT lengths picked by timing (fine_fft_length), else the minimum
+// 2,3,5-smooth lengths
 int setup_nufft_grid(NufftGrid& g, NufftDev& d, int n1, int nmodes2, const std::vector<int>& colk2,
                      const std::vector<double2>& phase1, double tol, int64_t M, double xmin,
-                     double xmax, bool full_rows, int bin_rows, int bin_cols, cudaStream_t s) {
+                     double xmax, bool full_rows, int bin_rows, int bin_cols, bool fp32, bool timed,
+                     cudaStream_t s) {
     g.w = es_width(tol);
     g.beta = 2.30 * g.w;
+    g.fp32 = fp32 ? 1 : 0;
     g.nf1 = (int)next_smooth(std::max<int64_t>(2 * (int64_t)n1, 2 * g.w));
     g.nf2 = (int)next_smooth(std::max<int64_t>(2 * (int64_t)nmodes2, 2 * g.w));
     g.n1 = n1;
     g.ncols = (int)colk2.size();
+    // timed for one transform, so that plans of one geometry share lengths whatever ntrans
+    if (timed) PF_TRY(fine_fft_length(g.nf1, g.ncols, fp32, s, &g.nf1));
     g.M = M;
     // the spreading tile (bin width + w - 1 columns) is half a warp wide for kernels up to
     // 10 cells (two half-warps share its rows by parity), one warp wide beyond
@@ -99,6 +105,7 @@ int setup_nufft_grid(NufftGrid& g, NufftDev& d, int n1, int nmodes2, const std::
             g.row_wrap = 0;
         }
     }
+    if (timed) PF_TRY(fine_fft_length(g.nf2, g.nrows, fp32, s, &g.nf2));
     std::vector<double2> mult1(n1);
     for (int i = 0; i < n1; ++i) {
         const double dec = es_deconv(mode_k(i, n1), g.nf1, g.w, g.beta);
@@ -263,8 +270,8 @@ int build_stretch(pfsht_plan* p, const double* d_theta, const double* d_phi, con
     std::vector<int> colk2(p->ncols);
     for (int c = 0; c < p->ncols; ++c) colk2[c] = c - lf.mmax;
     PF_TRY(setup_nufft_grid(p->ng, p->nd, lf.nth, lf.nph, colk2, phase, p->tol, p->M, Tmin, Tmax,
-                            false, o.nufft_bin_rows, o.nufft_bin_cols, s));
-    p->ng.fp32 = p->precision == PFSHT_PRECISION_MIXED;
+                            false, o.nufft_bin_rows, o.nufft_bin_cols,
+                            p->precision == PFSHT_PRECISION_MIXED, o.nufft_fft_lengths == 0, s));
     PF_TRY(nufft_setpts(p->ng, p->nd, Th.as<double>(), ph.as<double>(), s));
     PF_TRY(nufft_alloc(p->ng, p->nd, B));
     return 0;
@@ -791,7 +798,8 @@ pfsht_status pfsht_nufft_create(int32_t type, int32_t n1, int32_t n2, int32_t if
     std::vector<int> colk2(n2);
     for (int c = 0; c < n2; ++c) colk2[c] = mode_k(c, n2);
     std::vector<double2> ones(n1, make_double2(1.0, 0.0));
-    r = setup_nufft_grid(p->g, p->d, n1, n2, colk2, ones, tol, M, 0.0, 0.0, true, 0, 0, nullptr);
+    r = setup_nufft_grid(p->g, p->d, n1, n2, colk2, ones, tol, M, 0.0, 0.0, true, 0, 0, false,
+                         true, nullptr);
     if (!r) r = nufft_setpts(p->g, p->d, dx.as<double>(), dy.as<double>(), nullptr);
     if (!r) r = nufft_alloc(p->g, p->d, ntrans);
     if (r) return (pfsht_status)r;

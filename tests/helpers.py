@@ -43,3 +43,8 @@ def dot_rel(f, g, alm, a):
     lhs = np.vdot(np.ravel(f, order="F"), np.ravel(g, order="F"))
     rhs = np.vdot(np.ravel(alm, order="F"), np.ravel(a, order="F"))
     return abs(lhs - rhs) / abs(lhs)
+
+
+def plan_grid(plan):
+    """The NUFFT fine-grid lengths a device plan uses (for the oracle's ES NUFFT)."""
+    return plan.info["nf1"], plan.info["nf2"]

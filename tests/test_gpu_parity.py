@@ -3,7 +3,7 @@ Mirrors the reference's gpu/runtests.jl and test/test_transforms.jl gates."""
 import numpy as np
 import pytest
 
-from helpers import cap_points, cn, dot_rel, rel, to_dev, to_host
+from helpers import cap_points, cn, dot_rel, plan_grid, rel, to_dev, to_host
 
 pytestmark = pytest.mark.gpu
 
@@ -14,7 +14,7 @@ def test_ring_pass_matches_oracle(pf, O, cuda, L):
     rng = np.random.default_rng(11)
     th, ph = cap_points(4000, rng=rng)
     plan = pf.Plan(th, ph, lmax=L, tol=1e-8)
-    ref = O.Stretch(th, ph, L, 1e-8, nufft="es")
+    ref = O.Stretch(th, ph, L, 1e-8, nufft="es", nufft_grid=plan_grid(plan))
     alm = O.rand_alm(L, rng=rng)
     G_ref = ref.rings.rings_from_alm(alm)
     n = plan.info["nrings"]
@@ -36,7 +36,7 @@ def test_stretch_apply_matches_oracle(pf, O, cuda, L):
     M = 4 * int(round((L * np.deg2rad(20)) ** 2))
     th, ph = cap_points(M, rng=rng)
     plan = pf.Plan(th, ph, lmax=L, tol=1e-8)
-    ref = O.Stretch(th, ph, L, 1e-8, nufft="es")
+    ref = O.Stretch(th, ph, L, 1e-8, nufft="es", nufft_grid=plan_grid(plan))
     alm = O.rand_alm(L, rng=rng)
     f = to_host(plan * to_dev(alm[:, :, 0]))
     f_ref = ref.forward(alm, nthreads=8)[:, 0]

@@ -4,7 +4,7 @@ batching, determinism and the degree-split adjoint ring pass."""
 import numpy as np
 import pytest
 
-from helpers import cap_points, cn, dot_rel, rel, to_dev, to_host
+from helpers import cap_points, cn, dot_rel, plan_grid, rel, to_dev, to_host
 
 pytestmark = pytest.mark.gpu
 
@@ -88,7 +88,7 @@ def test_off_pole_and_southern_patches(pf, O, cuda, centre):
     g = cn(rng, 150)
     assert dot_rel(f, g, alm[:, :, 0], _adj(ps, g)) < 1e-12
     # and the device apply agrees with the oracle's own stretched leaf at round-off
-    so = O.Stretch(th, ph, L, tol, nufft="es")
+    so = O.Stretch(th, ph, L, tol, nufft="es", nufft_grid=plan_grid(ps))
     assert rel(f, so.forward(alm)[:, 0]) < 1e-11
     assert O.alm_reldiff(_adj(ps, g), so.adjoint(g)[:, :, 0], L) < 1e-10
 
@@ -101,7 +101,7 @@ def test_interior_patch_matches_oracle(pf, O, cuda):
     ph = 2 * np.pi * rng.random(3000)
     ps = pf.Plan(th, ph, lmax=L, tol=1e-8, method="stretch")
     assert ps.info["kind"] == "interior"
-    so = O.Stretch(th, ph, L, 1e-8, nufft="es")
+    so = O.Stretch(th, ph, L, 1e-8, nufft="es", nufft_grid=plan_grid(ps))
     alm = O.rand_alm(L, rng=rng)
     f = _fwd(ps, alm)
     assert rel(f, so.forward(alm, nthreads=8)[:, 0]) < 1e-11
@@ -204,7 +204,7 @@ def test_adjoint_degree_segments_match_oracle(pf, O, cuda, seg):
     L = 512
     th, ph = cap_points(6000, rng=rng)
     plan = pf.Plan(th, ph, lmax=L, tol=1e-8, segment_degrees=seg)
-    ref = O.Stretch(th, ph, L, 1e-8, nufft="es")
+    ref = O.Stretch(th, ph, L, 1e-8, nufft="es", nufft_grid=plan_grid(plan))
     n = plan.info["nrings"]
     Gr = np.asfortranarray(cn(rng, n, 2 * L + 1, 1))
     a = to_dev(np.zeros((L + 1, 2 * L + 1, 1), np.complex128, order="F"))
@@ -246,6 +246,49 @@ def test_nufft_seam_matches_direct_sum(pf, O, cuda, typ):
         out = to_dev(np.zeros((n1, n2), np.complex128, order="F"))
         p.exec(to_dev(c), out)
         ref = O.nufft_direct(1, n1, n2, -1, x, y, c)[:, :, 0]
+    assert rel(to_host(out), ref) < 200 * tol
+
+
+def test_timed_fine_grid_lengths(pf, O, cuda):
+    # NUFFT fine-grid lengths picked by timing the library FFT: within 10% above the minimum,
+    # the same for the same shape within a process, and the transform agrees with the
+    # minimal-length plan to the tolerance
+    rng = np.random.default_rng(90)
+    th, ph = cap_points(20000, rng=rng)
+    L, tol = 700, 1e-8
+    pt = pf.Plan(th, ph, lmax=L, tol=tol)
+    pm = pf.Plan(th, ph, lmax=L, tol=tol, fft_lengths="minimal")
+    geo = pf.plan_geometry(th, ph, lmax=L, tol=tol)
+    assert plan_grid(pm) == (geo["nf1"], geo["nf2"])
+    for a, b in zip(plan_grid(pt), plan_grid(pm)):
+        assert b <= a <= b + b // 10
+    assert plan_grid(pf.Plan(th, ph, lmax=L, tol=tol)) == plan_grid(pt)
+    alm = O.rand_alm(L, rng=rng)
+    assert rel(_fwd(pt, alm), _fwd(pm, alm)) < 10 * tol
+    g = cn(rng, len(th))
+    assert O.alm_reldiff(_adj(pt, g), _adj(pm, g), L) < 10 * tol
+    with pytest.raises(ValueError):
+        pf.Plan(th, ph, lmax=L, tol=tol, fft_lengths="fast")
+
+
+@pytest.mark.parametrize("typ,iflag", [(1, 1), (1, -1), (2, 1), (2, -1)])
+def test_nufft_seam_both_signs_odd_sizes(pf, O, cuda, typ, iflag):
+    # either exponent sign in both types, odd mode counts
+    rng = np.random.default_rng(82 + typ + iflag)
+    n1, n2, M, tol = 45, 27, 700, 1e-9
+    x = 2 * np.pi * rng.random(M) - np.pi
+    y = 2 * np.pi * rng.random(M)
+    p = pf.NUFFT(typ, n1, n2, iflag, x, y, tol)
+    if typ == 2:
+        c = np.asfortranarray(cn(rng, n1, n2))
+        out = to_dev(np.zeros(M, np.complex128))
+        p.exec(to_dev(c), out)
+        ref = O.nufft_direct(2, n1, n2, iflag, x, y, c)[:, 0]
+    else:
+        c = cn(rng, M)
+        out = to_dev(np.zeros((n1, n2), np.complex128, order="F"))
+        p.exec(to_dev(c), out)
+        ref = O.nufft_direct(1, n1, n2, iflag, x, y, c)[:, :, 0]
     assert rel(to_host(out), ref) < 200 * tol
 
 

@@ -166,6 +166,23 @@ def test_es_nufft_vs_direct_sum(O, tol):
         assert rel(es.exec(1, iflag, f), ref1) < 200 * tol
 
 
+@pytest.mark.parametrize("grid", [(84, 128), (96, 147), (105, 135)])
+def test_es_nufft_longer_fine_grids(O, grid):
+    # fine grids above the minimum (2 n) keep the accuracy: the deconvolution follows the length
+    rng = np.random.default_rng(83)
+    n1, n2, M, tol = 40, 64, 300, 1e-9
+    x = 2 * np.pi * rng.random(M)
+    y = 2 * np.pi * rng.random(M)
+    c = cn(rng, n1, n2)
+    es = O.ESNufft(n1, n2, x, y, tol, grid=grid)
+    assert (es.params()["nf1"], es.params()["nf2"]) == grid
+    assert rel(es.exec(2, 1, c), O.nufft_direct(2, n1, n2, 1, x, y, c)) < 200 * tol
+    f = cn(rng, M)
+    assert rel(es.exec(1, -1, f), O.nufft_direct(1, n1, n2, -1, x, y, f)) < 200 * tol
+    with pytest.raises(ValueError):
+        O.ESNufft(n1, n2, x, y, tol, grid=(79, 128))
+
+
 def test_es_nufft_type1_is_adjoint_of_type2(O):
     rng = np.random.default_rng(82)
     n1, n2, M = 32, 48, 500
