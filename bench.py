@@ -178,6 +178,14 @@ def run_reference(args, world, rank):
     return 0
 
 
+def fft_lengths_arg(v):
+    """--fft-lengths: "timed", "minimal" or N1xN2."""
+    if v in ("timed", "minimal"):
+        return v
+    a, b = v.lower().split("x")
+    return int(a), int(b)
+
+
 def config_dict(args, M):
     return {"workload": f"stretched-leaf fwd+adj, lmax={args.lmax}, 20deg polar cap, M={M}, "
                         f"tol={args.tol:g}, {args.precision}, ntrans=1",
@@ -504,7 +512,7 @@ def run_b200(args, world, rank, local):
     M, theta, phi, rng = workload(args.lmax)
     t0 = time.perf_counter()
     plan = pf.Plan(theta, phi, lmax=args.lmax, tol=args.tol, precision=args.precision,
-                   device=local)
+                   device=local, fft_lengths=fft_lengths_arg(args.fft_lengths))
     torch.cuda.synchronize()
     build_s = time.perf_counter() - t0
     info = plan.info
@@ -640,7 +648,9 @@ def run_b200(args, world, rank, local):
         "metric": "ms per fwd+adj apply", "value": value, "unit": "ms", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": config_dict(args, M),
+        "data": "synthetic",
+        "config": dict(config_dict(args, M), nufft_lengths=[info["nf1"], info["nf2"]],
+                       fft_lengths=args.fft_lengths),
         "ns_per_triple": ms_per_step * 1e6 / info["ring_work"],
         "ring_work": info["ring_work"],
         "plan_build_s": build_s,
@@ -673,6 +683,8 @@ def main():
     ap.add_argument("--lmax", type=int, default=2048)
     ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--fft-lengths", default="timed",
+                    help='NUFFT fine-grid FFT lengths: "timed" (plan default), "minimal" or N1xN2')
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-form measurement")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving measurement")

@@ -66,8 +66,10 @@ typedef struct pfsht_opts {
     int32_t nufft_fft_lengths;  /* NUFFT fine-grid FFT lengths: 0 = the fastest library FFT among
                                    the 7-smooth lengths within 10% above the minimum (timed at
                                    plan time, once per process and shape); 1 = the minimum
-                                   2,3,5-smooth lengths >= 2n (deterministic, as FINUFFT) */
-    int32_t reserved[6];
+                                   2,3,5-smooth lengths >= 2n (deterministic, as FINUFFT);
+                                   2 = nufft_nf1 x nufft_nf2 as given (each >= its minimum) */
+    int32_t nufft_nf1, nufft_nf2;
+    int32_t reserved[4];
 } pfsht_opts;
 
 typedef struct pfsht_plan pfsht_plan;

@@ -156,8 +156,9 @@ class Plan:
     tensors (float64). ``rings_per_lane`` / ``bin_rows`` / ``bin_cols`` are device tile
     shapes (0 = defaults); ``segment_degrees`` splits the adjoint ring pass along the degree
     axis (0 = auto, negative = never). ``fft_lengths`` is "timed" (NUFFT fine-grid lengths
-    picked by timing the library FFT, the default) or "minimal" (the smallest 2,3,5-smooth
-    lengths, deterministic); ``info["nf1"]``, ``info["nf2"]`` give the lengths in use.
+    picked by timing the library FFT, the default), "minimal" (the smallest 2,3,5-smooth
+    lengths, deterministic) or a pair (nf1, nf2) of lengths at or above the minimum;
+    ``info["nf1"]``, ``info["nf2"]`` give the lengths in use.
     """
 
     def __init__(self, theta, phi, *, lmax, tol=1e-10, ntrans=1, method="auto",
@@ -184,9 +185,13 @@ class Plan:
         o.nufft_bin_rows = int(bin_rows)
         o.nufft_bin_cols = int(bin_cols)
         o.ring_segment_degrees = int(segment_degrees)
-        if fft_lengths not in ("timed", "minimal"):
+        if isinstance(fft_lengths, (tuple, list)) and len(fft_lengths) == 2:
+            o.nufft_fft_lengths = 2
+            o.nufft_nf1, o.nufft_nf2 = int(fft_lengths[0]), int(fft_lengths[1])
+        elif fft_lengths in ("timed", "minimal"):
+            o.nufft_fft_lengths = 0 if fft_lengths == "timed" else 1
+        else:
             raise ValueError(f"unknown fft_lengths {fft_lengths!r}")
-        o.nufft_fft_lengths = 0 if fft_lengths == "timed" else 1
         if _is_torch(theta):
             torch = _torch()
             th = theta.to(torch.float64).contiguous()

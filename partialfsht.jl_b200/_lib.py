@@ -24,7 +24,7 @@ class Opts(C.Structure):
                 ("nufft_bin_cols", C.c_int32), ("oversample_theta", C.c_double),
                 ("oversample_phi", C.c_double), ("eps_apo_max", C.c_double),
                 ("ring_segment_degrees", C.c_int32), ("nufft_fft_lengths", C.c_int32),
-                ("reserved", C.c_int32 * 6)]
+                ("nufft_nf1", C.c_int32), ("nufft_nf2", C.c_int32), ("reserved", C.c_int32 * 4)]
 
 
 class PlanInfo(C.Structure):

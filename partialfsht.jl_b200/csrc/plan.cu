@@ -62,12 +62,12 @@ int upload(DevBuf& d, const std::vector<T>& h, cudaStream_t s) {
 int mode_k(int i, int n) { return i < (n + 1) / 2 ? i : i - n; }
 
 // NUFFT grid and per-mode factors; n1 modes along dim 1, columns -> k2 via colk2
-// timed: fine-grid FFT lengths picked by timing (fine_fft_length), else the minimum
-// 2,3,5-smooth lengths
+// lengths: 0 = fine-grid FFT lengths picked by timing (fine_fft_length), 1 = the minimum
+// 2,3,5-smooth lengths, 2 = nf1 x nf2 as given
 int setup_nufft_grid(NufftGrid& g, NufftDev& d, int n1, int nmodes2, const std::vector<int>& colk2,
                      const std::vector<double2>& phase1, double tol, int64_t M, double xmin,
-                     double xmax, bool full_rows, int bin_rows, int bin_cols, bool fp32, bool timed,
-                     cudaStream_t s) {
+                     double xmax, bool full_rows, int bin_rows, int bin_cols, bool fp32, int lengths,
+                     int nf1, int nf2, cudaStream_t s) {
     g.w = es_width(tol);
     g.beta = 2.30 * g.w;
     g.fp32 = fp32 ? 1 : 0;
@@ -75,6 +75,16 @@ int setup_nufft_grid(NufftGrid& g, NufftDev& d, int n1, int nmodes2, const std::
     g.nf2 = (int)next_smooth(std::max<int64_t>(2 * (int64_t)nmodes2, 2 * g.w));
     g.n1 = n1;
     g.ncols = (int)colk2.size();
+    const bool timed = lengths == 0;
+    if (lengths == 2) {
+        if (nf1 < std::max(2 * n1, 2 * g.w) || nf2 < std::max(2 * nmodes2, 2 * g.w) || nf1 > (1 << 24) ||
+            nf2 > (1 << 24))
+            return fail(PFSHT_ERR_ARGUMENT, "fine-grid lengths must be at least " +
+                                                std::to_string(std::max(2 * n1, 2 * g.w)) + " x " +
+                                                std::to_string(std::max(2 * nmodes2, 2 * g.w)));
+        g.nf1 = nf1;
+        g.nf2 = nf2;
+    }
     // timed for one transform, so that plans of one geometry share lengths whatever ntrans
     if (timed) PF_TRY(fine_fft_length(g.nf1, g.ncols, fp32, s, &g.nf1));
     g.M = M;
@@ -271,7 +281,8 @@ int build_stretch(pfsht_plan* p, const double* d_theta, const double* d_phi, con
     for (int c = 0; c < p->ncols; ++c) colk2[c] = c - lf.mmax;
     PF_TRY(setup_nufft_grid(p->ng, p->nd, lf.nth, lf.nph, colk2, phase, p->tol, p->M, Tmin, Tmax,
                             false, o.nufft_bin_rows, o.nufft_bin_cols,
-                            p->precision == PFSHT_PRECISION_MIXED, o.nufft_fft_lengths == 0, s));
+                            p->precision == PFSHT_PRECISION_MIXED, o.nufft_fft_lengths, o.nufft_nf1,
+                            o.nufft_nf2, s));
     PF_TRY(nufft_setpts(p->ng, p->nd, Th.as<double>(), ph.as<double>(), s));
     PF_TRY(nufft_alloc(p->ng, p->nd, B));
     return 0;
@@ -341,6 +352,8 @@ int plan_create(const double* theta, const double* phi, int64_t npts, int lmax, 
     if (!(o.oversample_theta >= 1) || !(o.oversample_phi >= 1))
         return fail(PFSHT_ERR_ARGUMENT, "oversampling factors must be >= 1");
     if (!(o.eps_apo_max > 0)) return fail(PFSHT_ERR_ARGUMENT, "eps_apo_max must be positive");
+    if (o.nufft_fft_lengths < 0 || o.nufft_fft_lengths > 2)
+        return fail(PFSHT_ERR_ARGUMENT, "nufft_fft_lengths must be 0 (timed), 1 (minimal) or 2 (given)");
     DeviceGuard dg(o.device);
     int dev = 0;
     PF_CUDA(cudaGetDevice(&dev));
@@ -798,8 +811,8 @@ pfsht_status pfsht_nufft_create(int32_t type, int32_t n1, int32_t n2, int32_t if
     std::vector<int> colk2(n2);
     for (int c = 0; c < n2; ++c) colk2[c] = mode_k(c, n2);
     std::vector<double2> ones(n1, make_double2(1.0, 0.0));
-    r = setup_nufft_grid(p->g, p->d, n1, n2, colk2, ones, tol, M, 0.0, 0.0, true, 0, 0, false,
-                         true, nullptr);
+    r = setup_nufft_grid(p->g, p->d, n1, n2, colk2, ones, tol, M, 0.0, 0.0, true, 0, 0, false, 0,
+                         0, 0, nullptr);
     if (!r) r = nufft_setpts(p->g, p->d, dx.as<double>(), dy.as<double>(), nullptr);
     if (!r) r = nufft_alloc(p->g, p->d, ntrans);
     if (r) return (pfsht_status)r;

@@ -269,6 +269,12 @@ def test_timed_fine_grid_lengths(pf, O, cuda):
     assert O.alm_reldiff(_adj(pt, g), _adj(pm, g), L) < 10 * tol
     with pytest.raises(ValueError):
         pf.Plan(th, ph, lmax=L, tol=tol, fft_lengths="fast")
+    # lengths given explicitly: the same transform as the timed plan that chose them
+    pg = pf.Plan(th, ph, lmax=L, tol=tol, fft_lengths=plan_grid(pt))
+    assert plan_grid(pg) == plan_grid(pt)
+    assert np.array_equal(_fwd(pg, alm), _fwd(pt, alm))
+    with pytest.raises(ValueError):
+        pf.Plan(th, ph, lmax=L, tol=tol, fft_lengths=(pm.info["nf1"] - 1, pm.info["nf2"]))
 
 
 @pytest.mark.parametrize("typ,iflag", [(1, 1), (1, -1), (2, 1), (2, -1)])
