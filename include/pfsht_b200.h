@@ -37,7 +37,14 @@ typedef enum {
     PFSHT_ERR_UNSUPPORTED = 7     /* option not built into this library */
 } pfsht_status;
 
-typedef enum { PFSHT_METHOD_AUTO = 0, PFSHT_METHOD_STRETCH = 1, PFSHT_METHOD_DIRECT = 2 } pfsht_method;
+/* AbstractAlgorithm (src/Cost.jl:15-30): AUTO is the cost model's choice (select_method,
+ * src/Cost.jl:171-201) among the stretched leaf, Direct and MultiBox. */
+typedef enum {
+    PFSHT_METHOD_AUTO = 0,
+    PFSHT_METHOD_STRETCH = 1,
+    PFSHT_METHOD_DIRECT = 2,
+    PFSHT_METHOD_MULTIBOX = 3   /* one stretched leaf per box of a partition (src/MultiBox.jl) */
+} pfsht_method;
 
 typedef enum {
     PFSHT_PRECISION_FP64 = 0,   /* plain form: FP64 everywhere */
@@ -46,7 +53,10 @@ typedef enum {
                                    the FP64 form (pfsht_plan_info.precision says which). */
 } pfsht_precision;
 
-typedef enum { PFSHT_KIND_POLE = 0, PFSHT_KIND_INTERIOR = 1, PFSHT_KIND_FULL = 2, PFSHT_KIND_DIRECT = 3 } pfsht_kind;
+typedef enum {
+    PFSHT_KIND_POLE = 0, PFSHT_KIND_INTERIOR = 1, PFSHT_KIND_FULL = 2, PFSHT_KIND_DIRECT = 3,
+    PFSHT_KIND_MULTIBOX = 4
+} pfsht_kind;
 
 /* Plan options: the keyword arguments of Plan(...) (src/Plan.jl:84-97) that change the
  * apply, plus the device knobs. Fill with pfsht_opts_default first. */
@@ -69,7 +79,8 @@ typedef struct pfsht_opts {
                                    2,3,5-smooth lengths >= 2n (deterministic, as FINUFFT);
                                    2 = nufft_nf1 x nufft_nf2 as given (each >= its minimum) */
     int32_t nufft_nf1, nufft_nf2;
-    int32_t reserved[4];
+    int32_t maxboxes;           /* MultiBox: at most this many boxes (src/Plan.jl:93; 0 = 8) */
+    int32_t reserved[3];
 } pfsht_opts;
 
 typedef struct pfsht_plan pfsht_plan;
@@ -124,6 +135,42 @@ pfsht_status pfsht_ring_adjoint(pfsht_plan* plan, const void* G, void* alm, void
 int64_t pfsht_ring_work(const pfsht_plan* plan);
 pfsht_status pfsht_plan_get_info(const pfsht_plan* plan, pfsht_plan_info* info);
 int64_t pfsht_workspace_bytes(const pfsht_plan* plan);
+
+/* ---- planner (src/Box.jl, src/Cost.jl), host only ---------------------------------------- */
+
+/* SphereBox (src/Box.jl:23-30): colatitude extent and the longitude arc from phi_start. */
+typedef struct pfsht_box {
+    double theta_lo, theta_hi, phi_start, phi_extent;
+    int32_t touches_north, touches_south;
+} pfsht_box;
+
+/* bounding_box (src/Box.jl:42-73): exact colatitude extent, longitude arc = complement of the
+ * largest circular gap (O(n), no sort). */
+pfsht_status pfsht_bounding_box(const double* theta, const double* phi, int64_t npts, pfsht_box* box);
+/* cost_direct / cost_stretch (src/Cost.jl:107-142) in the cost constants' units; cost_stretch is
+ * +inf where the stretched construction refuses the geometry. */
+double pfsht_cost_direct(int64_t npts, int32_t lmax, int32_t ntrans);
+double pfsht_cost_stretch(const pfsht_box* box, int64_t npts, int32_t lmax, int32_t ntrans, double tol);
+/* partition_boxes_costed (src/Box.jl:156-200) with cost_stretch: group_of_point[i] = box of point
+ * i (0-based, in the order boxes are reported); boxes / costs hold maxboxes entries. */
+pfsht_status pfsht_partition_boxes(const double* theta, const double* phi, int64_t npts,
+                                   int32_t lmax, int32_t ntrans, double tol, int32_t maxboxes,
+                                   int32_t* group_of_point, int32_t* nboxes, pfsht_box* boxes,
+                                   double* costs);
+/* select_method (src/Cost.jl:171-201) for AUTO: *method = STRETCH, DIRECT or MULTIBOX. */
+pfsht_status pfsht_select_method(const double* theta, const double* phi, int64_t npts,
+                                 int32_t lmax, int32_t ntrans, double tol, int32_t* method);
+/* set_cost_constants! / cost_calibrated (src/Cost.jl:60-74): process-wide per-unit costs. */
+pfsht_status pfsht_set_cost_constants(double ring, double fft, double spread, double ft_conn);
+pfsht_status pfsht_get_cost_constants(double* ring, double* fft, double* spread, double* ft_conn,
+                                      int32_t* calibrated);
+
+/* Boxes of a MultiBox plan (1 for a single-leaf plan, whose box is the plan itself): the box's
+ * stretched leaf geometry and, if indices is not NULL, its points (ascending 0-based indices
+ * into the plan's point set; info.npts of them). */
+int32_t pfsht_plan_num_boxes(const pfsht_plan* plan);
+pfsht_status pfsht_plan_box(const pfsht_plan* plan, int32_t box, pfsht_plan_info* info,
+                            int64_t* indices);
 
 /* Host-only plan geometry, no device touched: what pfsht_plan_create would choose for
  * these points (kind, sizes, ring_work). Points are host pointers. nf1/nf2 are the minimum

@@ -25,7 +25,9 @@ from ._lib import DimensionMismatch, PFSHTError, RefusedGeometry  # noqa: F401
 
 __all__ = ["Plan", "AdjointPlan", "Batch", "Server", "mul", "coeff_size", "sph_mode", "zeros_alm", "zeros_field",
            "plan_geometry", "ring_forward", "ring_adjoint", "NUFFT", "DimensionMismatch",
-           "RefusedGeometry", "PFSHTError", "version"]
+           "RefusedGeometry", "PFSHTError", "version", "bounding_box", "box_fsky", "cost_direct",
+           "cost_stretch", "partition_boxes", "select_method", "cost_constants",
+           "set_cost_constants", "cost_calibrated"]
 
 _lib.load()
 
@@ -150,8 +152,10 @@ def _stream_of(a, stream):
 class Plan:
     """Plan(theta, phi; lmax, tol=1e-10, ntrans=1, method="auto") (src/Plan.jl:84-116).
 
-    ``method`` is "auto" (stretched leaf, or the direct leaf where the stretched geometry is
-    refused, src/Cost.jl:121-122), "stretch" (refusal raises RefusedGeometry) or "direct".
+    ``method`` is "auto" (the cost model's choice among the stretched leaf, the direct leaf
+    and the multi-box leaf, src/Cost.jl:171-201), "stretch" (refusal raises RefusedGeometry),
+    "direct" or "multibox" (one stretched leaf per box of the partition, at most ``maxboxes``,
+    src/MultiBox.jl; ``boxes()`` lists them).
     ``precision`` is "fp64" (plain form) or "mixed". Points may be host arrays or CUDA
     tensors (float64). ``rings_per_lane`` / ``bin_rows`` / ``bin_cols`` are device tile
     shapes (0 = defaults); ``segment_degrees`` splits the adjoint ring pass along the degree
@@ -164,7 +168,7 @@ class Plan:
     def __init__(self, theta, phi, *, lmax, tol=1e-10, ntrans=1, method="auto",
                  precision="fp64", oversample_theta=1.0, oversample_phi=1.0, eps_apo_max=1.0,
                  device=None, rings_per_lane=0, bin_rows=0, bin_cols=0, segment_degrees=0,
-                 fft_lengths="timed"):
+                 fft_lengths="timed", maxboxes=8):
         self._h = None
         if len(theta) != len(phi):
             raise DimensionMismatch("θ and φ must have the same length")
@@ -185,6 +189,9 @@ class Plan:
         o.nufft_bin_rows = int(bin_rows)
         o.nufft_bin_cols = int(bin_cols)
         o.ring_segment_degrees = int(segment_degrees)
+        if maxboxes < 1:
+            raise ValueError("maxboxes must be >= 1")
+        o.maxboxes = int(maxboxes)
         if isinstance(fft_lengths, (tuple, list)) and len(fft_lengths) == 2:
             o.nufft_fft_lengths = 2
             o.nufft_nf1, o.nufft_nf2 = int(fft_lengths[0]), int(fft_lengths[1])
@@ -241,7 +248,24 @@ class Plan:
     @property
     def algorithm(self) -> str:
         """algorithm(plan) (src/Plan.jl:36)."""
-        return "DirectAlgorithm" if self.info["kind"] == "direct" else "StretchAlgorithm"
+        return {"direct": "DirectAlgorithm", "multibox": "MultiBoxAlgorithm"}.get(
+            self.info["kind"], "StretchAlgorithm")
+
+    def boxes(self) -> list:
+        """The plan's boxes (src/MultiBox.jl:75-79): for each, its leaf's info and the indices of
+        its points (ascending, 0-based). A single-leaf plan is its own one box."""
+        lib = _lib.load()
+        out = []
+        for i in range(int(lib.pfsht_plan_num_boxes(self._h))):
+            inf = _lib.PlanInfo()
+            _lib.check(lib.pfsht_plan_box(self._h, i, C.byref(inf), None), "plan_box")
+            idx = np.empty(inf.npts, dtype=np.int64)
+            _lib.check(lib.pfsht_plan_box(self._h, i, C.byref(inf), idx.ctypes.data), "plan_box")
+            d = {k: getattr(inf, k) for k, _ in _lib.PlanInfo._fields_}
+            d["kind"] = _lib.KINDS[inf.kind]
+            d["indices"] = idx
+            out.append(d)
+        return out
 
     def ring_work(self) -> int:
         """ring_work(plan) (src/Plan.jl:44): retained (l, m, ring) triples per apply."""
@@ -392,12 +416,13 @@ def dfs_fold(Ft, F, spin=0, stream=None):
 
 
 def plan_geometry(theta, phi, *, lmax, tol=1e-10, ntrans=1, method="auto",
-                  oversample_theta=1.0, oversample_phi=1.0, eps_apo_max=1.0) -> dict:
+                  oversample_theta=1.0, oversample_phi=1.0, eps_apo_max=1.0, maxboxes=8) -> dict:
     """Host-only: the geometry and sizes pfsht_plan_create would choose (no device used)."""
     th = np.ascontiguousarray(theta, dtype=np.float64)
     ph = np.ascontiguousarray(phi, dtype=np.float64)
     o = _lib.default_opts()
     o.method = _lib.METHODS[method]
+    o.maxboxes = int(maxboxes)
     o.oversample_theta = float(oversample_theta)
     o.oversample_phi = float(oversample_phi)
     o.eps_apo_max = float(eps_apo_max)
@@ -408,6 +433,106 @@ def plan_geometry(theta, phi, *, lmax, tol=1e-10, ntrans=1, method="auto",
     d = {k: getattr(inf, k) for k, _ in _lib.PlanInfo._fields_}
     d["kind"] = _lib.KINDS[inf.kind]
     return d
+
+
+# ---------------------------------------------------------------------------------------
+# planner (src/Box.jl, src/Cost.jl), host only
+# ---------------------------------------------------------------------------------------
+def _box_dict(b) -> dict:
+    return {"theta_lo": b.theta_lo, "theta_hi": b.theta_hi, "phi_start": b.phi_start,
+            "phi_extent": b.phi_extent, "touches_north": bool(b.touches_north),
+            "touches_south": bool(b.touches_south)}
+
+
+def _box_struct(d) -> "_lib.Box":
+    return _lib.Box(float(d["theta_lo"]), float(d["theta_hi"]), float(d["phi_start"]),
+                    float(d["phi_extent"]), int(bool(d["touches_north"])),
+                    int(bool(d["touches_south"])))
+
+
+def _points(theta, phi):
+    th = np.ascontiguousarray(theta, dtype=np.float64)
+    ph = np.ascontiguousarray(phi, dtype=np.float64)
+    if th.shape != ph.shape or th.ndim != 1:
+        raise DimensionMismatch("θ and φ must have the same length")
+    return th, ph
+
+
+def bounding_box(theta, phi) -> dict:
+    """bounding_box(θ, φ) (src/Box.jl:42-73): the exactly minimal colatitude x longitude box."""
+    th, ph = _points(theta, phi)
+    b = _lib.Box()
+    _lib.check(_lib.load().pfsht_bounding_box(th.ctypes.data, ph.ctypes.data, len(th), C.byref(b)),
+               "bounding_box")
+    return _box_dict(b)
+
+
+def box_fsky(box) -> float:
+    """box_fsky (src/Box.jl:98-104): fraction of the sphere the box covers."""
+    return (np.cos(box["theta_lo"]) - np.cos(box["theta_hi"])) * box["phi_extent"] / (4 * np.pi)
+
+
+def cost_direct(npts, lmax, ntrans=1) -> float:
+    """cost_direct (src/Cost.jl:107-108)."""
+    return float(_lib.load().pfsht_cost_direct(int(npts), int(lmax), int(ntrans)))
+
+
+def cost_stretch(box, npts, lmax, ntrans=1, tol=1e-10) -> float:
+    """cost_stretch (src/Cost.jl:117-142); inf where the stretched geometry is refused."""
+    b = _box_struct(box)
+    return float(_lib.load().pfsht_cost_stretch(C.byref(b), int(npts), int(lmax), int(ntrans),
+                                                float(tol)))
+
+
+def partition_boxes(theta, phi, *, lmax, ntrans=1, tol=1e-10, maxboxes=8):
+    """partition_boxes_costed(θ, φ, cost_stretch; maxboxes) (src/Box.jl:156-200): the groups
+    (ascending 0-based indices), their boxes and their predicted costs."""
+    th, ph = _points(theta, phi)
+    gop = np.empty(len(th), dtype=np.int32)
+    nb = C.c_int32()
+    boxes = (_lib.Box * int(maxboxes))()
+    costs = (C.c_double * int(maxboxes))()
+    _lib.check(_lib.load().pfsht_partition_boxes(th.ctypes.data, ph.ctypes.data, len(th), int(lmax),
+                                                 int(ntrans), float(tol), int(maxboxes),
+                                                 gop.ctypes.data, C.byref(nb), boxes, costs),
+               "partition_boxes")
+    n = nb.value
+    groups = [np.flatnonzero(gop == i) for i in range(n)]
+    return groups, [_box_dict(boxes[i]) for i in range(n)], [costs[i] for i in range(n)]
+
+
+def select_method(theta, phi, *, lmax, tol=1e-10, ntrans=1) -> str:
+    """select_method(θ, φ, lmax, tol, AutoAlgorithm(), ntrans) (src/Cost.jl:171-201):
+    "stretch", "direct" or "multibox"."""
+    th, ph = _points(theta, phi)
+    m = C.c_int32()
+    _lib.check(_lib.load().pfsht_select_method(th.ctypes.data, ph.ctypes.data, len(th), int(lmax),
+                                               int(ntrans), float(tol), C.byref(m)), "select_method")
+    return {v: k for k, v in _lib.METHODS.items()}[m.value]
+
+
+def cost_constants() -> dict:
+    """The planner's per-unit costs (src/Cost.jl:39-58) and whether they were installed."""
+    v = [C.c_double() for _ in range(4)]
+    cal = C.c_int32()
+    _lib.check(_lib.load().pfsht_get_cost_constants(*[C.byref(x) for x in v], C.byref(cal)))
+    return {"ring": v[0].value, "fft": v[1].value, "spread": v[2].value, "ft_conn": v[3].value,
+            "calibrated": bool(cal.value)}
+
+
+def set_cost_constants(*, ring=None, fft=None, spread=None, ft_conn=None) -> dict:
+    """set_cost_constants! (src/Cost.jl:60-71): install measured per-unit costs (process-wide);
+    the model then reports itself calibrated."""
+    c = cost_constants()
+    new = [c["ring"] if ring is None else ring, c["fft"] if fft is None else fft,
+           c["spread"] if spread is None else spread, c["ft_conn"] if ft_conn is None else ft_conn]
+    _lib.check(_lib.load().pfsht_set_cost_constants(*[float(x) for x in new]), "set_cost_constants")
+    return cost_constants()
+
+
+def cost_calibrated() -> bool:
+    """cost_calibrated() (src/Cost.jl:74)."""
+    return cost_constants()["calibrated"]
 
 
 class Batch:

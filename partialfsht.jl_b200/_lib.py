@@ -13,9 +13,9 @@ LIB_PATH = os.path.join(_HERE, "libpfsht_b200.so")
 HEADER_PATH = os.path.join(os.path.dirname(_HERE), "include", "pfsht_b200.h")
 
 OK, ERR_ARGUMENT, ERR_DIMENSION, ERR_REFUSED, ERR_CUDA, ERR_OOM, ERR_TIMEOUT, ERR_UNSUPPORTED = range(8)
-METHODS = {"auto": 0, "stretch": 1, "direct": 2}
+METHODS = {"auto": 0, "stretch": 1, "direct": 2, "multibox": 3}
 PRECISIONS = {"fp64": 0, "mixed": 1}
-KINDS = {0: "pole", 1: "interior", 2: "full", 3: "direct"}
+KINDS = {0: "pole", 1: "interior", 2: "full", 3: "direct", 4: "multibox"}
 
 
 class Opts(C.Structure):
@@ -24,7 +24,15 @@ class Opts(C.Structure):
                 ("nufft_bin_cols", C.c_int32), ("oversample_theta", C.c_double),
                 ("oversample_phi", C.c_double), ("eps_apo_max", C.c_double),
                 ("ring_segment_degrees", C.c_int32), ("nufft_fft_lengths", C.c_int32),
-                ("nufft_nf1", C.c_int32), ("nufft_nf2", C.c_int32), ("reserved", C.c_int32 * 4)]
+                ("nufft_nf1", C.c_int32), ("nufft_nf2", C.c_int32), ("maxboxes", C.c_int32),
+                ("reserved", C.c_int32 * 3)]
+
+
+class Box(C.Structure):
+    """pfsht_box: SphereBox (src/Box.jl:23-30)."""
+    _fields_ = [("theta_lo", C.c_double), ("theta_hi", C.c_double), ("phi_start", C.c_double),
+                ("phi_extent", C.c_double), ("touches_north", C.c_int32),
+                ("touches_south", C.c_int32)]
 
 
 class PlanInfo(C.Structure):
@@ -87,6 +95,17 @@ SIGNATURES = {
     "pfsht_server_stats": (C.c_int, [_vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
                                      C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "pfsht_server_destroy": (C.c_int, [_vp]),
+    "pfsht_bounding_box": (C.c_int, [_vp, _vp, C.c_int64, C.POINTER(Box)]),
+    "pfsht_cost_direct": (C.c_double, [C.c_int64, C.c_int32, C.c_int32]),
+    "pfsht_cost_stretch": (C.c_double, [C.POINTER(Box), C.c_int64, C.c_int32, C.c_int32, C.c_double]),
+    "pfsht_partition_boxes": (C.c_int, [_vp, _vp, C.c_int64, C.c_int32, C.c_int32, C.c_double,
+                                        C.c_int32, _vp, C.POINTER(C.c_int32), C.POINTER(Box), _dp]),
+    "pfsht_select_method": (C.c_int, [_vp, _vp, C.c_int64, C.c_int32, C.c_int32, C.c_double,
+                                      C.POINTER(C.c_int32)]),
+    "pfsht_set_cost_constants": (C.c_int, [C.c_double, C.c_double, C.c_double, C.c_double]),
+    "pfsht_get_cost_constants": (C.c_int, [_dp, _dp, _dp, _dp, C.POINTER(C.c_int32)]),
+    "pfsht_plan_num_boxes": (C.c_int32, [_vp]),
+    "pfsht_plan_box": (C.c_int, [_vp, C.c_int32, C.POINTER(PlanInfo), _vp]),
     "pfsht_profile_start": (C.c_int, [_vp, C.c_int32]),
     "pfsht_profile_stop": (C.c_int, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
     "pfsht_num_stages": (C.c_int32, []),

@@ -161,8 +161,12 @@ int batch_apply(pfsht_batch* b, bool fwd, const void* const* in, void* const* ou
 int batch_create(pfsht_plan* const* plans, int n, int nstreams, pfsht_batch** out) {
     if (!plans || !out || n < 1) return fail(PFSHT_ERR_ARGUMENT, "need at least one plan");
     if (nstreams < 0 || nstreams > 32) return fail(PFSHT_ERR_ARGUMENT, "nstreams must lie in 0..32");
-    for (int i = 0; i < n; ++i)
+    for (int i = 0; i < n; ++i) {
         if (!plans[i]) return fail(PFSHT_ERR_ARGUMENT, "NULL plan in the batch");
+        if (plans[i]->kind == kMultiBox)
+            return fail(PFSHT_ERR_UNSUPPORTED, "a multi-box plan cannot join a batch; batch its boxes' "
+                                               "geometries as plans of their own");
+    }
     const int dev = plans[0]->device;
     for (int i = 0; i < n; ++i) {
         if (plans[i]->device != dev) return fail(PFSHT_ERR_ARGUMENT, "all plans of a batch must share a device");

@@ -9,7 +9,7 @@
 
 namespace pf {
 
-enum Kind { kPole = 0, kInterior = 1, kFull = 2, kDirect = 3 };
+enum Kind { kPole = 0, kInterior = 1, kFull = 2, kDirect = 3, kMultiBox = 4 };
 
 struct Geom {
     int kind = kPole;

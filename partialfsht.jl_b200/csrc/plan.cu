@@ -24,6 +24,7 @@
 #include "../../include/pfsht_b200.h"
 #include "internal.cuh"
 #include "plan_internal.hpp"
+#include "planner.hpp"
 
 namespace pf {
 
@@ -140,6 +141,7 @@ int setup_nufft_grid(NufftGrid& g, NufftDev& d, int n1, int nmodes2, const std::
 
 int validate_common(int64_t npts, int lmax, int ntrans, double tol) {
     if (npts < 1) return fail(PFSHT_ERR_ARGUMENT, "need at least one point");
+    if (npts > INT32_MAX) return fail(PFSHT_ERR_ARGUMENT, "at most 2^31 - 1 points per plan");
     if (lmax < 0) return fail(PFSHT_ERR_ARGUMENT, "lmax must be nonnegative");
     if (ntrans < 1) return fail(PFSHT_ERR_ARGUMENT, "ntrans must be >= 1");
     if (!(tol > 0) || !(tol < 1)) return fail(PFSHT_ERR_ARGUMENT, "tol must lie in (0, 1)");
@@ -156,6 +158,15 @@ void fill_info(pfsht_plan* p) {
     in.precision = p->precision;
     in.npts = p->M;
     in.tol = p->tol;
+    if (p->kind == kMultiBox) {
+        for (const auto& c : p->boxes) {
+            in.ring_work += c->info.ring_work;
+            in.device_bytes += c->info.device_bytes;
+        }
+        in.device_bytes += (int64_t)(p->gidx.bytes + p->fg.bytes + p->acc.bytes + p->st_alm.bytes +
+                                     p->st_f.bytes);
+        return;
+    }
     if (p->kind == kDirect) {
         in.nrings = (int)p->M;
         in.mmax = p->L;
@@ -338,6 +349,108 @@ int build_direct(pfsht_plan* p, const double* h_theta, const double* h_phi, cuda
 }
 
 int plan_create(const double* theta, const double* phi, int64_t npts, int lmax, int ntrans,
+                double tol, int precision, const pfsht_opts* opts_in, pfsht_plan** out);
+
+// MultiBoxLeaf (src/MultiBox.jl:32-66): one stretched-leaf plan per group of the partition
+int build_multibox(pfsht_plan* p, const Partition& part, const double* th, const double* ph,
+                   int precision, const pfsht_opts& o) {
+    p->kind = kMultiBox;
+    const int nb = (int)part.groups.size();
+    if (nb < 1) return fail(PFSHT_ERR_ARGUMENT, "partition produced no boxes");
+    p->box_off.assign(nb + 1, 0);
+    std::vector<int32_t> idx;
+    idx.reserve(p->M);
+    for (int i = 0; i < nb; ++i) {
+        const std::vector<int32_t>& g = part.groups[i];
+        std::vector<double> tg(g.size()), pg(g.size());
+        for (size_t k = 0; k < g.size(); ++k) {
+            tg[k] = th[g[k]];
+            pg[k] = ph[g[k]];
+        }
+        pfsht_opts oc = o;
+        oc.method = PFSHT_METHOD_STRETCH;
+        oc.points_on_device = 0;
+        oc.device = p->device;
+        pfsht_plan* c = nullptr;
+        PF_TRY(plan_create(tg.data(), pg.data(), (int64_t)g.size(), p->L, p->B, p->tol, precision,
+                           &oc, &c));
+        p->boxes.emplace_back(c);
+        idx.insert(idx.end(), g.begin(), g.end());
+        p->box_off[i + 1] = p->box_off[i] + (int64_t)g.size();
+    }
+    p->precision = p->boxes[0]->precision;
+    PF_TRY(upload(p->gidx, idx, p->st_stream));
+    PF_TRY(p->fg.alloc(sizeof(double2) * (size_t)p->M * p->B));
+    if (nb > 1) PF_TRY(p->acc.alloc(sizeof(double2) * (size_t)(p->L + 1) * (2 * p->L + 1) * p->B));
+    return 0;
+}
+
+// f[idx[j], b] = fg[j, b] (the boxes' fields are a disjoint union, src/MultiBox.jl:83-94)
+__global__ void box_scatter_kernel(const double2* __restrict__ fg, const int* __restrict__ idx,
+                                   int64_t mb, int64_t M, int B, double2* __restrict__ f) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < mb * B;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t b = t / mb, j = t - b * mb;
+        f[idx[j] + M * b] = fg[t];
+    }
+}
+
+// fg[j, b] = f[idx[j], b]
+__global__ void box_gather_kernel(const double2* __restrict__ f, const int* __restrict__ idx,
+                                  int64_t mb, int64_t M, int B, double2* __restrict__ fg) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < mb * B;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t b = t / mb, j = t - b * mb;
+        fg[t] = f[idx[j] + M * b];
+    }
+}
+
+// a += c (the adjoint sums the boxes' coefficient arrays, src/MultiBox.jl:96-110)
+__global__ void coeff_add_kernel(double2* __restrict__ a, const double2* __restrict__ c, int64_t n) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const double2 x = a[t], y = c[t];
+        a[t] = make_double2(x.x + y.x, x.y + y.y);
+    }
+}
+
+// blocks of 256 threads for n elements (grid-stride loops beyond 148 x 16 blocks)
+unsigned grid_for(int64_t n) { return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 16)); }
+
+int apply_forward(pfsht_plan* p, const double2* alm, double2* f, cudaStream_t s);
+int apply_adjoint(pfsht_plan* p, const double2* f, double2* alm, cudaStream_t s);
+
+int multibox_forward(pfsht_plan* p, const double2* alm, double2* f, cudaStream_t s) {
+    for (size_t i = 0; i < p->boxes.size(); ++i) {
+        const int64_t mb = p->box_off[i + 1] - p->box_off[i];
+        double2* fgi = p->fg.as<double2>() + p->B * p->box_off[i];
+        PF_TRY(apply_forward(p->boxes[i].get(), alm, fgi, s));
+        box_scatter_kernel<<<grid_for(mb * p->B), 256, 0, s>>>(
+            fgi, p->gidx.as<int>() + p->box_off[i], mb, p->M, p->B, f);
+        PF_TRY(check_launch("box_scatter_kernel"));
+    }
+    return 0;
+}
+
+int multibox_adjoint(pfsht_plan* p, const double2* f, double2* alm, cudaStream_t s) {
+    const int64_t nc = (int64_t)(p->L + 1) * (2 * p->L + 1) * p->B;
+    for (size_t i = 0; i < p->boxes.size(); ++i) {
+        const int64_t mb = p->box_off[i + 1] - p->box_off[i];
+        double2* fgi = p->fg.as<double2>() + p->B * p->box_off[i];
+        box_gather_kernel<<<grid_for(mb * p->B), 256, 0, s>>>(
+            f, p->gidx.as<int>() + p->box_off[i], mb, p->M, p->B, fgi);
+        PF_TRY(check_launch("box_gather_kernel"));
+        // each box's adjoint overwrites its output: the first writes alm, the others are added
+        PF_TRY(apply_adjoint(p->boxes[i].get(), fgi, i == 0 ? alm : p->acc.as<double2>(), s));
+        if (i > 0) {
+            coeff_add_kernel<<<grid_for(nc), 256, 0, s>>>(alm, p->acc.as<double2>(), nc);
+            PF_TRY(check_launch("coeff_add_kernel"));
+        }
+    }
+    return 0;
+}
+
+int plan_create(const double* theta, const double* phi, int64_t npts, int lmax, int ntrans,
                 double tol, int precision, const pfsht_opts* opts_in, pfsht_plan** out) {
     if (!out) return fail(PFSHT_ERR_ARGUMENT, "out is NULL");
     *out = nullptr;
@@ -348,7 +461,7 @@ int plan_create(const double* theta, const double* phi, int64_t npts, int lmax, 
     pfsht_opts o;
     pfsht_opts_default(&o);
     if (opts_in) o = *opts_in;
-    if (o.method < 0 || o.method > 2) return fail(PFSHT_ERR_ARGUMENT, "unknown method");
+    if (o.method < 0 || o.method > 3) return fail(PFSHT_ERR_ARGUMENT, "unknown method");
     if (!(o.oversample_theta >= 1) || !(o.oversample_phi >= 1))
         return fail(PFSHT_ERR_ARGUMENT, "oversampling factors must be >= 1");
     if (!(o.eps_apo_max > 0)) return fail(PFSHT_ERR_ARGUMENT, "eps_apo_max must be positive");
@@ -404,7 +517,41 @@ int plan_create(const double* theta, const double* phi, int64_t npts, int lmax, 
     lo = std::fmax(lo, 0.0);
     hi = std::fmin(hi, M_PI);
 
-    bool direct = o.method == PFSHT_METHOD_DIRECT;
+    // the planner reads the points on the host (src/Cost.jl:171-201)
+    const double* hth = theta;
+    const double* hph = phi;
+    auto host_points = [&]() -> int {
+        if (!o.points_on_device) return 0;
+        if (h_theta.empty()) {
+            h_theta.resize(npts);
+            h_phi.resize(npts);
+            PF_CUDA(cudaMemcpyAsync(h_theta.data(), theta, sizeof(double) * npts, cudaMemcpyDeviceToHost, s));
+            PF_CUDA(cudaMemcpyAsync(h_phi.data(), phi, sizeof(double) * npts, cudaMemcpyDeviceToHost, s));
+            PF_CUDA(cudaStreamSynchronize(s));
+        }
+        hth = h_theta.data();
+        hph = h_phi.data();
+        return 0;
+    };
+    int method = o.method;
+    Partition part;
+    bool have_part = false;
+    if (method == PFSHT_METHOD_AUTO) {
+        PF_TRY(host_points());
+        method = select_method(hth, hph, npts, lmax, ntrans, tol, &part);
+        have_part = true;
+    }
+    if (method == PFSHT_METHOD_MULTIBOX) {
+        PF_TRY(host_points());
+        const int mb = o.maxboxes > 0 ? o.maxboxes : 8;
+        if (!have_part || mb != 8) partition_boxes_costed(hth, hph, npts, lmax, ntrans, tol, mb, part);
+        PF_TRY(build_multibox(p.get(), part, hth, hph, precision, o));
+        PF_CUDA(cudaStreamSynchronize(s));
+        fill_info(p.get());
+        *out = p.release();
+        return 0;
+    }
+    bool direct = method == PFSHT_METHOD_DIRECT;
     if (!direct) {
         std::string err;
         int r = build_leaf(lo, hi, lmax, ntrans, tol, o.eps_apo_max, o.oversample_theta,
@@ -416,16 +563,8 @@ int plan_create(const double* theta, const double* phi, int64_t npts, int lmax, 
         }
     }
     if (direct) {
-        if (o.points_on_device) {
-            h_theta.resize(npts);
-            h_phi.resize(npts);
-            PF_CUDA(cudaMemcpyAsync(h_theta.data(), theta, sizeof(double) * npts, cudaMemcpyDeviceToHost, s));
-            PF_CUDA(cudaMemcpyAsync(h_phi.data(), phi, sizeof(double) * npts, cudaMemcpyDeviceToHost, s));
-            PF_CUDA(cudaStreamSynchronize(s));
-            PF_TRY(build_direct(p.get(), h_theta.data(), h_phi.data(), s));
-        } else {
-            PF_TRY(build_direct(p.get(), theta, phi, s));
-        }
+        PF_TRY(host_points());
+        PF_TRY(build_direct(p.get(), hth, hph, s));
     } else {
         PF_TRY(build_stretch(p.get(), dth, dph, o, s));
     }
@@ -436,6 +575,7 @@ int plan_create(const double* theta, const double* phi, int64_t npts, int lmax, 
 }
 
 int apply_forward(pfsht_plan* p, const double2* alm, double2* f, cudaStream_t s) {
+    if (p->kind == kMultiBox) return multibox_forward(p, alm, f, s);
     clock_begin(&p->clk, s);
     PF_TRY(ring_forward(p->rt, p->ro_cols, p->fwd_items.view, alm, p->H.as<double2>(), p->B, s));
     if (p->kind != kDirect) clock_mark(&p->clk, kStRingFwd, s);
@@ -443,6 +583,7 @@ int apply_forward(pfsht_plan* p, const double2* alm, double2* f, cudaStream_t s)
 }
 
 int apply_adjoint(pfsht_plan* p, const double2* f, double2* alm, cudaStream_t s) {
+    if (p->kind == kMultiBox) return multibox_adjoint(p, f, alm, s);
     clock_begin(&p->clk, s);
     PF_TRY(plan_adjoint_before_ring(p, f, s));
     PF_TRY(ring_adjoint(p->rt, p->ro_cols, p->adj_items.view, p->H.as<double2>(), alm, p->B, s));
@@ -655,6 +796,8 @@ pfsht_status pfsht_adjoint_host(pfsht_plan* p, const void* f, void* alm) {
 pfsht_status pfsht_ring_forward(pfsht_plan* p, const void* alm, void* G, void* stream) {
     if (!p || !alm || !G) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "NULL argument");
     if (p->kind == kDirect) return (pfsht_status)fail(PFSHT_ERR_UNSUPPORTED, "direct plan has no ring set");
+    if (p->kind == kMultiBox)
+        return (pfsht_status)fail(PFSHT_ERR_UNSUPPORTED, "a multi-box plan has one ring set per box");
     DeviceGuard dg(p->device);
     cudaStream_t s = (cudaStream_t)stream;
     RingTables t = p->rt;
@@ -677,6 +820,8 @@ pfsht_status pfsht_ring_forward(pfsht_plan* p, const void* alm, void* G, void* s
 pfsht_status pfsht_ring_adjoint(pfsht_plan* p, const void* G, void* alm, void* stream) {
     if (!p || !alm || !G) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "NULL argument");
     if (p->kind == kDirect) return (pfsht_status)fail(PFSHT_ERR_UNSUPPORTED, "direct plan has no ring set");
+    if (p->kind == kMultiBox)
+        return (pfsht_status)fail(PFSHT_ERR_UNSUPPORTED, "a multi-box plan has one ring set per box");
     DeviceGuard dg(p->device);
     cudaStream_t s = (cudaStream_t)stream;
     RingTables t = p->rt;
@@ -702,6 +847,120 @@ pfsht_status pfsht_plan_get_info(const pfsht_plan* p, pfsht_plan_info* info) {
 
 int64_t pfsht_workspace_bytes(const pfsht_plan* p) { return p ? p->info.device_bytes : -1; }
 
+int32_t pfsht_plan_num_boxes(const pfsht_plan* p) {
+    if (!p) return -1;
+    return p->kind == kMultiBox ? (int32_t)p->boxes.size() : 1;
+}
+
+pfsht_status pfsht_plan_box(const pfsht_plan* p, int32_t box, pfsht_plan_info* info, int64_t* indices) {
+    if (!p) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "NULL plan");
+    const int32_t nb = pfsht_plan_num_boxes(p);
+    if (box < 0 || box >= nb) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "box index out of range");
+    if (p->kind != kMultiBox) {
+        if (info) *info = p->info;
+        if (indices)
+            for (int64_t i = 0; i < p->M; ++i) indices[i] = i;
+        return PFSHT_OK;
+    }
+    const pfsht_plan* c = p->boxes[box].get();
+    if (info) *info = c->info;
+    if (indices) {
+        const int64_t mb = p->box_off[box + 1] - p->box_off[box];
+        std::vector<int32_t> h(mb);
+        DeviceGuard dg(p->device);
+        if (mb > 0 && cudaMemcpy(h.data(), p->gidx.as<int32_t>() + p->box_off[box], sizeof(int32_t) * mb,
+                                 cudaMemcpyDeviceToHost) != cudaSuccess)
+            return (pfsht_status)fail(PFSHT_ERR_CUDA, "copying box indices");
+        for (int64_t i = 0; i < mb; ++i) indices[i] = h[i];
+    }
+    return PFSHT_OK;
+}
+
+static pfsht_box to_abi(const SphereBox& b) {
+    pfsht_box o;
+    o.theta_lo = b.lo;
+    o.theta_hi = b.hi;
+    o.phi_start = b.phistart;
+    o.phi_extent = b.phiext;
+    o.touches_north = b.touches_north ? 1 : 0;
+    o.touches_south = b.touches_south ? 1 : 0;
+    return o;
+}
+
+static SphereBox from_abi(const pfsht_box& o) {
+    SphereBox b;
+    b.lo = o.theta_lo;
+    b.hi = o.theta_hi;
+    b.phistart = o.phi_start;
+    b.phiext = o.phi_extent;
+    b.touches_north = o.touches_north != 0;
+    b.touches_south = o.touches_south != 0;
+    return b;
+}
+
+pfsht_status pfsht_bounding_box(const double* theta, const double* phi, int64_t npts, pfsht_box* box) {
+    if (!theta || !phi || !box) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "NULL argument");
+    if (npts < 1) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "need at least one point");
+    *box = to_abi(bounding_box(theta, phi, npts));
+    return PFSHT_OK;
+}
+
+double pfsht_cost_direct(int64_t npts, int32_t lmax, int32_t ntrans) {
+    return cost_direct(npts, lmax, ntrans);
+}
+
+double pfsht_cost_stretch(const pfsht_box* box, int64_t npts, int32_t lmax, int32_t ntrans, double tol) {
+    if (!box) return NAN;
+    return cost_stretch(from_abi(*box), npts, lmax, ntrans, tol);
+}
+
+pfsht_status pfsht_partition_boxes(const double* theta, const double* phi, int64_t npts,
+                                   int32_t lmax, int32_t ntrans, double tol, int32_t maxboxes,
+                                   int32_t* group_of_point, int32_t* nboxes, pfsht_box* boxes,
+                                   double* costs) {
+    if (!theta || !phi || !nboxes) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "NULL argument");
+    const int v = validate_common(npts, lmax, ntrans, tol);
+    if (v) return (pfsht_status)v;
+    if (maxboxes < 1) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "maxboxes must be >= 1");
+    Partition part;
+    partition_boxes_costed(theta, phi, npts, lmax, ntrans, tol, maxboxes, part);
+    *nboxes = (int32_t)part.groups.size();
+    for (size_t i = 0; i < part.groups.size(); ++i) {
+        if (group_of_point)
+            for (int32_t k : part.groups[i]) group_of_point[k] = (int32_t)i;
+        if (boxes) boxes[i] = to_abi(part.boxes[i]);
+        if (costs) costs[i] = part.costs[i];
+    }
+    return PFSHT_OK;
+}
+
+pfsht_status pfsht_select_method(const double* theta, const double* phi, int64_t npts, int32_t lmax,
+                                 int32_t ntrans, double tol, int32_t* method) {
+    if (!theta || !phi || !method) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "NULL argument");
+    const int v = validate_common(npts, lmax, ntrans, tol);
+    if (v) return (pfsht_status)v;
+    *method = select_method(theta, phi, npts, lmax, ntrans, tol, nullptr);
+    return PFSHT_OK;
+}
+
+pfsht_status pfsht_set_cost_constants(double ring, double fft, double spread, double ft_conn) {
+    if (!(ring > 0) || !(fft > 0) || !(spread > 0) || !(ft_conn > 0))
+        return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "cost constants must be positive");
+    set_cost_constants(ring, fft, spread, ft_conn);
+    return PFSHT_OK;
+}
+
+pfsht_status pfsht_get_cost_constants(double* ring, double* fft, double* spread, double* ft_conn,
+                                      int32_t* calibrated) {
+    const CostConstants c = cost_constants();
+    if (ring) *ring = c.ring;
+    if (fft) *fft = c.fft;
+    if (spread) *spread = c.spread;
+    if (ft_conn) *ft_conn = c.ft_conn;
+    if (calibrated) *calibrated = c.calibrated ? 1 : 0;
+    return PFSHT_OK;
+}
+
 pfsht_status pfsht_plan_geometry(const double* theta, const double* phi, int64_t npts, int32_t lmax,
                                  int32_t ntrans, double tol, const pfsht_opts* opts_in,
                                  pfsht_plan_info* info) {
@@ -723,7 +982,29 @@ pfsht_status pfsht_plan_geometry(const double* theta, const double* phi, int64_t
     info->ntrans = ntrans;
     info->npts = npts;
     info->tol = tol;
-    if (o.method == PFSHT_METHOD_DIRECT) {
+    int method = o.method;
+    Partition part;
+    bool have_part = false;
+    if (method == PFSHT_METHOD_AUTO) {
+        method = select_method(theta, phi, npts, lmax, ntrans, tol, &part);
+        have_part = true;
+    }
+    if (method == PFSHT_METHOD_MULTIBOX) {
+        const int mb = o.maxboxes > 0 ? o.maxboxes : 8;
+        if (!have_part || mb != 8) partition_boxes_costed(theta, phi, npts, lmax, ntrans, tol, mb, part);
+        info->kind = kMultiBox;
+        for (const SphereBox& b : part.boxes) {
+            Leaf lb;
+            std::string eb;
+            const int rb = build_leaf(b.lo, b.hi, lmax, ntrans, tol, o.eps_apo_max, o.oversample_theta,
+                                      o.oversample_phi, &lb, &eb);
+            if (rb == 2) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, eb);
+            if (rb == 1) return (pfsht_status)fail(PFSHT_ERR_REFUSED, eb);
+            info->ring_work += lb.ring_work;
+        }
+        return PFSHT_OK;
+    }
+    if (method == PFSHT_METHOD_DIRECT) {
         info->kind = kDirect;
         info->mmax = lmax;
         info->nrings = (int)npts;
@@ -863,6 +1144,10 @@ const char* pfsht_stage_name(int32_t stage) {
 
 pfsht_status pfsht_profile_start(pfsht_plan* p, int32_t max_marks) {
     if (!p || max_marks < 2) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "bad profile arguments");
+    for (auto& c : p->boxes) {
+        const pfsht_status r = pfsht_profile_start(c.get(), max_marks);
+        if (r) return r;
+    }
     DeviceGuard dg(p->device);
     StageClock& c = p->clk;
     while ((int)c.ev.size() < max_marks) {
@@ -880,6 +1165,24 @@ pfsht_status pfsht_profile_start(pfsht_plan* p, int32_t max_marks) {
 
 pfsht_status pfsht_profile_stop(pfsht_plan* p, double* stage_ms, int32_t* stage_count) {
     if (!p || !stage_ms || !stage_count) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "NULL argument");
+    if (p->kind == kMultiBox) {
+        // the boxes' stages, summed
+        std::vector<double> ms(kNumStages);
+        std::vector<int32_t> cnt(kNumStages);
+        for (int i = 0; i < kNumStages; ++i) {
+            stage_ms[i] = 0.0;
+            stage_count[i] = 0;
+        }
+        for (auto& c : p->boxes) {
+            const pfsht_status r = pfsht_profile_stop(c.get(), ms.data(), cnt.data());
+            if (r) return r;
+            for (int i = 0; i < kNumStages; ++i) {
+                stage_ms[i] += ms[i];
+                stage_count[i] += cnt[i];
+            }
+        }
+        return PFSHT_OK;
+    }
     DeviceGuard dg(p->device);
     StageClock& c = p->clk;
     for (int i = 0; i < kNumStages; ++i) {

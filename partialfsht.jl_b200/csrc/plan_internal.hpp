@@ -3,6 +3,9 @@
 #pragma once
 #include <cufft.h>
 
+#include <memory>
+#include <vector>
+
 #include "../../include/pfsht_b200.h"
 #include "internal.cuh"
 
@@ -38,6 +41,12 @@ struct pfsht_plan {
     // host-buffer staging
     DevBuf st_alm, st_f;
     cudaStream_t st_stream = nullptr;
+    // MultiBox (src/MultiBox.jl): one stretched-leaf plan per box; gidx holds the boxes' point
+    // indices one box after the other (box i at [box_off[i], box_off[i + 1])), fg the boxes'
+    // fields in the same order (box i at B box_off[i]), acc one coefficient array for the sum
+    std::vector<std::unique_ptr<pfsht_plan>> boxes;
+    std::vector<int64_t> box_off;
+    DevBuf gidx, fg, acc;
     pfsht_plan_info info{};
     StageClock clk;
     ~pfsht_plan() {

@@ -117,5 +117,5 @@ def test_baseline_config_sizes(pf):
     expect = {256: (80, 160, 360, 178), 1024: (216, 432, 1080, 513), 2048: (360, 720, 1920, 921)}
     for L, (nh, nth, nph, mmax) in expect.items():
         th = np.array([1e-3, np.deg2rad(20.0)])
-        g = pf.plan_geometry(th, np.zeros(2), lmax=L, tol=1e-8)
+        g = pf.plan_geometry(th, np.zeros(2), lmax=L, tol=1e-8, method="stretch")
         assert (g["nth_half"], g["nth"], g["nph"], g["mmax"]) == (nh, nth, nph, mmax)
