@@ -160,6 +160,18 @@ pfsht_status pfsht_partition_boxes(const double* theta, const double* phi, int64
 /* select_method (src/Cost.jl:171-201) for AUTO: *method = STRETCH, DIRECT or MULTIBOX. */
 pfsht_status pfsht_select_method(const double* theta, const double* phi, int64_t npts,
                                  int32_t lmax, int32_t ntrans, double tol, int32_t* method);
+/* The same three on device arrays of points (the O(n) scans run on the device, the cost model and
+ * the search loop on the host; results equal the host versions'). Plans of 2^15 points or more
+ * are planned this way. */
+pfsht_status pfsht_bounding_box_device(const double* theta, const double* phi, int64_t npts,
+                                       pfsht_box* box, void* stream);
+pfsht_status pfsht_partition_boxes_device(const double* theta, const double* phi, int64_t npts,
+                                          int32_t lmax, int32_t ntrans, double tol, int32_t maxboxes,
+                                          int32_t* group_of_point, int32_t* nboxes, pfsht_box* boxes,
+                                          double* costs, void* stream);
+pfsht_status pfsht_select_method_device(const double* theta, const double* phi, int64_t npts,
+                                        int32_t lmax, int32_t ntrans, double tol, int32_t* method,
+                                        void* stream);
 /* set_cost_constants! / cost_calibrated (src/Cost.jl:60-74): process-wide per-unit costs. */
 pfsht_status pfsht_set_cost_constants(double ring, double fft, double spread, double ft_conn);
 pfsht_status pfsht_get_cost_constants(double* ring, double* fft, double* spread, double* ft_conn,

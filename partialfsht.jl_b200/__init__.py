@@ -458,10 +458,29 @@ def _points(theta, phi):
     return th, ph
 
 
+def _device_points(theta, phi):
+    """CUDA float64 tensors (the planner's device scans), or None for host arrays."""
+    if not (_is_torch(theta) and theta.is_cuda):
+        return None
+    torch = _torch()
+    th = theta.to(torch.float64).contiguous()
+    ph = phi.to(dtype=torch.float64, device=th.device).contiguous()
+    if th.shape != ph.shape or th.dim() != 1:
+        raise DimensionMismatch("θ and φ must have the same length")
+    torch.cuda.current_stream(th.device).synchronize()
+    return th, ph
+
+
 def bounding_box(theta, phi) -> dict:
-    """bounding_box(θ, φ) (src/Box.jl:42-73): the exactly minimal colatitude x longitude box."""
-    th, ph = _points(theta, phi)
+    """bounding_box(θ, φ) (src/Box.jl:42-73): the exactly minimal colatitude x longitude box.
+    CUDA tensors are scanned on their device."""
     b = _lib.Box()
+    dp = _device_points(theta, phi)
+    if dp is not None:
+        _lib.check(_lib.load().pfsht_bounding_box_device(dp[0].data_ptr(), dp[1].data_ptr(),
+                                                         len(dp[0]), C.byref(b), None), "bounding_box")
+        return _box_dict(b)
+    th, ph = _points(theta, phi)
     _lib.check(_lib.load().pfsht_bounding_box(th.ctypes.data, ph.ctypes.data, len(th), C.byref(b)),
                "bounding_box")
     return _box_dict(b)
@@ -486,16 +505,24 @@ def cost_stretch(box, npts, lmax, ntrans=1, tol=1e-10) -> float:
 
 def partition_boxes(theta, phi, *, lmax, ntrans=1, tol=1e-10, maxboxes=8):
     """partition_boxes_costed(θ, φ, cost_stretch; maxboxes) (src/Box.jl:156-200): the groups
-    (ascending 0-based indices), their boxes and their predicted costs."""
-    th, ph = _points(theta, phi)
-    gop = np.empty(len(th), dtype=np.int32)
+    (ascending 0-based indices), their boxes and their predicted costs. CUDA tensors are scanned
+    on their device (the same result)."""
     nb = C.c_int32()
     boxes = (_lib.Box * int(maxboxes))()
     costs = (C.c_double * int(maxboxes))()
-    _lib.check(_lib.load().pfsht_partition_boxes(th.ctypes.data, ph.ctypes.data, len(th), int(lmax),
-                                                 int(ntrans), float(tol), int(maxboxes),
-                                                 gop.ctypes.data, C.byref(nb), boxes, costs),
-               "partition_boxes")
+    dp = _device_points(theta, phi)
+    if dp is not None:
+        gop = np.empty(len(dp[0]), dtype=np.int32)
+        _lib.check(_lib.load().pfsht_partition_boxes_device(
+            dp[0].data_ptr(), dp[1].data_ptr(), len(dp[0]), int(lmax), int(ntrans), float(tol),
+            int(maxboxes), gop.ctypes.data, C.byref(nb), boxes, costs, None), "partition_boxes")
+    else:
+        th, ph = _points(theta, phi)
+        gop = np.empty(len(th), dtype=np.int32)
+        _lib.check(_lib.load().pfsht_partition_boxes(th.ctypes.data, ph.ctypes.data, len(th),
+                                                     int(lmax), int(ntrans), float(tol),
+                                                     int(maxboxes), gop.ctypes.data, C.byref(nb),
+                                                     boxes, costs), "partition_boxes")
     n = nb.value
     groups = [np.flatnonzero(gop == i) for i in range(n)]
     return groups, [_box_dict(boxes[i]) for i in range(n)], [costs[i] for i in range(n)]
@@ -503,9 +530,16 @@ def partition_boxes(theta, phi, *, lmax, ntrans=1, tol=1e-10, maxboxes=8):
 
 def select_method(theta, phi, *, lmax, tol=1e-10, ntrans=1) -> str:
     """select_method(θ, φ, lmax, tol, AutoAlgorithm(), ntrans) (src/Cost.jl:171-201):
-    "stretch", "direct" or "multibox"."""
-    th, ph = _points(theta, phi)
+    "stretch", "direct" or "multibox" (CUDA tensors: scans on their device)."""
     m = C.c_int32()
+    dp = _device_points(theta, phi)
+    if dp is not None:
+        _lib.check(_lib.load().pfsht_select_method_device(dp[0].data_ptr(), dp[1].data_ptr(),
+                                                          len(dp[0]), int(lmax), int(ntrans),
+                                                          float(tol), C.byref(m), None),
+                   "select_method")
+        return {v: k for k, v in _lib.METHODS.items()}[m.value]
+    th, ph = _points(theta, phi)
     _lib.check(_lib.load().pfsht_select_method(th.ctypes.data, ph.ctypes.data, len(th), int(lmax),
                                                int(ntrans), float(tol), C.byref(m)), "select_method")
     return {v: k for k, v in _lib.METHODS.items()}[m.value]

@@ -102,6 +102,12 @@ SIGNATURES = {
                                         C.c_int32, _vp, C.POINTER(C.c_int32), C.POINTER(Box), _dp]),
     "pfsht_select_method": (C.c_int, [_vp, _vp, C.c_int64, C.c_int32, C.c_int32, C.c_double,
                                       C.POINTER(C.c_int32)]),
+    "pfsht_bounding_box_device": (C.c_int, [_vp, _vp, C.c_int64, C.POINTER(Box), _vp]),
+    "pfsht_partition_boxes_device": (C.c_int, [_vp, _vp, C.c_int64, C.c_int32, C.c_int32, C.c_double,
+                                               C.c_int32, _vp, C.POINTER(C.c_int32), C.POINTER(Box),
+                                               _dp, _vp]),
+    "pfsht_select_method_device": (C.c_int, [_vp, _vp, C.c_int64, C.c_int32, C.c_int32, C.c_double,
+                                             C.POINTER(C.c_int32), _vp]),
     "pfsht_set_cost_constants": (C.c_int, [C.c_double, C.c_double, C.c_double, C.c_double]),
     "pfsht_get_cost_constants": (C.c_int, [_dp, _dp, _dp, _dp, C.POINTER(C.c_int32)]),
     "pfsht_plan_num_boxes": (C.c_int32, [_vp]),

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "geometry.hpp"
+#include "planner.hpp"
 
 namespace pf {
 
@@ -280,6 +281,22 @@ int direct_phase_spread(const double2* f, const double* phi, int64_t M, int lmax
 // DFS (src/DFS.jl:13-56)
 int dfs_double(const double2* F, double2* Ft, int Nth, int Nph, int B, int spin, cudaStream_t s);
 int dfs_fold(double2* F, const double2* Ft, int Nth, int Nph, int B, int spin, cudaStream_t s);
+
+// the planner's point scans on the device (planner_dev.cu); theta / phi are device arrays and
+// the groups come back as device index lists, equal to the host planner's
+struct DevPartition {
+    std::vector<std::shared_ptr<DevBuf>> idx;
+    std::vector<int64_t> n;
+    std::vector<SphereBox> boxes;
+    std::vector<double> costs;
+};
+int bounding_box_device(const double* theta, const double* phi, int64_t n, cudaStream_t s,
+                        SphereBox* out);
+int partition_boxes_device(const double* theta, const double* phi, int64_t n, int lmax, int ntrans,
+                           double tol, int maxboxes, cudaStream_t s, DevPartition& out);
+// *method: 1 stretch, 2 direct, 3 multi-box (select_method of src/Cost.jl:171-201)
+int select_method_device(const double* theta, const double* phi, int64_t n, int lmax, int ntrans,
+                         double tol, cudaStream_t s, int* method, DevPartition* part);
 
 // launch-error check after a kernel (also counts the launch)
 int check_launch(const char* what);

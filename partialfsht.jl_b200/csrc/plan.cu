@@ -351,6 +351,9 @@ int build_direct(pfsht_plan* p, const double* h_theta, const double* h_phi, cuda
 int plan_create(const double* theta, const double* phi, int64_t npts, int lmax, int ntrans,
                 double tol, int precision, const pfsht_opts* opts_in, pfsht_plan** out);
 
+// point sets from this size on are planned by the device scans (planner_dev.cu)
+constexpr int64_t kDevicePlannerMin = 1 << 15;
+
 // MultiBoxLeaf (src/MultiBox.jl:32-66): one stretched-leaf plan per group of the partition
 int build_multibox(pfsht_plan* p, const Partition& part, const double* th, const double* ph,
                    int precision, const pfsht_opts& o) {
@@ -382,6 +385,53 @@ int build_multibox(pfsht_plan* p, const Partition& part, const double* th, const
     PF_TRY(upload(p->gidx, idx, p->st_stream));
     PF_TRY(p->fg.alloc(sizeof(double2) * (size_t)p->M * p->B));
     if (nb > 1) PF_TRY(p->acc.alloc(sizeof(double2) * (size_t)(p->L + 1) * (2 * p->L + 1) * p->B));
+    return 0;
+}
+
+// the same from a partition computed on the device: each box's points are gathered on the device
+// and its plan is built from them there
+__global__ void gather_points_by_index(const double* __restrict__ th, const double* __restrict__ ph,
+                                       const int* __restrict__ idx, int64_t n, double* __restrict__ tg,
+                                       double* __restrict__ pg) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        tg[t] = th[idx[t]];
+        pg[t] = ph[idx[t]];
+    }
+}
+
+int build_multibox_device(pfsht_plan* p, const DevPartition& part, const double* th, const double* ph,
+                          int precision, const pfsht_opts& o) {
+    p->kind = kMultiBox;
+    const int nb = (int)part.idx.size();
+    if (nb < 1) return fail(PFSHT_ERR_ARGUMENT, "partition produced no boxes");
+    cudaStream_t s = p->st_stream;
+    p->box_off.assign(nb + 1, 0);
+    for (int i = 0; i < nb; ++i) p->box_off[i + 1] = p->box_off[i] + part.n[i];
+    PF_TRY(p->gidx.alloc(sizeof(int32_t) * (size_t)p->M));
+    for (int i = 0; i < nb; ++i) {
+        const int64_t n = part.n[i];
+        PF_CUDA(cudaMemcpyAsync(p->gidx.as<int32_t>() + p->box_off[i], part.idx[i]->p, sizeof(int32_t) * n,
+                                cudaMemcpyDeviceToDevice, s));
+        DevBuf tg, pg;
+        PF_TRY(tg.alloc(sizeof(double) * n));
+        PF_TRY(pg.alloc(sizeof(double) * n));
+        gather_points_by_index<<<(unsigned)std::min<int64_t>((n + 255) / 256, 148 * 16), 256, 0, s>>>(
+            th, ph, part.idx[i]->as<int>(), n, tg.as<double>(), pg.as<double>());
+        PF_TRY(check_launch("gather_points_by_index"));
+        PF_CUDA(cudaStreamSynchronize(s));
+        pfsht_opts oc = o;
+        oc.method = PFSHT_METHOD_STRETCH;
+        oc.points_on_device = 1;
+        oc.device = p->device;
+        pfsht_plan* c = nullptr;
+        PF_TRY(plan_create(tg.as<double>(), pg.as<double>(), n, p->L, p->B, p->tol, precision, &oc, &c));
+        p->boxes.emplace_back(c);
+    }
+    p->precision = p->boxes[0]->precision;
+    PF_TRY(p->fg.alloc(sizeof(double2) * (size_t)p->M * p->B));
+    if (nb > 1) PF_TRY(p->acc.alloc(sizeof(double2) * (size_t)(p->L + 1) * (2 * p->L + 1) * p->B));
+    PF_CUDA(cudaStreamSynchronize(s));
     return 0;
 }
 
@@ -534,6 +584,25 @@ int plan_create(const double* theta, const double* phi, int64_t npts, int lmax, 
         return 0;
     };
     int method = o.method;
+    const int mb = o.maxboxes > 0 ? o.maxboxes : 8;
+    if (npts >= kDevicePlannerMin) {
+        // large point sets: the planner's scans run on the device copies of the points
+        DevPartition dpart;
+        bool have_dpart = false;
+        if (method == PFSHT_METHOD_AUTO) {
+            PF_TRY(select_method_device(dth, dph, npts, lmax, ntrans, tol, s, &method, &dpart));
+            have_dpart = true;
+        }
+        if (method == PFSHT_METHOD_MULTIBOX) {
+            if (!have_dpart || mb != 8)
+                PF_TRY(partition_boxes_device(dth, dph, npts, lmax, ntrans, tol, mb, s, dpart));
+            PF_TRY(build_multibox_device(p.get(), dpart, dth, dph, precision, o));
+            PF_CUDA(cudaStreamSynchronize(s));
+            fill_info(p.get());
+            *out = p.release();
+            return 0;
+        }
+    }
     Partition part;
     bool have_part = false;
     if (method == PFSHT_METHOD_AUTO) {
@@ -543,7 +612,6 @@ int plan_create(const double* theta, const double* phi, int64_t npts, int lmax, 
     }
     if (method == PFSHT_METHOD_MULTIBOX) {
         PF_TRY(host_points());
-        const int mb = o.maxboxes > 0 ? o.maxboxes : 8;
         if (!have_part || mb != 8) partition_boxes_costed(hth, hph, npts, lmax, ntrans, tol, mb, part);
         PF_TRY(build_multibox(p.get(), part, hth, hph, precision, o));
         PF_CUDA(cudaStreamSynchronize(s));
@@ -940,6 +1008,57 @@ pfsht_status pfsht_select_method(const double* theta, const double* phi, int64_t
     const int v = validate_common(npts, lmax, ntrans, tol);
     if (v) return (pfsht_status)v;
     *method = select_method(theta, phi, npts, lmax, ntrans, tol, nullptr);
+    return PFSHT_OK;
+}
+
+pfsht_status pfsht_partition_boxes_device(const double* theta, const double* phi, int64_t npts,
+                                          int32_t lmax, int32_t ntrans, double tol, int32_t maxboxes,
+                                          int32_t* group_of_point, int32_t* nboxes, pfsht_box* boxes,
+                                          double* costs, void* stream) {
+    if (!theta || !phi || !nboxes) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "NULL argument");
+    const int v = validate_common(npts, lmax, ntrans, tol);
+    if (v) return (pfsht_status)v;
+    if (maxboxes < 1) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "maxboxes must be >= 1");
+    cudaStream_t s = (cudaStream_t)stream;
+    DevPartition part;
+    int r = partition_boxes_device(theta, phi, npts, lmax, ntrans, tol, maxboxes, s, part);
+    if (r) return (pfsht_status)r;
+    *nboxes = (int32_t)part.idx.size();
+    for (size_t i = 0; i < part.idx.size(); ++i) {
+        if (group_of_point) {
+            std::vector<int32_t> h(part.n[i]);
+            if (part.n[i] > 0 && cudaMemcpy(h.data(), part.idx[i]->p, sizeof(int32_t) * part.n[i],
+                                            cudaMemcpyDeviceToHost) != cudaSuccess)
+                return (pfsht_status)fail(PFSHT_ERR_CUDA, "copying box indices");
+            for (int32_t k : h) group_of_point[k] = (int32_t)i;
+        }
+        if (boxes) boxes[i] = to_abi(part.boxes[i]);
+        if (costs) costs[i] = part.costs[i];
+    }
+    return PFSHT_OK;
+}
+
+pfsht_status pfsht_select_method_device(const double* theta, const double* phi, int64_t npts,
+                                        int32_t lmax, int32_t ntrans, double tol, int32_t* method,
+                                        void* stream) {
+    if (!theta || !phi || !method) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "NULL argument");
+    const int v = validate_common(npts, lmax, ntrans, tol);
+    if (v) return (pfsht_status)v;
+    int m = 0;
+    const int r = select_method_device(theta, phi, npts, lmax, ntrans, tol, (cudaStream_t)stream, &m, nullptr);
+    if (r) return (pfsht_status)r;
+    *method = m;
+    return PFSHT_OK;
+}
+
+pfsht_status pfsht_bounding_box_device(const double* theta, const double* phi, int64_t npts,
+                                       pfsht_box* box, void* stream) {
+    if (!theta || !phi || !box) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "NULL argument");
+    if (npts < 1) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "need at least one point");
+    SphereBox b;
+    const int r = bounding_box_device(theta, phi, npts, (cudaStream_t)stream, &b);
+    if (r) return (pfsht_status)r;
+    *box = to_abi(b);
     return PFSHT_OK;
 }
 

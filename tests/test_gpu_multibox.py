@@ -126,3 +126,43 @@ def test_multibox_in_the_serving_loop_not_in_batches(pf, O, cuda):
     _ = p * to_dev(np.asfortranarray(a))
     st = p.profile_stop()
     assert st["ring_fwd"][1] == 2 and st["interp"][1] == 2
+
+
+def test_device_planner_equals_host_planner(pf, O, cuda):
+    # the planner's scans on the device give the host planner's boxes, groups and costs
+    import torch
+    rng = np.random.default_rng(80)
+    sets = []
+    th, ph = _caps(rng, 40000, 0.2)
+    sets.append((th, ph, 512))
+    t, p = [], []
+    for k in range(5):
+        t.append(0.6 + 0.3 * k + 0.05 * rng.random(9000))
+        p.append(1.2 * k + 0.1 * rng.random(9000) - 2.0)  # negative longitudes: reduced mod 2 pi
+    sets.append((np.concatenate(t), np.concatenate(p), 1024))
+    half = np.deg2rad(8)
+    sets.append((np.pi / 2 + half * (2 * rng.random(60000) - 1), 2 * np.pi * rng.random(60000), 256))
+    sets.append((np.full(5000, 1.0), np.concatenate([0.05 * rng.random(2500),
+                                                     2 * np.pi - 0.05 * rng.random(2500)]), 128))
+    for th, ph, L in sets:
+        dth = torch.from_numpy(th).to(cuda)
+        dph = torch.from_numpy(ph).to(cuda)
+        assert pf.bounding_box(dth, dph) == pf.bounding_box(th, ph)
+        for mb in (3, 8):
+            gh, bh, ch = pf.partition_boxes(th, ph, lmax=L, tol=1e-8, maxboxes=mb)
+            gd, bd, cd = pf.partition_boxes(dth, dph, lmax=L, tol=1e-8, maxboxes=mb)
+            assert len(gh) == len(gd)
+            for a, b in zip(gh, gd):
+                assert np.array_equal(a, b)
+            assert bh == bd and ch == cd
+        assert pf.select_method(dth, dph, lmax=L, tol=1e-8) == pf.select_method(th, ph, lmax=L, tol=1e-8)
+    # a plan of >= 2^15 points is planned on the device: the same boxes as the host partition
+    th, ph, L = sets[0]
+    plan = pf.Plan(torch.from_numpy(th).to(cuda), torch.from_numpy(ph).to(cuda), lmax=L, tol=1e-8)
+    assert plan.info["kind"] == "multibox"
+    gh, _, _ = pf.partition_boxes(th, ph, lmax=L, tol=1e-8)
+    assert [list(b["indices"]) for b in plan.boxes()] == [list(g) for g in gh]
+    alm = O.rand_alm(L, rng=rng)[:, :, 0]
+    g = cn(rng, len(th))
+    f = _fwd(plan, alm)
+    assert dot_rel(f, g, alm, _adj(plan, g)) < 1e-12
