@@ -184,6 +184,23 @@ int32_t pfsht_plan_num_boxes(const pfsht_plan* plan);
 pfsht_status pfsht_plan_box(const pfsht_plan* plan, int32_t box, pfsht_plan_info* info,
                             int64_t* indices);
 
+/* ---- analysis: solve! (src/Analysis.jl:375-436) -------------------------------------------- */
+
+typedef enum {
+    PFSHT_SOLVE_CG = 0,      /* :cg -- stopped at rtol (the stopping rule is the regularisation) */
+    PFSHT_SOLVE_WIENER = 1,  /* :wiener -- Tikhonov with the prior C_l (required) */
+    PFSHT_SOLVE_MINNORM = 2  /* :minnorm -- rtol tightened to min(rtol, 1e-12) */
+} pfsht_solve_mode;
+
+/* Conjugate gradients on (A^H W A + C^-1) alm = A^H W f on the device: f and alm are device
+ * arrays in the plan's layouts (alm is overwritten with the solution); prior is a host array of
+ * lmax + 1 values C_l (WIENER only, NULL otherwise); w is a device array of npts point weights or
+ * NULL. Each iteration is one CUDA graph with device-side scalars; the updates freeze where the
+ * reference's loop breaks. *iters and *relres are the reference's info.iters and info.relres. */
+pfsht_status pfsht_solve(pfsht_plan* plan, const void* f, void* alm, int32_t mode, double rtol,
+                         int32_t maxiter, const double* prior, const double* w, void* stream,
+                         int32_t* iters, double* relres);
+
 /* Host-only plan geometry, no device touched: what pfsht_plan_create would choose for
  * these points (kind, sizes, ring_work). Points are host pointers. nf1/nf2 are the minimum
  * fine-grid lengths; a plan built with timed lengths may use longer ones (pfsht_plan_get_info). */

@@ -27,7 +27,7 @@ __all__ = ["Plan", "AdjointPlan", "Batch", "Server", "mul", "coeff_size", "sph_m
            "plan_geometry", "ring_forward", "ring_adjoint", "NUFFT", "DimensionMismatch",
            "RefusedGeometry", "PFSHTError", "version", "bounding_box", "box_fsky", "cost_direct",
            "cost_stretch", "partition_boxes", "select_method", "cost_constants",
-           "set_cost_constants", "cost_calibrated"]
+           "set_cost_constants", "cost_calibrated", "solve", "shannon_number", "spectral_resolution"]
 
 _lib.load()
 
@@ -222,7 +222,7 @@ class Plan:
         _lib.check(_lib.load().pfsht_plan_create(pth, pph, len(th), int(lmax), int(ntrans),
                                                  float(tol), _lib.PRECISIONS[precision],
                                                  C.byref(o), C.byref(h)), "Plan")
-        del keep
+        self._points = keep  # the plan's points (bounding box for solve's info)
         self._h = h
         self.lmax = int(lmax)
         self.ntrans = int(ntrans)
@@ -543,6 +543,75 @@ def select_method(theta, phi, *, lmax, tol=1e-10, ntrans=1) -> str:
     _lib.check(_lib.load().pfsht_select_method(th.ctypes.data, ph.ctypes.data, len(th), int(lmax),
                                                int(ntrans), float(tol), C.byref(m)), "select_method")
     return {v: k for k, v in _lib.METHODS.items()}[m.value]
+
+
+def shannon_number(lmax, box_or_fsky) -> float:
+    """shannon_number (src/Box.jl:123-132): (lmax+1)^2 f_sky."""
+    fsky = box_fsky(box_or_fsky) if isinstance(box_or_fsky, dict) else float(box_or_fsky)
+    return (int(lmax) + 1) ** 2 * fsky
+
+
+def spectral_resolution(box) -> float:
+    """spectral_resolution (src/Box.jl:141-154): pi / (the box's larger angular extent)."""
+    tiny = np.sqrt(np.finfo(np.float64).eps)
+    mid = min(max((box["theta_lo"] + box["theta_hi"]) / 2, tiny), np.pi - tiny)
+    lam = max(box["theta_hi"] - box["theta_lo"], box["phi_extent"] * np.sin(mid))
+    return np.inf if lam <= 0 else np.pi / lam
+
+
+_SOLVE_MODES = {"cg": 0, "wiener": 1, "minnorm": 2}
+
+
+def solve(alm, plan, f, *, mode="cg", rtol=1e-6, maxiter=500, prior=None, w=None, stream=None):
+    """solve!(alm, plan, f; mode, rtol, maxiter, prior, w) (src/Analysis.jl:375-436):
+    conjugate gradients on (A^H W A + C^-1) alm = A^H W f, run on the device (one CUDA graph per
+    iteration, scalars on the device). ``alm`` (overwritten) and ``f`` are CUDA tensors or host
+    arrays; ``prior`` is C_l for l = 0..lmax ("wiener" only); ``w`` per-point weights. Returns
+    (alm, info) with info's mode, iters, relres, shannon and Δℓ."""
+    if mode not in _SOLVE_MODES:
+        raise ValueError(f"mode must be cg, wiener or minnorm, got {mode!r}")
+    if mode == "wiener" and prior is None:
+        raise ValueError("wiener needs a prior C_l: that prior is what makes the problem well posed")
+    _check_array(alm, _coeff_shapes(plan.lmax, plan.ntrans), "coefficient array")
+    _check_array(f, _field_shapes(plan.npts, plan.ntrans), "field")
+    torch = _torch()
+    dev = torch.device("cuda", plan.device if plan.device >= 0 else torch.cuda.current_device())
+    on_dev = _is_torch(alm) and alm.is_cuda
+    if on_dev != (_is_torch(f) and f.is_cuda):
+        raise ValueError("alm and f must both be CUDA tensors or both host arrays")
+    if on_dev:
+        a_d, f_d = alm, f
+    else:
+        a_d = zeros_alm(plan.lmax, plan.ntrans, device=dev)
+        f_d = zeros_field(plan.npts, plan.ntrans, device=dev)
+        f_d.copy_(torch.from_numpy(np.asarray(f)))
+    pr = None
+    if prior is not None:
+        pr = np.ascontiguousarray(prior, dtype=np.float64)
+        if len(pr) < plan.lmax + 1:
+            raise DimensionMismatch(f"prior must cover l = 0:{plan.lmax}, got {len(pr)} entries")
+    wd = None
+    if w is not None:
+        wd = (w if _is_torch(w) else torch.from_numpy(np.ascontiguousarray(w, dtype=np.float64)))
+        wd = wd.to(device=dev, dtype=torch.float64).contiguous()
+        if wd.numel() != plan.npts:
+            raise DimensionMismatch(f"weights have {wd.numel()} entries, field has {plan.npts}")
+    s = _stream_of(a_d, stream)
+    torch.cuda.current_stream(dev).synchronize()
+    it = C.c_int32()
+    rel = C.c_double()
+    _lib.check(_lib.load().pfsht_solve(plan._h, _ptr(f_d), _ptr(a_d), _SOLVE_MODES[mode], float(rtol),
+                                       int(maxiter), pr.ctypes.data if pr is not None else None,
+                                       wd.data_ptr() if wd is not None else None, s,
+                                       C.byref(it), C.byref(rel)), "solve!")
+    if not on_dev:
+        torch.cuda.synchronize(dev)
+        np.copyto(alm, a_d.cpu().numpy(), casting="no")
+    th, ph = plan._points
+    box = bounding_box(th, ph)
+    info = {"mode": mode, "iters": it.value, "relres": rel.value,
+            "shannon": shannon_number(plan.lmax, box), "Δℓ": spectral_resolution(box)}
+    return alm, info
 
 
 def cost_constants() -> dict:

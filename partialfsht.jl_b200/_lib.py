@@ -108,6 +108,8 @@ SIGNATURES = {
                                                _dp, _vp]),
     "pfsht_select_method_device": (C.c_int, [_vp, _vp, C.c_int64, C.c_int32, C.c_int32, C.c_double,
                                              C.POINTER(C.c_int32), _vp]),
+    "pfsht_solve": (C.c_int, [_vp, _vp, _vp, C.c_int32, C.c_double, C.c_int32, _vp, _vp, _vp,
+                              C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
     "pfsht_set_cost_constants": (C.c_int, [C.c_double, C.c_double, C.c_double, C.c_double]),
     "pfsht_get_cost_constants": (C.c_int, [_dp, _dp, _dp, _dp, C.POINTER(C.c_int32)]),
     "pfsht_plan_num_boxes": (C.c_int32, [_vp]),
