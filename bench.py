@@ -493,6 +493,50 @@ def run_serve(args, world, rank, local):
     return 0
 
 
+def run_solve(args, world, rank, local):
+    """--config solve: solve! (CG) on the device at the headline workload; ms per iteration
+    against one fwd+adj apply (the iteration adds two dot products and three vector updates,
+    and the host stays out of the loop)."""
+    import time
+
+    import torch
+    from __graft_entry__ import load_package
+    pf = load_package()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    M, theta, phi, rng = workload(args.lmax)
+    plan = pf.Plan(theta, phi, lmax=args.lmax, tol=args.tol, precision=args.precision, device=local,
+                   fft_lengths=fft_lengths_arg(args.fft_lengths))
+    alm = torch.from_numpy(rand_alm_host(args.lmax, rng)).to(dev).permute(2, 1, 0)[:, :, 0]
+    f = plan * alm
+    fin = pf.zeros_field(M, device=dev)
+    aout = pf.zeros_alm(args.lmax, device=dev)
+    T_apply, _ = time_applies(pf, plan, [alm], [f], fin, aout, 20, 3, torch.cuda.current_stream(dev))
+    ms_apply = T_apply / 20
+
+    def solve_ms(n):
+        a = pf.zeros_alm(args.lmax, device=dev)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _, info = pf.solve(a, plan, f, mode="cg", rtol=1e-30, maxiter=n)
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) * 1e3, info
+
+    solve_ms(2)  # warm-up: workspace, capture, the plan's bounding box for the info
+    t_short, i_short = solve_ms(5)
+    t_long, i_long = solve_ms(5 + max(100, args.steps // 2))
+    per_iter = (t_long - t_short) / (i_long["iters"] - i_short["iters"])
+    line = {"metric": "ms per CG iteration (solve!, fwd + adj + 2 dots + 3 updates)",
+            "value": per_iter, "unit": "ms", "n_gpus": 1, "higher_is_better": False,
+            "data": "synthetic", "dtype": "f64",
+            "config": dict(config_dict(args, M), solve="cg, rtol below reach, iterations "
+                           f"{i_short['iters']} vs {i_long['iters']} differenced (wall clock)"),
+            "ms_per_fwd_adj_apply": ms_apply, "overhead_per_iteration_ms": per_iter - ms_apply,
+            "relres_after": i_long["relres"]}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_b200(args, world, rank, local):
     import ctypes as C
 
@@ -688,9 +732,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-form measurement")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving measurement")
-    ap.add_argument("--config", default="headline", choices=["headline", "batch", "serve"],
+    ap.add_argument("--config", default="headline", choices=["headline", "batch", "serve", "solve"],
                     help="headline (default): the lmax 2048 cap; batch: 64 plans in one graph; "
-                         "serve: the request loop")
+                         "serve: the request loop; solve: CG iterations of solve!")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
@@ -703,6 +747,8 @@ def main():
             return run_batch(args, world, rank, local) if rank == 0 else 0
         if args.config == "serve":
             return run_serve(args, world, rank, local) if rank == 0 else 0
+        if args.config == "solve":
+            return run_solve(args, world, rank, local) if rank == 0 else 0
         return run_b200(args, world, rank, local)
     finally:
         if world > 1:

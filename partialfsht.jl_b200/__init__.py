@@ -607,8 +607,9 @@ def solve(alm, plan, f, *, mode="cg", rtol=1e-6, maxiter=500, prior=None, w=None
     if not on_dev:
         torch.cuda.synchronize(dev)
         np.copyto(alm, a_d.cpu().numpy(), casting="no")
-    th, ph = plan._points
-    box = bounding_box(th, ph)
+    box = getattr(plan, "_box", None)
+    if box is None:
+        box = plan._box = bounding_box(*plan._points)
     info = {"mode": mode, "iters": it.value, "relres": rel.value,
             "shannon": shannon_number(plan.lmax, box), "Δℓ": spectral_resolution(box)}
     return alm, info

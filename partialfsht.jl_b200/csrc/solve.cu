@@ -56,13 +56,22 @@ __global__ void __launch_bounds__(kThreads) dot_partial_kernel(const double2* __
                                                                const double2* __restrict__ y,
                                                                int64_t n, double2* __restrict__ part) {
     __shared__ double2 sh[kThreads];
-    double sr = 0.0, si = 0.0;
-    for (int64_t t = blockIdx.x * (int64_t)kThreads + threadIdx.x; t < n; t += (int64_t)gridDim.x * kThreads) {
+    double sr = 0.0, si = 0.0, tr = 0.0, ti = 0.0;
+    const int64_t step = (int64_t)gridDim.x * kThreads;
+    int64_t t = blockIdx.x * (int64_t)kThreads + threadIdx.x;
+    for (; t + step < n; t += 2 * step) {  // two loads of each array in flight
+        const double2 a = x[t], b = y[t], c = x[t + step], e = y[t + step];
+        sr += a.x * b.x + a.y * b.y;
+        si += a.x * b.y - a.y * b.x;
+        tr += c.x * e.x + c.y * e.y;
+        ti += c.x * e.y - c.y * e.x;
+    }
+    if (t < n) {
         const double2 a = x[t], b = y[t];
         sr += a.x * b.x + a.y * b.y;
         si += a.x * b.y - a.y * b.x;
     }
-    sh[threadIdx.x] = make_double2(sr, si);
+    sh[threadIdx.x] = make_double2(sr + tr, si + ti);
     __syncthreads();
     for (int o = kThreads / 2; o > 0; o >>= 1) {
         if (threadIdx.x < o) {
@@ -117,22 +126,39 @@ __global__ void __launch_bounds__(kThreads) alpha_kernel(const double2* __restri
     }
 }
 
-// alm += alpha p; r -= alpha Ap
-__global__ void update_xr_kernel(double2* __restrict__ alm, double2* __restrict__ r,
-                                 const double2* __restrict__ p, const double2* __restrict__ Ap,
-                                 int64_t n, const SolveState* __restrict__ st) {
-    if (st->done) return;
+// alm += alpha p; r -= alpha Ap; and the per-block partial sums of |r|^2 of the new residual
+// (for dot(r, r)) in the same pass. Frozen: r is unchanged and the partials are its norm.
+__global__ void __launch_bounds__(kThreads) update_xr_kernel(double2* __restrict__ alm,
+                                                             double2* __restrict__ r,
+                                                             const double2* __restrict__ p,
+                                                             const double2* __restrict__ Ap, int64_t n,
+                                                             const SolveState* __restrict__ st,
+                                                             double2* __restrict__ part) {
+    __shared__ double2 sh[kThreads];
+    const bool frozen = st->done != 0;
     const double2 a = st->alpha;
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
-        const double2 pv = p[t], qv = Ap[t];
-        double2 x = alm[t], y = r[t];
-        x.x += a.x * pv.x - a.y * pv.y;
-        x.y += a.x * pv.y + a.y * pv.x;
-        y.x -= a.x * qv.x - a.y * qv.y;
-        y.y -= a.x * qv.y + a.y * qv.x;
-        alm[t] = x;
-        r[t] = y;
+    double sr = 0.0;
+    for (int64_t t = blockIdx.x * (int64_t)kThreads + threadIdx.x; t < n; t += (int64_t)gridDim.x * kThreads) {
+        double2 y = r[t];
+        if (!frozen) {
+            const double2 pv = p[t], qv = Ap[t];
+            double2 x = alm[t];
+            x.x += a.x * pv.x - a.y * pv.y;
+            x.y += a.x * pv.y + a.y * pv.x;
+            y.x -= a.x * qv.x - a.y * qv.y;
+            y.y -= a.x * qv.y + a.y * qv.x;
+            alm[t] = x;
+            r[t] = y;
+        }
+        sr += y.x * y.x + y.y * y.y;
     }
+    sh[threadIdx.x] = make_double2(sr, 0.0);
+    __syncthreads();
+    for (int o = kThreads / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) sh[threadIdx.x].x += sh[threadIdx.x + o].x;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
 }
 
 // rsnew = dot(r, r); count the iteration; stop at rel <= tol, else beta = rsnew / rsold
@@ -287,8 +313,7 @@ int run_solve(pfsht_plan* pl, const double2* f, double2* alm, int mode, double r
     if (!rc) {
         dot_partial_kernel<<<kDotBlocks, kThreads, 0, cs>>>(d_p, d_Ap, nc, d_part);
         alpha_kernel<<<1, kThreads, 0, cs>>>(d_part, st);
-        update_xr_kernel<<<grid_n(nc), kThreads, 0, cs>>>(alm, d_r, d_p, d_Ap, nc, st);
-        dot_partial_kernel<<<kDotBlocks, kThreads, 0, cs>>>(d_r, d_r, nc, d_part);
+        update_xr_kernel<<<kDotBlocks, kThreads, 0, cs>>>(alm, d_r, d_p, d_Ap, nc, st, d_part);
         rsnew_kernel<<<1, kThreads, 0, cs>>>(d_part, st);
         update_p_kernel<<<grid_n(nc), kThreads, 0, cs>>>(d_p, d_r, nc, st);
         rc = check_launch("solve iteration kernels");
