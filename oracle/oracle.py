@@ -109,6 +109,19 @@ def lib():
         "orc_direct_adjoint": (None, [vp, vp, vp, C.c_int]),
         "orc_stretch_create": (vp, [_dp, _dp, C.c_int64, C.c_int, C.c_int, C.c_double, C.c_int,
                                     C.c_double, C.c_double, C.c_double, C.POINTER(C.c_int)]),
+        "orc_stretch_create_spin": (vp, [_dp, _dp, C.c_int64, C.c_int, C.c_int, C.c_double, C.c_int,
+                                         C.c_double, C.c_double, C.c_double, C.c_int,
+                                         C.POINTER(C.c_int)]),
+        "orc_wigner_d": (C.c_double, [C.c_int, C.c_int, C.c_int, C.c_double]),
+        "orc_spin_rings_create": (vp, [_dp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int]),
+        "orc_spin_rings_destroy": (None, [vp]),
+        "orc_spin_rings_mmax": (C.c_int, [vp]),
+        "orc_spin_rings_nchunks": (C.c_int, [vp]),
+        "orc_spin_rings_work": (C.c_int64, [vp]),
+        "orc_spin_rings_from_alm": (None, [vp, vp, vp, C.c_int]),
+        "orc_spin_alm_from_rings": (None, [vp, vp, vp, C.c_int]),
+        "orc_spin_direct": (None, [C.c_int, _dp, _dp, C.c_int64, C.c_int, C.c_int, C.c_int, vp, vp,
+                                   C.c_int]),
         "orc_stretch_destroy": (None, [vp]),
         "orc_stretch_info_get": (None, [vp, C.POINTER(_StretchInfo)]),
         "orc_stretch_tables": (None, [vp, _dp, _dp, _dp, _dp, _dp]),
@@ -518,16 +531,17 @@ class Stretch:
     the minimum 2,3,5-smooth lengths), e.g. to those of a device plan."""
 
     def __init__(self, theta, phi, lmax, tol, ntrans=1, nufft="es", eps_apo_max=1.0,
-                 oversample_theta=1.0, oversample_phi=1.0, nufft_grid=None):
+                 oversample_theta=1.0, oversample_phi=1.0, nufft_grid=None, spin=0):
         self.theta = _f64(theta)
         self.phi = _f64(phi)
         self.M = len(self.theta)
+        self.spin = int(spin)
         st = C.c_int(0)
         kind = {"direct": 0, "es": 1, "es_exact": 2}[nufft]
-        self._h = lib().orc_stretch_create(self.theta, self.phi, self.M, int(lmax), int(ntrans),
-                                           float(tol), kind, float(eps_apo_max),
-                                           float(oversample_theta), float(oversample_phi),
-                                           C.byref(st))
+        self._h = lib().orc_stretch_create_spin(self.theta, self.phi, self.M, int(lmax), int(ntrans),
+                                                float(tol), kind, float(eps_apo_max),
+                                                float(oversample_theta), float(oversample_phi),
+                                                self.spin, C.byref(st))
         if not self._h:
             if st.value == 1:
                 raise RefusedGeometry("stretched transform is degenerate at this lmax and tol")
@@ -540,7 +554,8 @@ class Stretch:
         self.info = {name: getattr(i, name) for name, _ in _StretchInfo._fields_}
         self.info["kind"] = KINDS[i.kind]
         self.lmax, self.ntrans = int(lmax), int(ntrans)
-        self.rings = Rings._borrow(lib().orc_stretch_rings_engine(self._h), self.lmax, self.ntrans)
+        self.rings = (Rings._borrow(lib().orc_stretch_rings_engine(self._h), self.lmax, self.ntrans)
+                      if self.spin == 0 else None)
 
     def __del__(self):
         if getattr(self, "_h", None):
@@ -576,3 +591,103 @@ class Stretch:
 def cdot(a, b) -> complex:
     """Julia's dot(a, b) = sum(conj(a) .* b)."""
     return complex(np.vdot(np.ravel(a, order="F"), np.ravel(b, order="F")))
+
+
+# ---------------------------------------------------------------------------------------
+# spin-weighted transforms (src/Spin.jl); coefficients in the (l+1, m+lmax+1) layout
+# ---------------------------------------------------------------------------------------
+def wigner_d(l, m, n, beta):
+    """wigner_d (src/Spin.jl:58-131)."""
+    return float(lib().orc_wigner_d(int(l), int(m), int(n), float(beta)))
+
+
+def sylm(s, l, m, theta, phi):
+    """sYlm (src/Spin.jl:138-142): N_l d^l_{m,-s}(theta) e^{i m phi}."""
+    if abs(s) > l:
+        return 0j
+    return np.sqrt((2 * l + 1) / (4 * np.pi)) * wigner_d(l, m, -s, theta) * np.exp(1j * m * phi)
+
+
+def spin_coeff_index(l, m, lmax):
+    """spin_coeff_index (src/Layout.jl:28-29), 0-based (row, column)."""
+    return l, m + lmax
+
+
+def spin_valid_mask(lmax, spin):
+    """Slots holding a spin-s mode: |m| <= l and l >= |s|."""
+    l = np.arange(lmax + 1)[:, None]
+    m = np.arange(-lmax, lmax + 1)[None, :]
+    return (np.abs(m) <= l) & (l >= abs(spin))
+
+
+def rand_spin_alm(lmax, spin, ntrans=1, rng=None):
+    rng = np.random.default_rng(0) if rng is None else rng
+    a = np.zeros((lmax + 1, 2 * lmax + 1, ntrans), np.complex128, order="F")
+    mask = spin_valid_mask(lmax, spin)
+    for b in range(ntrans):
+        a[:, :, b][mask] = rng.standard_normal(mask.sum()) + 1j * rng.standard_normal(mask.sum())
+    return a
+
+
+class SpinRings:
+    """SpinRings (src/Spin.jl:175-280) on ascending ring colatitudes."""
+
+    def __init__(self, theta_rings, lmax, spin, eps, ntrans=1, reflect=False):
+        self.theta = np.ascontiguousarray(theta_rings, dtype=np.float64)
+        self.lmax, self.spin, self.ntrans = int(lmax), int(spin), int(ntrans)
+        self._h = lib().orc_spin_rings_create(self.theta, len(self.theta), self.lmax, self.spin,
+                                              float(eps), self.ntrans, 1 if reflect else 0)
+        if not self._h:
+            raise ValueError("ring colatitudes must be ascending and unimodal in their limits")
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().orc_spin_rings_destroy(self._h)
+            self._h = None
+
+    @property
+    def mmax(self):
+        return int(lib().orc_spin_rings_mmax(self._h))
+
+    @property
+    def nchunks(self):
+        return int(lib().orc_spin_rings_nchunks(self._h))
+
+    def ring_work(self):
+        return int(lib().orc_spin_rings_work(self._h))
+
+    def rings_from_alm(self, alm, nthreads=1):
+        alm = _as3(alm, None)
+        G = np.zeros((len(self.theta), 2 * self.lmax + 1, self.ntrans), np.complex128, order="F")
+        lib().orc_spin_rings_from_alm(self._h, _ptr(alm), _ptr(G), int(nthreads))
+        return G
+
+    def alm_from_rings(self, G, nthreads=1):
+        G = np.asfortranarray(np.asarray(G, dtype=np.complex128).reshape(
+            (len(self.theta), 2 * self.lmax + 1, self.ntrans), order="F"))
+        alm = np.zeros((self.lmax + 1, 2 * self.lmax + 1, self.ntrans), np.complex128, order="F")
+        lib().orc_spin_alm_from_rings(self._h, _ptr(G), _ptr(alm), int(nthreads))
+        return alm
+
+
+class SpinDirect:
+    """SpinDirectLeaf (src/Spin.jl:557-630): the O(M L^2) spin oracle."""
+
+    def __init__(self, theta, phi, lmax, spin, ntrans=1):
+        self.theta, self.phi = _f64(theta), _f64(phi)
+        self.lmax, self.spin, self.ntrans = int(lmax), int(spin), int(ntrans)
+
+    def forward(self, alm, nthreads=1):
+        alm = _as3(alm, None)
+        f = np.zeros((len(self.theta), self.ntrans), np.complex128, order="F")
+        lib().orc_spin_direct(1, self.theta, self.phi, len(self.theta), self.lmax, self.spin,
+                              self.ntrans, _ptr(alm), _ptr(f), int(nthreads))
+        return f
+
+    def adjoint(self, f, nthreads=1):
+        f = np.asfortranarray(np.asarray(f, dtype=np.complex128).reshape(
+            (len(self.theta), self.ntrans), order="F"))
+        alm = np.zeros((self.lmax + 1, 2 * self.lmax + 1, self.ntrans), np.complex128, order="F")
+        lib().orc_spin_direct(0, self.theta, self.phi, len(self.theta), self.lmax, self.spin,
+                              self.ntrans, _ptr(f), _ptr(alm), int(nthreads))
+        return alm

@@ -1301,6 +1301,8 @@ struct orc_stretch {
     double *th_r, *Th_r, *w, *Thp, *php;
     cplx *phase;
     orc_rings* eng;
+    int spin;
+    orc_spin_rings* seng;  /* spin != 0: the Wigner-d engine (src/Stretch.jl:190-192) */
     int nufft_kind;
     orc_esnufft* es;
     cplx *G, *Fphi, *F, *Ft, *Fhat;
@@ -1309,6 +1311,13 @@ struct orc_stretch {
 orc_stretch* orc_stretch_create(const double* theta, const double* phi, int64_t M, int lmax,
                                 int ntrans, double tol, int nufft_kind, double eps_apo_max,
                                 double ovs_th, double ovs_ph, int* status) {
+    return orc_stretch_create_spin(theta, phi, M, lmax, ntrans, tol, nufft_kind, eps_apo_max,
+                                   ovs_th, ovs_ph, 0, status);
+}
+
+orc_stretch* orc_stretch_create_spin(const double* theta, const double* phi, int64_t M, int lmax,
+                                     int ntrans, double tol, int nufft_kind, double eps_apo_max,
+                                     double ovs_th, double ovs_ph, int spin, int* status) {
     *status = 0;
     if (M < 1 || lmax < 0 || ntrans < 1) { *status = 2; return NULL; }
     /* bounding_box colatitude extent (src/Box.jl:51-59) */
@@ -1342,10 +1351,19 @@ orc_stretch* orc_stretch_create(const double* theta, const double* phi, int64_t 
     s->th_r = (double*)malloc(sizeof(double) * nth_half);
     s->Th_r = (double*)malloc(sizeof(double) * nth_half);
     orc_stretch_rings(&g, nth_half, s->th_r, s->Th_r);
-    s->eng = orc_rings_create(s->th_r, nth_half, lmax, tol, ntrans, flip);
-    if (!s->eng) { *status = 2; orc_stretch_destroy(s); return NULL; }
-    int mmax = s->eng->mmax;
-    int nph = (int)orc_next_smooth_even((int64_t)ceil((2.0 * mmax + 1) * ovs_ph));
+    s->spin = spin;
+    int mmax;
+    if (spin == 0) {
+        s->eng = orc_rings_create(s->th_r, nth_half, lmax, tol, ntrans, flip);
+        if (!s->eng) { *status = 2; orc_stretch_destroy(s); return NULL; }
+        mmax = s->eng->mmax;
+    } else {
+        s->seng = orc_spin_rings_create(s->th_r, nth_half, lmax, spin, tol, ntrans, flip);
+        if (!s->seng) { *status = 2; orc_stretch_destroy(s); return NULL; }
+        mmax = orc_spin_rings_mmax(s->seng);
+    }
+    int mm = mmax > abs(spin) ? mmax : abs(spin);
+    int nph = (int)orc_next_smooth_even((int64_t)ceil((2.0 * mm + 1) * ovs_ph));
     s->w = (double*)malloc(sizeof(double) * nth_half);
     for (int i = 0; i < nth_half; ++i) s->w[i] = orc_stretch_window(&g, s->Th_r[i]);
     s->Thp = (double*)malloc(sizeof(double) * M);
@@ -1384,7 +1402,7 @@ orc_stretch* orc_stretch_create(const double* theta, const double* phi, int64_t 
     in->mmax = mmax;
     in->nrings = nth_half;
     in->K = g.K;
-    in->ring_work = orc_rings_work(s->eng);
+    in->ring_work = spin == 0 ? orc_rings_work(s->eng) : orc_spin_rings_work(s->seng);
     in->M = M;
     in->eps = g.eps;
     in->beta = g.beta;
@@ -1404,6 +1422,7 @@ void orc_stretch_destroy(orc_stretch* s) {
     if (!s) return;
     free(s->th_r); free(s->Th_r); free(s->w); free(s->Thp); free(s->php); free(s->phase);
     orc_rings_destroy(s->eng);
+    orc_spin_rings_destroy(s->seng);
     orc_esnufft_destroy(s->es);
     free(s->G); free(s->Fphi); free(s->F); free(s->Ft); free(s->Fhat);
     free(s);
@@ -1434,7 +1453,8 @@ void orc_stretch_forward(orc_stretch* s, const double* alm, double* f, int nthre
     const int L = in->lmax, B = in->ntrans, nh = in->nth_half, nth = in->nth, nph = in->nph;
     const int64_t M = in->M;
     /* _fill_rings! */
-    orc_rings_from_alm(s->eng, alm, (double*)s->G, nthreads);
+    if (s->spin == 0) orc_rings_from_alm(s->eng, alm, (double*)s->G, nthreads);
+    else orc_spin_rings_from_alm(s->seng, alm, (double*)s->G, nthreads);
     /* _rings_to_grid!: _pack_orders! (src/Stretch.jl:341-350) then bfft along phi */
     int mk = mkeep_of(nph, L);
     memset(s->Fphi, 0, sizeof(cplx) * (size_t)nh * nph * B);
@@ -1457,7 +1477,7 @@ void orc_stretch_forward(orc_stretch* s, const double* alm, double* f, int nthre
             }
     /* _periodize! */
     if (in->kind == ORC_INTERIOR) memcpy(s->Ft, s->F, sizeof(cplx) * (size_t)nh * nph * B);
-    else orc_dfs_double((double*)s->F, (double*)s->Ft, nh, nph, B, 0);
+    else orc_dfs_double((double*)s->F, (double*)s->Ft, nh, nph, B, s->spin);
     /* 2-D fft, then phase */
     memcpy(s->Fhat, s->Ft, sizeof(cplx) * (size_t)nth * nph * B);
     for (int b = 0; b < B; ++b) {
@@ -1496,7 +1516,7 @@ void orc_stretch_adjoint(orc_stretch* s, const double* f, double* alm, int nthre
         orc_fft_rows(blk, nth, nph, +1, nthreads);
     }
     if (in->kind == ORC_INTERIOR) memcpy(s->F, s->Ft, sizeof(cplx) * (size_t)nh * nph * B);
-    else orc_dfs_fold((double*)s->F, (const double*)s->Ft, nh, nph, B, 0);
+    else orc_dfs_fold((double*)s->F, (const double*)s->Ft, nh, nph, B, s->spin);
     for (int b = 0; b < B; ++b)
         for (int j = 0; j < nph; ++j)
             for (int i = 0; i < nh; ++i) {
@@ -1516,5 +1536,416 @@ void orc_stretch_adjoint(orc_stretch* s, const double* f, double* alm, int nthre
             memcpy(s->G + (int64_t)nh * (L - m) + (int64_t)nh * (2 * L + 1) * b,
                    s->Fphi + (int64_t)nh * (nph - m) + (int64_t)nh * nph * b, sizeof(cplx) * nh);
     }
-    orc_alm_from_rings(s->eng, (const double*)s->G, alm, nthreads);
+    if (s->spin == 0) orc_alm_from_rings(s->eng, (const double*)s->G, alm, nthreads);
+    else orc_spin_alm_from_rings(s->seng, (const double*)s->G, alm, nthreads);
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* spin-weighted transforms (src/Spin.jl)                                                 */
+/* ------------------------------------------------------------------------------------ */
+static double spin_Nl(int l) { return sqrt((2.0 * l + 1) / (4 * M_PI)); }
+static inline cplx c_make(double re, double im) { cplx r = {re, im}; return r; }
+
+/* log sqrt(C(2l, l - a)) (src/Spin.jl:26-29) */
+static double half_lbinom(int l, int a) {
+    return (lgamma(2.0 * l + 1) - lgamma((double)(l - a) + 1) - lgamma((double)(l + a) + 1)) / 2;
+}
+
+/* _d_extremal (src/Spin.jl:38-51): log|d^l_{a,b}(beta)| and its sign, |b| = l */
+static void d_extremal(int l, int a, int b, double beta, double* lg, double* sg) {
+    double c = cos(beta / 2), s = sin(beta / 2);
+    double lb = half_lbinom(l, a);
+    int pc, ps;
+    double sgn;
+    if (b == l) { pc = l + a; ps = l - a; sgn = 1.0; }
+    else { pc = l - a; ps = l + a; sgn = ((l - a) % 2 == 0) ? 1.0 : -1.0; }
+    double lc = pc == 0 ? 0.0 : (c > 0 ? (double)pc * log(c) : -INFINITY);
+    double ls = ps == 0 ? 0.0 : (s > 0 ? (double)ps * log(s) : -INFINITY);
+    *lg = lb + lc + ls;
+    *sg = sgn;
+}
+
+/* wigner_d (src/Spin.jl:58-131): block-scaled degree recurrence at fixed (m, n) */
+double orc_wigner_d(int l, int mm, int nn, double b) {
+    if (abs(mm) > l || abs(nn) > l) return 0.0;
+    double tiny = sqrt(DBL_EPSILON);
+    if (b <= tiny) return mm == nn ? 1.0 : 0.0;
+    if (b >= M_PI - tiny) return mm == -nn ? (((l - nn) % 2 == 0) ? 1.0 : -1.0) : 0.0;
+    int l0 = abs(mm) > abs(nn) ? abs(mm) : abs(nn);
+    double lg, sg;
+    if (abs(nn) == l0) {
+        d_extremal(l0, mm, nn == l0 ? l0 : -l0, b, &lg, &sg);
+    } else {
+        d_extremal(l0, nn, mm == l0 ? l0 : -l0, b, &lg, &sg);
+        if (((nn - mm) % 2 + 2) % 2 == 1) sg = -sg;
+    }
+    if (!isfinite(lg)) return 0.0;
+    double E = ceil(lg / log(2.0));
+    double d1 = sg * exp(lg - E * log(2.0));
+    if (l == l0) return d1 * exp2(E);
+    double cb = cos(b);
+    double d0 = 0.0;
+    int Lc = l0;
+    if (l0 == 0) {
+        d0 = d1;
+        d1 = d1 * cb;
+        Lc = 1;
+        if (l == 1) return d1 * exp2(E);
+    }
+    int steps = 0;
+    while (Lc < l) {
+        int L1 = Lc + 1;
+        double sm1 = sqrt(fmax(0.0, (double)(L1 * L1 - mm * mm)));
+        double sn1 = sqrt(fmax(0.0, (double)(L1 * L1 - nn * nn)));
+        double den = (double)Lc * sm1 * sn1;
+        if (den <= 0) { d0 = d1; d1 = 0.0; Lc = L1; continue; }
+        double sm0 = sqrt(fmax(0.0, (double)(Lc * Lc - mm * mm)));
+        double sn0 = sqrt(fmax(0.0, (double)(Lc * Lc - nn * nn)));
+        double c1 = (double)(2 * Lc + 1) * ((double)Lc * (double)L1 * cb - (double)mm * (double)nn) / den;
+        double c0 = (double)L1 * sm0 * sn0 / den;
+        double dn = c1 * d1 - c0 * d0;
+        d0 = d1;
+        d1 = dn;
+        Lc = L1;
+        if (++steps == RESCALE_STRIDE) {
+            steps = 0;
+            double mx = fmax(fabs(d1), fabs(d0));
+            if (mx > 0 && isfinite(mx)) {
+                double sh = ceil(log2(mx));
+                if (sh != 0) { double f = exp2(-sh); d1 *= f; d0 *= f; E += sh; }
+            }
+        }
+    }
+    return d1 * exp2(E);
+}
+
+/* SpinRings (src/Spin.jl:175-280) */
+struct orc_spin_rings {
+    int n, L, s, B, mmax;
+    double eps;
+    double *cos_t, *log2cos, *log2sin, *Nl, *lb2, *sg;
+    int *pc, *ps, *mlim, *jlo, *jhi; /* jlo/jhi over m = -L..L */
+    int nchunks, *clo, *chi;
+};
+
+orc_spin_rings* orc_spin_rings_create(const double* theta, int n, int lmax, int spin, double eps,
+                                      int ntrans, int reflect) {
+    if (lmax < 0 || ntrans < 1 || n < 1) return NULL;
+    for (int j = 1; j < n; ++j)
+        if (theta[j] < theta[j - 1]) return NULL;
+    orc_spin_rings* e = (orc_spin_rings*)calloc(1, sizeof(orc_spin_rings));
+    const int L = lmax, nm = 2 * lmax + 1, as = abs(spin);
+    e->n = n; e->L = L; e->s = spin; e->B = ntrans; e->eps = eps;
+    e->cos_t = (double*)malloc(sizeof(double) * n);
+    e->log2cos = (double*)malloc(sizeof(double) * n);
+    e->log2sin = (double*)malloc(sizeof(double) * n);
+    e->mlim = (int*)malloc(sizeof(int) * n);
+    e->Nl = (double*)malloc(sizeof(double) * (L + 1));
+    e->lb2 = (double*)malloc(sizeof(double) * nm);
+    e->sg = (double*)malloc(sizeof(double) * nm);
+    e->pc = (int*)malloc(sizeof(int) * nm);
+    e->ps = (int*)malloc(sizeof(int) * nm);
+    e->jlo = (int*)malloc(sizeof(int) * nm);
+    e->jhi = (int*)malloc(sizeof(int) * nm);
+    e->clo = (int*)malloc(sizeof(int) * n);
+    e->chi = (int*)malloc(sizeof(int) * n);
+    double csgn = reflect ? -1.0 : 1.0;
+    for (int j = 0; j < n; ++j) {
+        double t = theta[j];
+        e->cos_t[j] = csgn * cos(t);
+        double ch = cos(t / 2), sh = fabs(sin(t / 2));
+        if (reflect) { double x = ch; ch = sh; sh = x; }
+        e->log2cos[j] = ch > 0 ? log2(ch) : -INFINITY;
+        e->log2sin[j] = sh > 0 ? log2(sh) : -INFINITY;
+        int ml = orc_polar_mmax(t, L, eps);
+        e->mlim[j] = ml > as ? ml : as;
+    }
+    int* jlo0 = (int*)malloc(sizeof(int) * (L + 1));
+    int* jhi0 = (int*)malloc(sizeof(int) * (L + 1));
+    if (orc_nested_ranges(e->mlim, n, L, jlo0, jhi0) != 0) {
+        free(jlo0); free(jhi0);
+        orc_spin_rings_destroy(e);
+        return NULL;
+    }
+    for (int m = 0; m <= L; ++m) {
+        e->jlo[m + L] = e->jlo[L - m] = jlo0[m];
+        e->jhi[m + L] = e->jhi[L - m] = jhi0[m];
+    }
+    free(jlo0); free(jhi0);
+    const int nn = -spin;
+    const double inv_ln2 = 1.0 / log(2.0);
+    for (int m = -L; m <= L; ++m) {
+        int idx = m + L;
+        int l0 = abs(m) > abs(nn) ? abs(m) : abs(nn);
+        if (l0 > L) { e->lb2[idx] = -INFINITY; e->pc[idx] = 0; e->ps[idx] = 0; e->sg[idx] = 1.0; continue; }
+        int a, b;
+        double extra;
+        if (abs(nn) == l0) { a = m; b = nn == l0 ? l0 : -l0; extra = 1.0; }
+        else { a = nn; b = m == l0 ? l0 : -l0; extra = ((((nn - m) % 2) + 2) % 2 == 1) ? -1.0 : 1.0; }
+        double sgn;
+        if (b == l0) { e->pc[idx] = l0 + a; e->ps[idx] = l0 - a; sgn = 1.0; }
+        else { e->pc[idx] = l0 - a; e->ps[idx] = l0 + a; sgn = ((l0 - a) % 2 == 0) ? 1.0 : -1.0; }
+        e->lb2[idx] = half_lbinom(l0, a) * inv_ln2;
+        e->sg[idx] = sgn * extra;
+    }
+    /* _spin_ring_chunks (src/Spin.jl:291-317) */
+    int i = 0, nc = 0;
+    while (i < n) {
+        int stop = i;
+        int l0max = e->mlim[i] > as ? e->mlim[i] : as;
+        while (stop < n - 1) {
+            int nxt = stop + 1;
+            if (nxt - i + 1 > CHUNK_MAX) break;
+            double spanc = fabs(e->log2cos[nxt] - e->log2cos[i]);
+            double spans = fabs(e->log2sin[nxt] - e->log2sin[i]);
+            double span = fmax(isfinite(spanc) ? spanc : INFINITY, isfinite(spans) ? spans : INFINITY);
+            int l0 = l0max;
+            if (e->mlim[nxt] > l0) l0 = e->mlim[nxt];
+            if (as > l0) l0 = as;
+            if (2.0 * l0 * span > CHUNK_HEADROOM_BITS) break;
+            l0max = l0;
+            stop = nxt;
+        }
+        e->clo[nc] = i;
+        e->chi[nc] = stop;
+        ++nc;
+        i = stop + 1;
+    }
+    e->nchunks = nc;
+    for (int l = 0; l <= L; ++l) e->Nl[l] = spin_Nl(l);
+    int mx = 0;
+    for (int j = 0; j < n; ++j) mx = e->mlim[j] > mx ? e->mlim[j] : mx;
+    e->mmax = mx;
+    return e;
+}
+
+void orc_spin_rings_destroy(orc_spin_rings* e) {
+    if (!e) return;
+    free(e->cos_t); free(e->log2cos); free(e->log2sin); free(e->mlim); free(e->Nl); free(e->lb2);
+    free(e->sg); free(e->pc); free(e->ps); free(e->jlo); free(e->jhi); free(e->clo); free(e->chi);
+    free(e);
+}
+
+int orc_spin_rings_mmax(const orc_spin_rings* e) { return e->mmax; }
+int orc_spin_rings_nchunks(const orc_spin_rings* e) { return e->nchunks; }
+
+/* retained (l, m, ring) triples of the spin walk: m = -L..L, l from max(|m|, |s|) */
+int64_t orc_spin_rings_work(const orc_spin_rings* e) {
+    int64_t w = 0;
+    for (int m = -e->L; m <= e->L; ++m) {
+        int nj = e->jhi[m + e->L] - e->jlo[m + e->L] + 1;
+        int l0 = abs(m) > abs(e->s) ? abs(m) : abs(e->s);
+        if (nj > 0 && l0 <= e->L) w += (int64_t)nj * (e->L - l0 + 1);
+    }
+    return w;
+}
+
+static double spin_seed_log2(const orc_spin_rings* e, int j, double lb2, int pc, int ps) {
+    double v = lb2;
+    if (pc != 0) v += (double)pc * e->log2cos[j];
+    if (ps != 0) v += (double)ps * e->log2sin[j];
+    return v;
+}
+
+/* spin coefficient (l, m) of transform b in the (l+1, m+lmax+1) layout (src/Layout.jl:28-29) */
+static size_t spin_idx(int l, int m, int L, int b) {
+    return (size_t)l + (size_t)(L + 1) * (m + L) + (size_t)(L + 1) * (2 * L + 1) * b;
+}
+
+/* _spin_chunk! (src/Spin.jl:376-490) */
+static void spin_chunk(int fwd, const orc_spin_rings* e, cplx* G, const cplx* almin, cplx* almout,
+                       int m, int r0, int r1, double* d1, double* d0, cplx* acc) {
+    const int L = e->L, B = e->B, off = L, nn = -e->s, nr = r1 - r0 + 1;
+    int l0 = abs(m) > abs(nn) ? abs(m) : abs(nn);
+    if (l0 > L) return;
+    const int mi = m + L;
+    const double lb2 = e->lb2[mi], sg = e->sg[mi];
+    const int pc = e->pc[mi], ps = e->ps[mi];
+    double E = -INFINITY;
+    for (int j = r0; j <= r1; ++j) E = fmax(E, spin_seed_log2(e, j, lb2, pc, ps));
+    E = isfinite(E) ? ceil(E) : 0.0;
+    for (int k = 0; k < nr; ++k) {
+        double v = spin_seed_log2(e, r0 + k, lb2, pc, ps);
+        d1[k] = isfinite(v) ? sg * exp2(v - E) : 0.0;
+        d0[k] = 0.0;
+    }
+    const size_t gs = (size_t)e->n * (2 * L + 1);
+    for (int b = 0; b < B; ++b)
+        for (int k = 0; k < nr; ++k)
+            acc[k + (size_t)nr * b] = fwd ? c_make(0, 0) : G[(r0 + k) + (size_t)e->n * (m + off) + gs * b];
+    /* touch at l0 */
+    if (fwd) {
+        for (int b = 0; b < B; ++b) {
+            cplx a = c_scale(almin[spin_idx(l0, m, L, b)], e->Nl[l0]);
+            if (a.re == 0 && a.im == 0) continue;
+            for (int k = 0; k < nr; ++k) acc[k + (size_t)nr * b] = c_add(acc[k + (size_t)nr * b], c_scale(a, d1[k]));
+        }
+    } else {
+        double f = exp2(E) * e->Nl[l0];
+        for (int b = 0; b < B; ++b) {
+            cplx s = c_make(0, 0);
+            for (int k = 0; k < nr; ++k) s = c_add(s, c_scale(acc[k + (size_t)nr * b], d1[k]));
+            cplx* t = &almout[spin_idx(l0, m, L, b)];
+            *t = c_add(*t, c_scale(s, f));
+        }
+    }
+    int steps = 0, Lc = l0;
+    while (Lc < L) {
+        int L1 = Lc + 1;
+        double sm1 = sqrt(fmax(0.0, (double)(L1 * L1 - m * m)));
+        double sn1 = sqrt(fmax(0.0, (double)(L1 * L1 - nn * nn)));
+        double den = (double)Lc * sm1 * sn1;
+        if (den <= 0) {
+            for (int k = 0; k < nr; ++k) { d0[k] = d1[k]; d1[k] = 0.0; }
+            Lc = L1;
+            continue;
+        }
+        double sm0 = sqrt(fmax(0.0, (double)(Lc * Lc - m * m)));
+        double sn0 = sqrt(fmax(0.0, (double)(Lc * Lc - nn * nn)));
+        double a1 = (double)(2 * Lc + 1) * (double)Lc * (double)L1 / den;
+        double a2 = (double)(2 * Lc + 1) * (double)m * (double)nn / den;
+        double a0 = (double)L1 * sm0 * sn0 / den;
+        for (int k = 0; k < nr; ++k) {
+            double dn = (a1 * e->cos_t[r0 + k] - a2) * d1[k] - a0 * d0[k];
+            d0[k] = d1[k];
+            d1[k] = dn;
+        }
+        Lc = L1;
+        if (fwd) {
+            double N = e->Nl[Lc];
+            for (int b = 0; b < B; ++b) {
+                cplx a = c_scale(almin[spin_idx(Lc, m, L, b)], N);
+                if (a.re == 0 && a.im == 0) continue;
+                for (int k = 0; k < nr; ++k) acc[k + (size_t)nr * b] = c_add(acc[k + (size_t)nr * b], c_scale(a, d1[k]));
+            }
+        } else {
+            double f = exp2(E) * e->Nl[Lc];
+            for (int b = 0; b < B; ++b) {
+                cplx s = c_make(0, 0);
+                for (int k = 0; k < nr; ++k) s = c_add(s, c_scale(acc[k + (size_t)nr * b], d1[k]));
+                cplx* t = &almout[spin_idx(Lc, m, L, b)];
+                *t = c_add(*t, c_scale(s, f));
+            }
+        }
+        if (++steps == RESCALE_STRIDE && Lc < L) {
+            steps = 0;
+            double mx = 0.0;
+            for (int k = 0; k < nr; ++k) mx = fmax(mx, fmax(fabs(d1[k]), fabs(d0[k])));
+            if (mx > 0 && isfinite(mx)) {
+                double sh = ceil(log2(mx));
+                if (sh != 0) {
+                    double f = exp2(-sh);
+                    for (int k = 0; k < nr; ++k) { d1[k] *= f; d0[k] *= f; }
+                    if (fwd)
+                        for (int q = 0; q < nr * B; ++q) acc[q] = c_scale(acc[q], f);
+                    E += sh;
+                }
+            }
+        }
+    }
+    if (fwd) {
+        double f = exp2(E);
+        for (int b = 0; b < B; ++b)
+            for (int k = 0; k < nr; ++k) {
+                cplx* t = &G[(r0 + k) + (size_t)e->n * (m + off) + gs * b];
+                *t = c_add(*t, c_scale(acc[k + (size_t)nr * b], f));
+            }
+    }
+}
+
+static void spin_walk(int fwd, const orc_spin_rings* e, cplx* G, const cplx* almin, cplx* almout,
+                      int nthreads) {
+    int cw = 1;
+    for (int c = 0; c < e->nchunks; ++c) cw = (e->chi[c] - e->clo[c] + 1) > cw ? (e->chi[c] - e->clo[c] + 1) : cw;
+    int ns = nthreads_ok(nthreads);
+#ifdef _OPENMP
+#pragma omp parallel num_threads(ns > 0 ? ns : 1)
+#endif
+    {
+        int t = 0, nt = 1;
+#ifdef _OPENMP
+        t = omp_get_thread_num();
+        nt = omp_get_num_threads();
+#endif
+        double* d1 = (double*)malloc(sizeof(double) * cw);
+        double* d0 = (double*)malloc(sizeof(double) * cw);
+        cplx* acc = (cplx*)malloc(sizeof(cplx) * (size_t)cw * e->B);
+        /* orders are independent: each touches its own G column and coefficients */
+        for (int m = -e->L + t; m <= e->L; m += nt) {
+            int lo = e->jlo[m + e->L], hi = e->jhi[m + e->L];
+            if (hi < lo) continue;
+            for (int c = 0; c < e->nchunks; ++c) {
+                int r0 = e->clo[c] > lo ? e->clo[c] : lo;
+                int r1 = e->chi[c] < hi ? e->chi[c] : hi;
+                if (r1 < r0) continue;
+                spin_chunk(fwd, e, G, almin, almout, m, r0, r1, d1, d0, acc);
+            }
+        }
+        free(d1); free(d0); free(acc);
+    }
+}
+
+/* spin_rings_from_alm! / spin_alm_from_rings! (src/Spin.jl:319-341) */
+void orc_spin_rings_from_alm(const orc_spin_rings* e, const double* alm, double* G, int nthreads) {
+    memset(G, 0, sizeof(double) * 2 * (size_t)e->n * (2 * e->L + 1) * e->B);
+    spin_walk(1, e, (cplx*)G, (const cplx*)alm, NULL, nthreads);
+}
+
+void orc_spin_alm_from_rings(const orc_spin_rings* e, const double* G, double* alm, int nthreads) {
+    memset(alm, 0, sizeof(double) * 2 * (size_t)(e->L + 1) * (2 * e->L + 1) * e->B);
+    spin_walk(0, e, (cplx*)G, NULL, (cplx*)alm, nthreads);
+}
+
+/* SpinDirectLeaf (src/Spin.jl:557-630): sorted points, spin rings with eps = 0, phases */
+typedef struct { double t; int64_t i; } th_idx;
+static int cmp_th(const void* a, const void* b) {
+    const th_idx* x = (const th_idx*)a; const th_idx* y = (const th_idx*)b;
+    if (x->t < y->t) return -1;
+    if (x->t > y->t) return 1;
+    return x->i < y->i ? -1 : (x->i > y->i);
+}
+
+void orc_spin_direct(int fwd, const double* theta, const double* phi, int64_t M, int L, int spin,
+                     int ntrans, const double* in, double* out, int nthreads) {
+    th_idx* srt = (th_idx*)malloc(sizeof(th_idx) * M);
+    for (int64_t i = 0; i < M; ++i) { srt[i].t = theta[i]; srt[i].i = i; }
+    qsort(srt, M, sizeof(th_idx), cmp_th);
+    double* ths = (double*)malloc(sizeof(double) * M);
+    for (int64_t i = 0; i < M; ++i) ths[i] = srt[i].t;
+    orc_spin_rings* e = orc_spin_rings_create(ths, (int)M, L, spin, 0.0, ntrans, 0);
+    const int B = ntrans, off = L;
+    const size_t gs = (size_t)M * (2 * L + 1);
+    cplx* G = (cplx*)calloc(gs * B, sizeof(cplx));
+    if (fwd) {
+        orc_spin_rings_from_alm(e, in, (double*)G, nthreads);
+        cplx* f = (cplx*)out;
+        for (int b = 0; b < B; ++b)
+            for (int64_t i = 0; i < M; ++i) {
+                double ph0 = phi[srt[i].i];
+                cplx acc = G[i + (size_t)M * off + gs * b];
+                for (int m = 1; m <= L; ++m) {
+                    cplx ph = c_cis((double)m * ph0);
+                    acc = c_add(acc, c_add(c_mul(G[i + (size_t)M * (m + off) + gs * b], ph),
+                                           c_mul(G[i + (size_t)M * (off - m) + gs * b], c_conj(ph))));
+                }
+                f[srt[i].i + (size_t)M * b] = acc;
+            }
+    } else {
+        const cplx* f = (const cplx*)in;
+        for (int b = 0; b < B; ++b)
+            for (int64_t i = 0; i < M; ++i) {
+                cplx fi = f[srt[i].i + (size_t)M * b];
+                if (fi.re == 0 && fi.im == 0) continue;
+                double ph0 = phi[srt[i].i];
+                G[i + (size_t)M * off + gs * b] = fi;
+                for (int m = 1; m <= L; ++m) {
+                    cplx ph = c_cis((double)m * ph0);
+                    G[i + (size_t)M * (m + off) + gs * b] = c_mul(fi, c_conj(ph));
+                    G[i + (size_t)M * (off - m) + gs * b] = c_mul(fi, ph);
+                }
+            }
+        orc_spin_alm_from_rings(e, (const double*)G, out, nthreads);
+    }
+    orc_spin_rings_destroy(e);
+    free(G); free(ths); free(srt);
 }

@@ -123,6 +123,10 @@ typedef struct {
 orc_stretch* orc_stretch_create(const double* theta, const double* phi, int64_t M, int lmax,
                                 int ntrans, double tol, int nufft_kind, double eps_apo_max,
                                 double oversample_theta, double oversample_phi, int* status);
+orc_stretch* orc_stretch_create_spin(const double* theta, const double* phi, int64_t M, int lmax,
+                                     int ntrans, double tol, int nufft_kind, double eps_apo_max,
+                                     double oversample_theta, double oversample_phi, int spin,
+                                     int* status);
 void orc_stretch_destroy(orc_stretch*);
 void orc_stretch_info_get(const orc_stretch*, orc_stretch_info*);
 int orc_stretch_set_nufft_grid(orc_stretch*, int nf1, int nf2);  /* ES NUFFT leaves only */
@@ -132,6 +136,22 @@ void orc_stretch_forward(orc_stretch*, const double* alm, double* f, int nthread
 void orc_stretch_adjoint(orc_stretch*, const double* f, double* alm, int nthreads);
 /* the ring engine of the leaf (for stage-level parity) */
 const orc_rings* orc_stretch_rings_engine(const orc_stretch*);
+
+
+/* spin-weighted transforms (src/Spin.jl) */
+double orc_wigner_d(int l, int m, int n, double beta);
+typedef struct orc_spin_rings orc_spin_rings;
+orc_spin_rings* orc_spin_rings_create(const double* theta, int n, int lmax, int spin, double eps,
+                                      int ntrans, int reflect);
+void orc_spin_rings_destroy(orc_spin_rings*);
+int orc_spin_rings_mmax(const orc_spin_rings*);
+int orc_spin_rings_nchunks(const orc_spin_rings*);
+int64_t orc_spin_rings_work(const orc_spin_rings*);
+void orc_spin_rings_from_alm(const orc_spin_rings*, const double* alm, double* G, int nthreads);
+void orc_spin_alm_from_rings(const orc_spin_rings*, const double* G, double* alm, int nthreads);
+/* SpinDirectLeaf: fwd 1: alm -> f; fwd 0: f -> alm (spin layout (l+1, m+lmax+1)) */
+void orc_spin_direct(int fwd, const double* theta, const double* phi, int64_t M, int lmax, int spin,
+                     int ntrans, const double* in, double* out, int nthreads);
 
 #ifdef __cplusplus
 }

@@ -10,6 +10,8 @@ digits (the role of Julia's BigFloat) and writes them as JSON:
                    plus the outer-ring turning-point cases of test/test_legendre.jl:71-81
   direct_small.json  f_i = sum a_lm Y_lm(theta_i, phi_i) and the adjoint sum
                    conj(Y_lm) f_i for a small seeded case (test/test_transforms.jl:9-31)
+  wigner_d_kat.json  d^l_{mn}(beta) at the high-degree cases of test/test_spin.jl:23-33
+                   (python tests/golden/make_golden.py wigner)
 
 Run from the repository root:  python tests/golden/make_golden.py
 """
@@ -122,5 +124,53 @@ def main():
     print("wrote", os.path.join(HERE, "alf_kat.json"), os.path.join(HERE, "direct_small.json"))
 
 
+def wigner_d_mp(l, m, n, beta):
+    """d^l_{mn}(beta) at mpmath precision: the extremal closed form at l0 = max(|m|, |n|)
+    (src/Spin.jl:10-16, with d^j_{a,b} = (-1)^{a-b} d^j_{b,a} to move the extremal index
+    second) and the degree recurrence of src/Spin.jl:6-8, no scaling needed."""
+    if abs(m) > l or abs(n) > l:
+        return mp.mpf(0)
+    b = mp.mpf(beta)
+    c, s = mp.cos(b / 2), mp.sin(b / 2)
+    l0 = max(abs(m), abs(n))
+
+    def extremal(j, a, bb):
+        lb = mp.sqrt(mp.binomial(2 * j, j - a))
+        if bb == j:
+            return lb * c ** (j + a) * s ** (j - a)
+        return (-1) ** (j - a) * lb * c ** (j - a) * s ** (j + a)
+
+    if abs(n) == l0:
+        d1 = extremal(l0, m, l0 if n == l0 else -l0)
+    else:
+        d1 = extremal(l0, n, l0 if m == l0 else -l0) * (-1) ** ((n - m) % 2)
+    d0 = mp.mpf(0)
+    Lc = l0
+    cb = mp.cos(b)
+    if l0 == 0:
+        d0, d1, Lc = d1, d1 * cb, 1
+    while Lc < l:
+        L1 = Lc + 1
+        den = Lc * mp.sqrt(L1 * L1 - m * m) * mp.sqrt(L1 * L1 - n * n)
+        c1 = (2 * Lc + 1) * (Lc * L1 * cb - m * n) / den
+        c0 = L1 * mp.sqrt(max(0, Lc * Lc - m * m)) * mp.sqrt(max(0, Lc * Lc - n * n)) / den
+        d0, d1 = d1, c1 * d1 - c0 * d0
+        Lc = L1
+    return d1 if l > l0 or l0 == 0 else d1
+
+
+def wigner_kat():
+    """The high-degree Wigner-d cases of test/test_spin.jl:23-33."""
+    cases = [(512, 100, -2, 0.8), (2048, 700, -1, 0.5), (4096, 30, -2, 1.1), (1024, 0, 0, 2.0),
+             (300, 250, 3, 0.05), (64, -20, 5, 2.9)]
+    out = []
+    for l, m, n, b in cases:
+        out.append({"l": l, "m": m, "n": n, "beta": b, "d": mp.nstr(wigner_d_mp(l, m, n, b), 40)})
+    json.dump(out, open(os.path.join(HERE, "wigner_d_kat.json"), "w"), indent=1)
+
+
 if __name__ == "__main__":
+    if len(sys.argv) > 1 and sys.argv[1] == "wigner":
+        wigner_kat()
+        sys.exit(0)
     main()
