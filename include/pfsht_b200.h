@@ -80,7 +80,11 @@ typedef struct pfsht_opts {
                                    2 = nufft_nf1 x nufft_nf2 as given (each >= its minimum) */
     int32_t nufft_nf1, nufft_nf2;
     int32_t maxboxes;           /* MultiBox: at most this many boxes (src/Plan.jl:93; 0 = 8) */
-    int32_t reserved[3];
+    int32_t spin;               /* spin weight s, |s| <= lmax (src/Plan.jl:87,101-102): s != 0
+                                   transforms spin-s fields with coefficients sa_lm at
+                                   l + (lmax+1)(m+lmax) (src/Layout.jl:28-29), the ring pass in
+                                   FP64 whatever the precision mode; not in batches */
+    int32_t reserved[2];
 } pfsht_opts;
 
 typedef struct pfsht_plan pfsht_plan;
@@ -97,6 +101,8 @@ typedef struct pfsht_plan_info {
     int32_t nufft_w, nf1, nf2, row0, nrows, ncols;
     double nufft_beta;
     int64_t device_bytes; /* device memory the plan holds */
+    int32_t spin;         /* spin weight */
+    int32_t pad_;
 } pfsht_plan_info;
 
 /* Fill defaults (method AUTO, host points, current device, oversampling 1, eps_apo_max 1). */

@@ -163,17 +163,22 @@ class Plan:
     picked by timing the library FFT, the default), "minimal" (the smallest 2,3,5-smooth
     lengths, deterministic) or a pair (nf1, nf2) of lengths at or above the minimum;
     ``info["nf1"]``, ``info["nf2"]`` give the lengths in use.
+    ``spin`` (|spin| <= lmax) transforms spin-weighted fields, f = sum sa_lm sY_lm, with the
+    coefficient (l, m) at ``alm[l, m + lmax]`` (src/Layout.jl:28-29, ``spin_coeff_index``);
+    entries below l = max(|m|, |spin|) are ignored by the forward and zeroed by the adjoint.
     """
 
     def __init__(self, theta, phi, *, lmax, tol=1e-10, ntrans=1, method="auto",
                  precision="fp64", oversample_theta=1.0, oversample_phi=1.0, eps_apo_max=1.0,
                  device=None, rings_per_lane=0, bin_rows=0, bin_cols=0, segment_degrees=0,
-                 fft_lengths="timed", maxboxes=8):
+                 fft_lengths="timed", maxboxes=8, spin=0):
         self._h = None
         if len(theta) != len(phi):
             raise DimensionMismatch("θ and φ must have the same length")
         if lmax < 0:
             raise ValueError("lmax must be nonnegative")
+        if spin != 0 and abs(spin) > lmax:
+            raise ValueError(f"(|spin| = {abs(spin)}) > lmax = {lmax}")
         if ntrans < 1:
             raise ValueError("ntrans must be ≥ 1")
         if method not in _lib.METHODS:
@@ -192,6 +197,7 @@ class Plan:
         if maxboxes < 1:
             raise ValueError("maxboxes must be >= 1")
         o.maxboxes = int(maxboxes)
+        o.spin = int(spin)
         if isinstance(fft_lengths, (tuple, list)) and len(fft_lengths) == 2:
             o.nufft_fft_lengths = 2
             o.nufft_nf1, o.nufft_nf2 = int(fft_lengths[0]), int(fft_lengths[1])
@@ -228,6 +234,7 @@ class Plan:
         self.ntrans = int(ntrans)
         self.tol = float(tol)
         self.npts = len(theta)
+        self.spin = int(spin)
         self.precision = precision
         inf = _lib.PlanInfo()
         _lib.check(_lib.load().pfsht_plan_get_info(self._h, C.byref(inf)))
@@ -296,7 +303,7 @@ class Plan:
 
     def __repr__(self):
         return (f"PartialFSHT.Plan(lmax={self.lmax}, npts={self.npts}, ntrans={self.ntrans}, "
-                f"spin=0, algorithm={self.algorithm})")
+                f"spin={self.spin}, algorithm={self.algorithm})")
 
     @property
     def H(self) -> "AdjointPlan":
@@ -416,13 +423,15 @@ def dfs_fold(Ft, F, spin=0, stream=None):
 
 
 def plan_geometry(theta, phi, *, lmax, tol=1e-10, ntrans=1, method="auto",
-                  oversample_theta=1.0, oversample_phi=1.0, eps_apo_max=1.0, maxboxes=8) -> dict:
+                  oversample_theta=1.0, oversample_phi=1.0, eps_apo_max=1.0, maxboxes=8,
+                  spin=0) -> dict:
     """Host-only: the geometry and sizes pfsht_plan_create would choose (no device used)."""
     th = np.ascontiguousarray(theta, dtype=np.float64)
     ph = np.ascontiguousarray(phi, dtype=np.float64)
     o = _lib.default_opts()
     o.method = _lib.METHODS[method]
     o.maxboxes = int(maxboxes)
+    o.spin = int(spin)
     o.oversample_theta = float(oversample_theta)
     o.oversample_phi = float(oversample_phi)
     o.eps_apo_max = float(eps_apo_max)

@@ -25,7 +25,7 @@ class Opts(C.Structure):
                 ("oversample_phi", C.c_double), ("eps_apo_max", C.c_double),
                 ("ring_segment_degrees", C.c_int32), ("nufft_fft_lengths", C.c_int32),
                 ("nufft_nf1", C.c_int32), ("nufft_nf2", C.c_int32), ("maxboxes", C.c_int32),
-                ("reserved", C.c_int32 * 3)]
+                ("spin", C.c_int32), ("reserved", C.c_int32 * 2)]
 
 
 class Box(C.Structure):
@@ -45,7 +45,8 @@ class PlanInfo(C.Structure):
                 ("eps_apo", C.c_double), ("Theta1", C.c_double), ("sigma", C.c_double),
                 ("ThetaT", C.c_double), ("nufft_w", C.c_int32), ("nf1", C.c_int32),
                 ("nf2", C.c_int32), ("row0", C.c_int32), ("nrows", C.c_int32),
-                ("ncols", C.c_int32), ("nufft_beta", C.c_double), ("device_bytes", C.c_int64)]
+                ("ncols", C.c_int32), ("nufft_beta", C.c_double), ("device_bytes", C.c_int64),
+                ("spin", C.c_int32), ("pad_", C.c_int32)]
 
 
 _vp = C.c_void_p

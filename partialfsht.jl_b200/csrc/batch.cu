@@ -166,6 +166,9 @@ int batch_create(pfsht_plan* const* plans, int n, int nstreams, pfsht_batch** ou
         if (plans[i]->kind == kMultiBox)
             return fail(PFSHT_ERR_UNSUPPORTED, "a multi-box plan cannot join a batch; batch its boxes' "
                                                "geometries as plans of their own");
+        if (plans[i]->spin != 0)
+            return fail(PFSHT_ERR_UNSUPPORTED, "a spin plan cannot join a batch (the batched ring "
+                                               "pass is the scalar recurrence)");
     }
     const int dev = plans[0]->device;
     for (int i = 0; i < n; ++i) {

@@ -192,7 +192,7 @@ double jl_mod(double x, double y) {
 }
 
 int build_leaf(double lo, double hi, int L, int B, double tol, double eps_apo_max,
-               double ovs_th, double ovs_ph, Leaf* out, std::string* err) {
+               double ovs_th, double ovs_ph, Leaf* out, std::string* err, int spin) {
     const double tiny = std::sqrt(DBL_EPSILON);
     Geom g0, g;
     int r = try_geometry(lo, hi, L, tol, eps_apo_max, &g0);
@@ -251,7 +251,8 @@ int build_leaf(double lo, double hi, int L, int B, double tol, double eps_apo_ma
         double as = std::fabs(s);
         lf.cos_t[j] = csgn * c;
         lf.log2sin[j] = as > 0 ? std::log2(as) : -INFINITY;
-        lf.mlim[j] = polar_mmax(lf.theta_rings[j], L, tol);
+        // spin: never below |s|, where d^l_{m,-s} is not small (src/Spin.jl:222-225)
+        lf.mlim[j] = std::max(polar_mmax(lf.theta_rings[j], L, tol), std::abs(spin));
     }
     if (!nested_ranges(lf.mlim, L, lf.jlo, lf.jhi)) {
         *err = "retained-order limits are not unimodal in colatitude";
@@ -259,13 +260,24 @@ int build_leaf(double lo, double hi, int L, int B, double tol, double eps_apo_ma
     }
     sectorial_log2c(L, lf.log2c);
     lf.mmax = *std::max_element(lf.mlim.begin(), lf.mlim.end());
-    lf.nph = (int)next_smooth_even((int64_t)std::ceil((2.0 * lf.mmax + 1) * ovs_ph));
+    lf.spin = spin;
+    lf.nph = (int)next_smooth_even(
+        (int64_t)std::ceil((2.0 * std::max(lf.mmax, std::abs(spin)) + 1) * ovs_ph));
     lf.w.resize(n);
     for (int i = 0; i < n; ++i) lf.w[i] = window(g, lf.Theta_rings[i]);
     int64_t wk = 0;
-    for (int m = 0; m <= L; ++m) {
-        int nj = lf.jhi[m] - lf.jlo[m] + 1;
-        if (nj > 0) wk += (int64_t)nj * (L - m + 1);
+    if (spin == 0) {
+        for (int m = 0; m <= L; ++m) {
+            int nj = lf.jhi[m] - lf.jlo[m] + 1;
+            if (nj > 0) wk += (int64_t)nj * (L - m + 1);
+        }
+    } else {
+        // the spin walk: every order m = -L..L separately, from l0 = max(|m|, |s|)
+        for (int m = -L; m <= L; ++m) {
+            const int am = std::abs(m), l0 = std::max(am, std::abs(spin));
+            int nj = lf.jhi[am] - lf.jlo[am] + 1;
+            if (nj > 0 && l0 <= L) wk += (int64_t)nj * (L - l0 + 1);
+        }
     }
     lf.ring_work = wk;
     return 0;

@@ -43,12 +43,13 @@ struct Leaf {
     std::vector<double> theta_rings, Theta_rings, w, cos_t, log2sin, log2c;
     std::vector<int> mlim, jlo, jhi;
     int64_t ring_work = 0;
+    int spin = 0;
 };
 
 // 0 ok, 1 refused geometry, 2 bad arguments (message in err)
 int build_leaf(double box_lo, double box_hi, int lmax, int ntrans, double tol,
                double eps_apo_max, double ovs_theta, double ovs_phi, Leaf* out,
-               std::string* err);
+               std::string* err, int spin = 0);
 
 // ES kernel parameters of the NUFFT (published FINUFFT choice at upsampling 2)
 int es_width(double tol);

@@ -196,6 +196,39 @@ int ring_adjoint(const RingTables& t, const RingOut& o, const RingItems& it, con
                  double2* alm, int B, cudaStream_t s);
 
 // ---------------------------------------------------------------------------------------
+// spin-weighted ring pass (spin.cu): G[j, m] = sum_l sa_{lm} N_l d^l_{m,-s}(theta_j) for
+// m = -lmax..lmax and its transpose (src/Spin.jl:319-490); coefficients (l, m) at
+// l + (lmax + 1)(m + lmax) (src/Layout.jl:28-29)
+// ---------------------------------------------------------------------------------------
+struct SpinTables {
+    const double* cos_t = nullptr;    // nrings, reflection sign folded in
+    const double* log2cos = nullptr;  // nrings: log2 cos(t/2) (log2 sin(t/2) when reflected)
+    const double* log2sin = nullptr;  // nrings: log2 |sin(t/2)| (log2 cos(t/2) when reflected)
+    const double* lb2 = nullptr;      // 2 lmax + 1: seed log2 binomial per order (-inf: none)
+    const double* sg = nullptr;       // 2 lmax + 1: seed sign
+    const int* pc = nullptr;          // 2 lmax + 1: seed power of cos(t/2)
+    const int* ps = nullptr;          // 2 lmax + 1: seed power of sin(t/2)
+    const double* w = nullptr;        // nrings window, or null for 1
+    int lmax = 0, spin = 0, nrings = 0;
+};
+struct SpinTablesOwner {
+    DevBuf cos_t, log2cos, log2sin, lb2, sg, pc, ps;
+    SpinTables t;
+};
+// tables of a ring set (ring colatitudes theta_rings; reflect: the rings stand for pi - theta)
+int build_spin_tables(const std::vector<double>& theta_rings, bool reflect, int lmax, int spin,
+                      SpinTablesOwner& own, cudaStream_t s);
+// items over (m = -lmax..lmax, tiles of rings_per_tile retained rings), heaviest first; jlo/jhi
+// indexed by |m| (uploaded into own.jlo / own.jhi)
+int build_spin_items(const std::vector<int>& jlo, const std::vector<int>& jhi, int lmax, int spin,
+                     int rings_per_tile, RingItemsOwner& own, cudaStream_t s);
+int spin_ring_forward(const SpinTables& t, const RingOut& o, const RingItems& it,
+                      const double2* alm, double2* out, int B, cudaStream_t s);
+// overwrites alm (entries below l = max(|m|, |s|) zero)
+int spin_ring_adjoint(const SpinTables& t, const RingOut& o, const RingItems& it,
+                      const double2* in, double2* alm, int B, cudaStream_t s);
+
+// ---------------------------------------------------------------------------------------
 // per-stage CUDA-event timing of applies (diagnostics; off unless a profile is active)
 // ---------------------------------------------------------------------------------------
 enum Stage {

@@ -158,6 +158,7 @@ void fill_info(pfsht_plan* p) {
     in.precision = p->precision;
     in.npts = p->M;
     in.tol = p->tol;
+    in.spin = p->spin;
     if (p->kind == kMultiBox) {
         for (const auto& c : p->boxes) {
             in.ring_work += c->info.ring_work;
@@ -236,35 +237,43 @@ int build_stretch(pfsht_plan* p, const double* d_theta, const double* d_phi, con
     const int L = p->L, B = p->B;
     p->kind = lf.g.kind;
     p->nrings = lf.nth_half;
-    PF_TRY(upload(p->cos_t, lf.cos_t, s));
-    PF_TRY(upload(p->log2sin, lf.log2sin, s));
-    PF_TRY(upload(p->log2c, lf.log2c, s));
     PF_TRY(upload(p->w, lf.w, s));
-    const bool mix = p->precision == PFSHT_PRECISION_MIXED;
-    PF_TRY(build_ab_table(L, lf.mmax, mix ? 16 : 64, p->ab, p->aboff, s));
-    p->rt.mix = mix;
-    p->rt.stride = mix ? 16 : 64;
-    p->rt.cos_t = p->cos_t.as<double>();
-    p->rt.log2sin = p->log2sin.as<double>();
-    p->rt.log2c = p->log2c.as<double>();
-    p->rt.w = p->w.as<double>();
-    p->rt.ab = p->ab.as<double2>();
-    p->rt.aboff = p->aboff.as<int64_t>();
-    p->rt.lmax = L;
-    p->rt.nrings = lf.nth_half;
-    // forward tiles of 64 rings in the FP64 form (more warps) and of 128 in the mixed form
-    // (measured faster), adjoint tiles of 128 (amortises its reduction), split along the degree
-    // axis when the tiles alone leave the GPU under-filled
-    PF_TRY(build_ring_items(lf.jlo, lf.jhi, L, lf.mmax, p->R > 0 ? p->R : (mix ? 4 : 2),
-                            p->fwd_items, s));
-    PF_TRY(build_adjoint_items(p, lf.jlo, lf.jhi, lf.mmax, s));
+    if (p->spin != 0) {
+        // the Wigner-d ring pass (spin.cu) in FP64 whatever the precision mode; tiles of 64 rings
+        PF_TRY(build_spin_tables(lf.theta_rings, lf.flip, L, p->spin, p->spt, s));
+        p->spt.t.w = p->w.as<double>();
+        PF_TRY(build_spin_items(lf.jlo, lf.jhi, L, p->spin, 64, p->fwd_items, s));
+    } else {
+        PF_TRY(upload(p->cos_t, lf.cos_t, s));
+        PF_TRY(upload(p->log2sin, lf.log2sin, s));
+        PF_TRY(upload(p->log2c, lf.log2c, s));
+        const bool mix = p->precision == PFSHT_PRECISION_MIXED;
+        PF_TRY(build_ab_table(L, lf.mmax, mix ? 16 : 64, p->ab, p->aboff, s));
+        p->rt.mix = mix;
+        p->rt.stride = mix ? 16 : 64;
+        p->rt.cos_t = p->cos_t.as<double>();
+        p->rt.log2sin = p->log2sin.as<double>();
+        p->rt.log2c = p->log2c.as<double>();
+        p->rt.w = p->w.as<double>();
+        p->rt.ab = p->ab.as<double2>();
+        p->rt.aboff = p->aboff.as<int64_t>();
+        p->rt.lmax = L;
+        p->rt.nrings = lf.nth_half;
+        // forward tiles of 64 rings in the FP64 form (more warps) and of 128 in the mixed form
+        // (measured faster), adjoint tiles of 128 (amortises its reduction), split along the
+        // degree axis when the tiles alone leave the GPU under-filled
+        PF_TRY(build_ring_items(lf.jlo, lf.jhi, L, lf.mmax, p->R > 0 ? p->R : (mix ? 4 : 2),
+                                p->fwd_items, s));
+        PF_TRY(build_adjoint_items(p, lf.jlo, lf.jhi, lf.mmax, s));
+    }
     p->ncols = 2 * lf.mmax + 1;
     p->ro_cols.ld = lf.nth;
     p->ro_cols.bstride = (int64_t)lf.nth * p->ncols;
     p->ro_cols.col_off = lf.mmax;
     p->ro_cols.nrows = lf.nth;
     p->ro_cols.reflect = lf.g.kind == kInterior ? 0 : 1;
-    p->ro_cols.spin_sgn = 1.0;
+    // the DFS mirror rows carry (-1)^s (src/DFS.jl:13-33)
+    p->ro_cols.spin_sgn = (p->spin & 1) ? -1.0 : 1.0;
     p->ro_cols.nrings_out = lf.nth_half;
     p->ro_cols.zero_rest = 1;
     PF_TRY(p->H.alloc(sizeof(double2) * (size_t)lf.nth * p->ncols * B));
@@ -299,26 +308,32 @@ int build_stretch(pfsht_plan* p, const double* d_theta, const double* d_phi, con
     return 0;
 }
 
-int build_direct(pfsht_plan* p, const double* h_theta, const double* h_phi, cudaStream_t s) {
-    const int L = p->L, B = p->B;
+// the Direct leaf's ring set: every point a ring, every order on every point (eps = 0,
+// src/Direct.jl:262-263)
+int build_direct_rings(pfsht_plan* p, const double* h_theta, cudaStream_t s) {
+    const int L = p->L;
     const int64_t M = p->M;
-    if (M > INT32_MAX) return fail(PFSHT_ERR_ARGUMENT, "too many points for the direct method");
-    p->kind = kDirect;
-    p->nrings = (int)M;
-    std::vector<double> cs(M), l2s(M), ph(M);
+    std::vector<int> jlo(L + 1, 0), jhi(L + 1, (int)M - 1);
+    if (p->spin != 0) {
+        // SpinDirectLeaf (src/Spin.jl:557-630); the points keep their order (the walk needs no
+        // sorted rings)
+        std::vector<double> th(h_theta, h_theta + M);
+        PF_TRY(build_spin_tables(th, false, L, p->spin, p->spt, s));
+        p->spt.t.w = nullptr;
+        return build_spin_items(jlo, jhi, L, p->spin, 64, p->fwd_items, s);
+    }
+    std::vector<double> cs(M), l2s(M);
     for (int64_t i = 0; i < M; ++i) {
         const double sn = std::sin(h_theta[i]), c = std::cos(h_theta[i]);
         const double as = std::fabs(sn);
         cs[i] = c;
         l2s[i] = as > 0 ? std::log2(as) : -INFINITY;
-        ph[i] = h_phi[i];
     }
     std::vector<double> l2c;
     sectorial_log2c(L, l2c);
     PF_TRY(upload(p->cos_t, cs, s));
     PF_TRY(upload(p->log2sin, l2s, s));
     PF_TRY(upload(p->log2c, l2c, s));
-    PF_TRY(upload(p->phi_pts, ph, s));
     const bool mix = p->precision == PFSHT_PRECISION_MIXED;
     PF_TRY(build_ab_table(L, L, mix ? 16 : 64, p->ab, p->aboff, s));
     p->rt.mix = mix;
@@ -331,10 +346,18 @@ int build_direct(pfsht_plan* p, const double* h_theta, const double* h_phi, cuda
     p->rt.aboff = p->aboff.as<int64_t>();
     p->rt.lmax = L;
     p->rt.nrings = (int)M;
-    // eps = 0: every order on every point (src/Direct.jl:262-263)
-    std::vector<int> jlo(L + 1, 0), jhi(L + 1, (int)M - 1);
     PF_TRY(build_ring_items(jlo, jhi, L, L, p->R > 0 ? p->R : 2, p->fwd_items, s));
-    PF_TRY(build_adjoint_items(p, jlo, jhi, L, s));
+    return build_adjoint_items(p, jlo, jhi, L, s);
+}
+
+int build_direct(pfsht_plan* p, const double* h_theta, const double* h_phi, cudaStream_t s) {
+    const int L = p->L, B = p->B;
+    const int64_t M = p->M;
+    if (M > INT32_MAX) return fail(PFSHT_ERR_ARGUMENT, "too many points for the direct method");
+    p->kind = kDirect;
+    p->nrings = (int)M;
+    PF_TRY(build_direct_rings(p, h_theta, s));
+    PF_TRY(upload(p->phi_pts, std::vector<double>(h_phi, h_phi + M), s));
     p->ncols = 2 * L + 1;
     p->ro_cols.ld = M;
     p->ro_cols.bstride = M * (2 * L + 1);
@@ -515,6 +538,9 @@ int plan_create(const double* theta, const double* phi, int64_t npts, int lmax, 
     if (!(o.oversample_theta >= 1) || !(o.oversample_phi >= 1))
         return fail(PFSHT_ERR_ARGUMENT, "oversampling factors must be >= 1");
     if (!(o.eps_apo_max > 0)) return fail(PFSHT_ERR_ARGUMENT, "eps_apo_max must be positive");
+    if (o.spin != 0 && std::abs(o.spin) > lmax)
+        return fail(PFSHT_ERR_ARGUMENT, "(|spin| = " + std::to_string(std::abs(o.spin)) +
+                                            ") > lmax = " + std::to_string(lmax));
     if (o.nufft_fft_lengths < 0 || o.nufft_fft_lengths > 2)
         return fail(PFSHT_ERR_ARGUMENT, "nufft_fft_lengths must be 0 (timed), 1 (minimal) or 2 (given)");
     DeviceGuard dg(o.device);
@@ -534,6 +560,7 @@ int plan_create(const double* theta, const double* phi, int64_t npts, int lmax, 
     p->R = o.ring_rings_per_lane == 2 || o.ring_rings_per_lane == 4 || o.ring_rings_per_lane == 8
                ? o.ring_rings_per_lane : 0;
     p->seg_degrees = o.ring_segment_degrees;
+    p->spin = o.spin;
     PF_CUDA(cudaStreamCreateWithFlags(&p->st_stream, cudaStreamNonBlocking));
     cudaStream_t s = p->st_stream;
 
@@ -623,7 +650,7 @@ int plan_create(const double* theta, const double* phi, int64_t npts, int lmax, 
     if (!direct) {
         std::string err;
         int r = build_leaf(lo, hi, lmax, ntrans, tol, o.eps_apo_max, o.oversample_theta,
-                           o.oversample_phi, &p->leaf, &err);
+                           o.oversample_phi, &p->leaf, &err, o.spin);
         if (r == 2) return fail(PFSHT_ERR_ARGUMENT, err);
         if (r == 1) {
             if (o.method == PFSHT_METHOD_STRETCH) return fail(PFSHT_ERR_REFUSED, err);
@@ -645,7 +672,10 @@ int plan_create(const double* theta, const double* phi, int64_t npts, int lmax, 
 int apply_forward(pfsht_plan* p, const double2* alm, double2* f, cudaStream_t s) {
     if (p->kind == kMultiBox) return multibox_forward(p, alm, f, s);
     clock_begin(&p->clk, s);
-    PF_TRY(ring_forward(p->rt, p->ro_cols, p->fwd_items.view, alm, p->H.as<double2>(), p->B, s));
+    if (p->spin != 0)
+        PF_TRY(spin_ring_forward(p->spt.t, p->ro_cols, p->fwd_items.view, alm, p->H.as<double2>(), p->B, s));
+    else
+        PF_TRY(ring_forward(p->rt, p->ro_cols, p->fwd_items.view, alm, p->H.as<double2>(), p->B, s));
     if (p->kind != kDirect) clock_mark(&p->clk, kStRingFwd, s);
     return plan_forward_after_ring(p, f, s);
 }
@@ -654,7 +684,10 @@ int apply_adjoint(pfsht_plan* p, const double2* f, double2* alm, cudaStream_t s)
     if (p->kind == kMultiBox) return multibox_adjoint(p, f, alm, s);
     clock_begin(&p->clk, s);
     PF_TRY(plan_adjoint_before_ring(p, f, s));
-    PF_TRY(ring_adjoint(p->rt, p->ro_cols, p->adj_items.view, p->H.as<double2>(), alm, p->B, s));
+    if (p->spin != 0)
+        PF_TRY(spin_ring_adjoint(p->spt.t, p->ro_cols, p->fwd_items.view, p->H.as<double2>(), alm, p->B, s));
+    else
+        PF_TRY(ring_adjoint(p->rt, p->ro_cols, p->adj_items.view, p->H.as<double2>(), alm, p->B, s));
     clock_mark(&p->clk, p->kind == kDirect ? kStDirect : kStRingAdj, s);
     return 0;
 }
@@ -751,10 +784,13 @@ static std::vector<AlmBlock> alm_blocks(int L) {
     return v;
 }
 
-// bytes a host apply moves: the coefficient blocks and the field
+// bytes a host apply moves: the coefficient blocks (the whole array for a spin plan, whose
+// (l, m + lmax) layout has no staircase) and the field
 static void host_bytes(const pfsht_plan* p, int64_t* alm_bytes, int64_t* f_bytes) {
     int64_t a = 0;
-    for (const AlmBlock& b : alm_blocks(p->L)) a += (int64_t)b.rows * (b.c1 - b.c0);
+    if (p->spin != 0) a = (int64_t)(p->L + 1) * (2 * p->L + 1);
+    else
+        for (const AlmBlock& b : alm_blocks(p->L)) a += (int64_t)b.rows * (b.c1 - b.c0);
     *alm_bytes = a * (int64_t)sizeof(double2) * p->B;
     *f_bytes = (int64_t)sizeof(double2) * p->M * p->B;
 }
@@ -765,6 +801,11 @@ static int alm_copy(pfsht_plan* p, void* host, bool to_device, cudaStream_t s) {
     const size_t tr = col * (2 * L + 1);
     char* h = static_cast<char*>(host);
     char* d = p->st_alm.as<char>();
+    if (p->spin != 0) {
+        if (to_device) PF_CUDA(cudaMemcpyAsync(d, h, tr * p->B, cudaMemcpyHostToDevice, s));
+        else PF_CUDA(cudaMemcpyAsync(h, d, tr * p->B, cudaMemcpyDeviceToHost, s));
+        return 0;
+    }
     for (int b = 0; b < p->B; ++b) {
         for (const AlmBlock& k : alm_blocks(L)) {
             const size_t off = tr * b + col * k.c0;
@@ -783,6 +824,7 @@ static int alm_copy(pfsht_plan* p, void* host, bool to_device, cudaStream_t s) {
 // zero the padding rows of the host array that the block copies leave out (rows past each
 // block's height), on host threads while the copies run
 static void alm_zero_host_padding(const pfsht_plan* p, void* host) {
+    if (p->spin != 0) return;  // copied whole
     const int L = p->L;
     const std::vector<AlmBlock> blocks = alm_blocks(L);
     std::vector<int> rows(2 * L + 1);
@@ -881,6 +923,12 @@ pfsht_status pfsht_ring_forward(pfsht_plan* p, const void* alm, void* G, void* s
     const size_t bytes = sizeof(double2) * (size_t)o.bstride * p->B;
     cudaError_t e = cudaMemsetAsync(G, 0, bytes, s);
     if (e != cudaSuccess) return (pfsht_status)fail(PFSHT_ERR_CUDA, cudaGetErrorString(e));
+    if (p->spin != 0) {
+        SpinTables st = p->spt.t;
+        st.w = nullptr;
+        return (pfsht_status)spin_ring_forward(st, o, p->fwd_items.view, (const double2*)alm,
+                                               (double2*)G, p->B, s);
+    }
     return (pfsht_status)ring_forward(t, o, p->fwd_items.view,
                                       (const double2*)alm, (double2*)G, p->B, s);
 }
@@ -901,6 +949,12 @@ pfsht_status pfsht_ring_adjoint(pfsht_plan* p, const void* G, void* alm, void* s
     o.nrows = p->nrings;
     o.reflect = 0;
     o.nrings_out = p->nrings;
+    if (p->spin != 0) {
+        SpinTables st = p->spt.t;
+        st.w = nullptr;
+        return (pfsht_status)spin_ring_adjoint(st, o, p->fwd_items.view, (const double2*)G,
+                                               (double2*)alm, p->B, s);
+    }
     return (pfsht_status)ring_adjoint(t, o, p->adj_items.view,
                                       (const double2*)G, (double2*)alm, p->B, s);
 }
@@ -1089,6 +1143,8 @@ pfsht_status pfsht_plan_geometry(const double* theta, const double* phi, int64_t
     pfsht_opts o;
     pfsht_opts_default(&o);
     if (opts_in) o = *opts_in;
+    if (o.spin != 0 && std::abs(o.spin) > lmax)
+        return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "|spin| > lmax");
     double lo = INFINITY, hi = -INFINITY;
     for (int64_t i = 0; i < npts; ++i) {
         lo = std::fmin(lo, theta[i]);
@@ -1101,6 +1157,7 @@ pfsht_status pfsht_plan_geometry(const double* theta, const double* phi, int64_t
     info->ntrans = ntrans;
     info->npts = npts;
     info->tol = tol;
+    info->spin = o.spin;
     int method = o.method;
     Partition part;
     bool have_part = false;
@@ -1116,7 +1173,7 @@ pfsht_status pfsht_plan_geometry(const double* theta, const double* phi, int64_t
             Leaf lb;
             std::string eb;
             const int rb = build_leaf(b.lo, b.hi, lmax, ntrans, tol, o.eps_apo_max, o.oversample_theta,
-                                      o.oversample_phi, &lb, &eb);
+                                      o.oversample_phi, &lb, &eb, o.spin);
             if (rb == 2) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, eb);
             if (rb == 1) return (pfsht_status)fail(PFSHT_ERR_REFUSED, eb);
             info->ring_work += lb.ring_work;
@@ -1132,7 +1189,7 @@ pfsht_status pfsht_plan_geometry(const double* theta, const double* phi, int64_t
     Leaf lf;
     std::string err;
     int r = build_leaf(lo, hi, lmax, ntrans, tol, o.eps_apo_max, o.oversample_theta,
-                       o.oversample_phi, &lf, &err);
+                       o.oversample_phi, &lf, &err, o.spin);
     if (r == 2) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, err);
     if (r == 1) {
         if (o.method == PFSHT_METHOD_STRETCH) return (pfsht_status)fail(PFSHT_ERR_REFUSED, err);

@@ -28,6 +28,10 @@ struct pfsht_plan {
     RingSegments adj_seg;  // degree segments of the adjoint items
     int seg_degrees = 0;   // requested segment length (0 = auto, < 0 = none)
     RingTables rt;
+    // spin weight s (src/Spin.jl): s != 0 runs the Wigner-d ring pass on spt with the items in
+    // fwd_items for both directions; coefficients in the (l, m + lmax) layout
+    int spin = 0;
+    SpinTablesOwner spt;
     RingOut ro_cols;  // the apply's column array H (or G for the direct leaf)
     // column array: nth x ncols x B (stretch) or M x (2L+1) x B (direct)
     DevBuf H;
