@@ -537,6 +537,80 @@ def run_solve(args, world, rank, local):
     return 0
 
 
+def rand_spin_alm_host(lmax, spin, rng):
+    """Spin coefficients (l, m + lmax) as complex N(0,1)/(l+1) where l >= max(|m|, |s|)."""
+    L = lmax
+    l = np.arange(L + 1)[:, None]
+    m = np.arange(-L, L + 1)[None, :]
+    mask = (np.abs(m) <= l) & (l >= abs(spin))
+    a = (rng.standard_normal((L + 1, 2 * L + 1)) + 1j * rng.standard_normal((L + 1, 2 * L + 1)))
+    return np.asfortranarray(a / np.sqrt(2) / (l + 1) * mask)
+
+
+def run_spin(args, world, rank, local):
+    """--config spin: the spin-s stretched leaf (src/Spin.jl, s = --spin) at the headline
+    workload: ms per fwd+adj, stage times, ns per retained (l, m, ring) triple, accuracy against
+    the spin Direct leaf on a subsample and the dot test; the CPU restatement of the spin apply
+    timed beside it."""
+    import torch
+    from __graft_entry__ import load_package
+    pf = load_package()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    s = args.spin
+    M, theta, phi, rng = workload(args.lmax)
+    plan = pf.Plan(theta, phi, lmax=args.lmax, tol=args.tol, device=local, spin=s,
+                   fft_lengths=fft_lengths_arg(args.fft_lengths))
+    info = plan.info
+    alms = [torch.from_numpy(np.ascontiguousarray(rand_spin_alm_host(args.lmax, s, rng).T)).to(dev).T
+            for _ in range(3)]
+    fins = [torch.from_numpy((rng.standard_normal(M) + 1j * rng.standard_normal(M)) / np.sqrt(2)).to(dev)
+            for _ in range(3)]
+    fout = pf.zeros_field(M, device=dev)
+    aout = pf.zeros_alm(args.lmax, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    n0 = pf._lib.load().pfsht_launch_count()
+    T, stages = time_applies(pf, plan, alms, fins, fout, aout, args.steps, args.warmup, stream)
+    launches = (pf._lib.load().pfsht_launch_count() - n0) * args.steps // (args.steps + args.warmup)
+    ms = T / args.steps
+    # accuracy: the spin Direct leaf (FP64, every order on every point) on a seeded subsample
+    sub = np.sort(np.random.default_rng(7).choice(M, 4096, replace=False))
+    pd = pf.Plan(theta[sub], phi[sub], lmax=args.lmax, tol=args.tol, method="direct", spin=s,
+                 device=local)
+    f = plan * alms[0]
+    fd = pd * alms[0]
+    fs = f[torch.from_numpy(sub).to(dev)]
+    err = float(torch.linalg.vector_norm(fs - fd) / torch.linalg.vector_norm(fd))
+    a = plan.H * fins[0]
+    lhs = torch.vdot(f, fins[0]).item()
+    rhs = torch.vdot(alms[0].T.reshape(-1), a.T.reshape(-1)).item()
+    dot = abs(lhs - rhs) / abs(lhs)
+    cpu = None
+    if not args.no_cpu:
+        from oracle import oracle as O
+        nthreads = os.cpu_count() or 1
+        S = O.Stretch(theta, phi, args.lmax, args.tol, nufft="es", spin=s)
+        ah = rand_spin_alm_host(args.lmax, s, rng)[:, :, None]
+        g = np.asfortranarray(fins[0].cpu().numpy()[:, None])
+        t0 = time.perf_counter()
+        S.forward(ah, nthreads=nthreads)
+        S.adjoint(g, nthreads=nthreads)
+        cpu = {"value": (time.perf_counter() - t0) * 1e3, "unit": "ms", "cores": nthreads,
+               "kind": "port", "sample": "full workload, one spin fwd+adj of the C restatement"}
+    line = {"metric": f"ms per spin-{s} fwd+adj apply", "value": ms, "unit": "ms", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": False, "dtype": "f64", "data": "synthetic",
+            "config": dict(config_dict(args, M), spin=s,
+                           alm="complex N(0,1)/(l+1) where l >= max(|m|, |s|), (l, m + lmax) layout"),
+            "ring_work": info["ring_work"], "ns_per_triple": ms * 1e6 / info["ring_work"],
+            "stages_ms": {k: round(v[0] / v[1], 4) for k, v in stages.items()},
+            "accuracy": {"tol": args.tol, "l2_rel_vs_spin_direct": err, "dot_rel": dot,
+                         "sample": "4096 seeded points, spin Direct leaf on the device"},
+            "cpu_baseline": cpu, "gpu_launches": launches}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_b200(args, world, rank, local):
     import ctypes as C
 
@@ -732,9 +806,12 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-form measurement")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving measurement")
-    ap.add_argument("--config", default="headline", choices=["headline", "batch", "serve", "solve"],
+    ap.add_argument("--config", default="headline",
+                    choices=["headline", "batch", "serve", "solve", "spin"],
                     help="headline (default): the lmax 2048 cap; batch: 64 plans in one graph; "
-                         "serve: the request loop; solve: CG iterations of solve!")
+                         "serve: the request loop; solve: CG iterations of solve!; spin: the "
+                         "spin-s leaf on the headline workload")
+    ap.add_argument("--spin", type=int, default=2, help="spin weight of --config spin")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
@@ -749,6 +826,8 @@ def main():
             return run_serve(args, world, rank, local) if rank == 0 else 0
         if args.config == "solve":
             return run_solve(args, world, rank, local) if rank == 0 else 0
+        if args.config == "spin":
+            return run_spin(args, world, rank, local) if rank == 0 else 0
         return run_b200(args, world, rank, local)
     finally:
         if world > 1:
