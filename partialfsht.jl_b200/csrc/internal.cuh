@@ -209,10 +209,11 @@ struct SpinTables {
     const int* pc = nullptr;          // 2 lmax + 1: seed power of cos(t/2)
     const int* ps = nullptr;          // 2 lmax + 1: seed power of sin(t/2)
     const double* w = nullptr;        // nrings window, or null for 1
+    const double4* lt = nullptr;      // lmax + 1: (1/sqrt(l^2 - s^2), sqrt(l^2 - s^2), 1/l, N_l)
     int lmax = 0, spin = 0, nrings = 0;
 };
 struct SpinTablesOwner {
-    DevBuf cos_t, log2cos, log2sin, lb2, sg, pc, ps;
+    DevBuf cos_t, log2cos, log2sin, lb2, sg, pc, ps, lt;
     SpinTables t;
 };
 // tables of a ring set (ring colatitudes theta_rings; reflect: the rings stand for pi - theta)

@@ -239,10 +239,10 @@ int build_stretch(pfsht_plan* p, const double* d_theta, const double* d_phi, con
     p->nrings = lf.nth_half;
     PF_TRY(upload(p->w, lf.w, s));
     if (p->spin != 0) {
-        // the Wigner-d ring pass (spin.cu) in FP64 whatever the precision mode; tiles of 64 rings
+        // the Wigner-d ring pass (spin.cu) in FP64 whatever the precision mode; tiles of 128 rings
         PF_TRY(build_spin_tables(lf.theta_rings, lf.flip, L, p->spin, p->spt, s));
         p->spt.t.w = p->w.as<double>();
-        PF_TRY(build_spin_items(lf.jlo, lf.jhi, L, p->spin, 64, p->fwd_items, s));
+        PF_TRY(build_spin_items(lf.jlo, lf.jhi, L, p->spin, 128, p->fwd_items, s));
     } else {
         PF_TRY(upload(p->cos_t, lf.cos_t, s));
         PF_TRY(upload(p->log2sin, lf.log2sin, s));
@@ -320,7 +320,7 @@ int build_direct_rings(pfsht_plan* p, const double* h_theta, cudaStream_t s) {
         std::vector<double> th(h_theta, h_theta + M);
         PF_TRY(build_spin_tables(th, false, L, p->spin, p->spt, s));
         p->spt.t.w = nullptr;
-        return build_spin_items(jlo, jhi, L, p->spin, 64, p->fwd_items, s);
+        return build_spin_items(jlo, jhi, L, p->spin, 128, p->fwd_items, s);
     }
     std::vector<double> cs(M), l2s(M);
     for (int64_t i = 0; i < M; ++i) {

@@ -6,11 +6,15 @@
 // seeded at l0 = max(|m|, |s|) from the extremal closed form, sg 2^(lb2 + pc log2 cos(t/2) +
 // ps log2 sin(t/2)), with the log-binomial, exponents and sign tabulated per order and the two
 // logarithms per ring (src/Spin.jl:190-245), and carries its own power-of-two exponent (the
-// reference shares one per ring chunk; a per-ring exponent is at least as accurate). The
-// recurrence d_{l+1} = (a1 cos t - a2) d_l - a0 d_{l-1} (src/Spin.jl:6-8) costs three FP64
-// operations per (ring, degree); its coefficients for the next 32 degrees are computed one per
-// lane and staged in shared memory, with N_l and the coefficient (forward). Every 64 degrees the
-// state is renormalised by a power of two read from its exponent field (exact).
+// reference shares one per ring chunk; power-of-two scalings are exact, so both give the same
+// values to rounding). The recurrence d_{l+1} = (a1 cos t - a2) d_l - a0 d_{l-1}
+// (src/Spin.jl:6-8) costs three FP64 operations per (ring, degree). Its coefficients for the next
+// 32 degrees are computed one degree per lane and staged in shared memory:
+//     a1 = (2l-1) l / (sm sn),  a2 = (2l-1) m n / ((l-1) sm sn),  a0 = l sm' sn' / ((l-1) sm sn),
+// sm = sqrt(l^2 - m^2), sn = sqrt(l^2 - n^2) and the primed values at l - 1 (the reference's
+// expressions with den = (l-1) sm sn divided through), from one reciprocal square root and one
+// square root per lane and a per-degree table of 1/sn, sn, 1/l and N_l. Every 32 degrees the
+// state is renormalised by a power of two read from its exponent field.
 // Forward: each ring accumulates N_l a_{lm} d_l and writes G (windowed, mirrored into the DFS
 // rows with sign (-1)^(m+s), zeros for the rings the order does not retain).
 // Adjoint: each ring scales its G value by its window and 2^E once per exponent change; per
@@ -29,8 +33,7 @@ namespace pf {
 namespace {
 
 constexpr int kSpinWarps = 4;     // forward: warps per block
-constexpr int kSpinAdjWarps = 2;  // adjoint: warps per block (17 KB of shared memory each)
-constexpr int kSpinStride = 64;  // renormalisation stride (src/Legendre.jl:16)
+constexpr int kSpinAdjWarps = 2;  // adjoint: warps per block (18 KB of shared memory each)
 
 struct SpinCoef {
     double a1, a2, a0, N;
@@ -42,26 +45,26 @@ __device__ __forceinline__ int spin_renorm_shift(double q1, double q2) {
     return (e == 0 || e == 0x7ff) ? 0 : e - 1022;
 }
 
-// recurrence coefficients taking d_{L1 - 1}, d_{L1 - 2} to d_{L1} (src/Spin.jl:404-416)
-__device__ __forceinline__ SpinCoef spin_coef(int L1, int m, int n) {
+// recurrence coefficients taking d_{L1 - 1}, d_{L1 - 2} to d_{L1} (src/Spin.jl:404-416); L1 > l0,
+// so L1^2 - m^2 > 0 and L1 - 1 >= 1
+__device__ __forceinline__ SpinCoef spin_coef(const double4* __restrict__ lt, int L1, int m, int n) {
     const int Lc = L1 - 1;
-    const double sm1 = sqrt(fmax(0.0, (double)L1 * L1 - (double)m * m));
-    const double sn1 = sqrt(fmax(0.0, (double)L1 * L1 - (double)n * n));
-    const double den = (double)Lc * sm1 * sn1;
-    const double sm0 = sqrt(fmax(0.0, (double)Lc * Lc - (double)m * m));
-    const double sn0 = sqrt(fmax(0.0, (double)Lc * Lc - (double)n * n));
-    SpinCoef c;
-    c.a1 = (double)(2 * Lc + 1) * (double)Lc * (double)L1 / den;
-    c.a2 = (double)(2 * Lc + 1) * (double)m * (double)n / den;
-    c.a0 = (double)L1 * sm0 * sn0 / den;
-    c.N = sqrt((2.0 * L1 + 1) / (4 * M_PI));
-    return c;
+    const double4 t1 = lt[L1], t0 = lt[Lc];  // (1/sn, sn, 1/l, N_l)
+    const double q = rsqrt((double)L1 * L1 - (double)m * m) * t1.x;  // 1 / (sm1 sn1)
+    const double sm0 = sqrt((double)Lc * Lc - (double)m * m);
+    const double c = (double)(2 * Lc + 1);
+    SpinCoef k;
+    k.a1 = c * (double)L1 * q;
+    k.a2 = c * ((double)m * (double)n) * t0.z * q;
+    k.a0 = (double)L1 * sm0 * t0.y * t0.z * q;
+    k.N = t1.w;
+    return k;
 }
 
 __device__ __forceinline__ size_t sidx(int l, int m, int L) { return (size_t)l + (size_t)(L + 1) * (m + L); }
 
 struct SpinFwdSmem {
-    SpinCoef c[32];
+    double a1[32], a2[32], a0[32];
     double2 a[32];  // N_l a_{lm}
 };
 
@@ -104,7 +107,7 @@ __device__ void spin_fwd_item(const SpinTables& t, const RingOut& o, const RingI
         }
     }
     {
-        const double N0 = sqrt((2.0 * l0 + 1) / (4 * M_PI));
+        const double N0 = t.lt[l0].w;
         const double2 a = ab[sidx(l0, m, L)];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
@@ -112,42 +115,47 @@ __device__ void spin_fwd_item(const SpinTables& t, const RingOut& o, const RingI
             acc[r].y = a.y * N0 * d1[r];
         }
     }
-    int steps = 0;
+    auto step = [&](int i) {
+        const double a1 = sm.a1[i], a2 = sm.a2[i], a0 = sm.a0[i];
+        const double2 a = sm.a[i];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const double dn = fma(fma(a1, x[r], -a2), d1[r], -(a0 * d0[r]));
+            d0[r] = d1[r];
+            d1[r] = dn;
+            acc[r].x = fma(a.x, dn, acc[r].x);
+            acc[r].y = fma(a.y, dn, acc[r].y);
+        }
+    };
     for (int lb = l0 + 1; lb <= L; lb += 32) {
         const int nl = min(32, L - lb + 1);
         __syncwarp();
         if (lane < nl) {
-            const SpinCoef c = spin_coef(lb + lane, m, n);
-            sm.c[lane] = c;
+            const SpinCoef c = spin_coef(t.lt, lb + lane, m, n);
+            sm.a1[lane] = c.a1;
+            sm.a2[lane] = c.a2;
+            sm.a0[lane] = c.a0;
             const double2 a = ab[sidx(lb + lane, m, L)];
             sm.a[lane] = make_double2(a.x * c.N, a.y * c.N);
         }
         __syncwarp();
-        for (int i = 0; i < nl; ++i) {
-            const SpinCoef c = sm.c[i];
-            const double2 a = sm.a[i];
+        if (nl == 32) {
+#pragma unroll 8
+            for (int i = 0; i < 32; ++i) step(i);
+        } else {
+            for (int i = 0; i < nl; ++i) step(i);
+        }
+        // renormalise every 32 degrees (exact powers of two)
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const double dn = fma(fma(c.a1, x[r], -c.a2), d1[r], -(c.a0 * d0[r]));
-                d0[r] = d1[r];
-                d1[r] = dn;
-                acc[r].x = fma(a.x, dn, acc[r].x);
-                acc[r].y = fma(a.y, dn, acc[r].y);
-            }
-            if (++steps == kSpinStride) {
-                steps = 0;
-#pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    const int sh = spin_renorm_shift(d1[r], d0[r]);
-                    if (sh != 0) {
-                        const double f = scalbn(1.0, -sh);
-                        d1[r] *= f;
-                        d0[r] *= f;
-                        acc[r].x *= f;
-                        acc[r].y *= f;
-                        E[r] += sh;
-                    }
-                }
+        for (int r = 0; r < R; ++r) {
+            const int sh = spin_renorm_shift(d1[r], d0[r]);
+            if (sh != 0) {
+                const double f = scalbn(1.0, -sh);
+                d1[r] *= f;
+                d0[r] *= f;
+                acc[r].x *= f;
+                acc[r].y *= f;
+                E[r] += sh;
             }
         }
     }
@@ -187,7 +195,8 @@ spin_fwd_kernel(SpinTables t, RingOut o, const RingItem* __restrict__ items, int
             }
         }
         const int reff = (item.n + 31) >> 5;
-        if (reff >= 2) spin_fwd_item<2>(t, o, item, alm, out, b, sm[warp], lane);
+        if (reff >= 3) spin_fwd_item<4>(t, o, item, alm, out, b, sm[warp], lane);
+        else if (reff == 2) spin_fwd_item<2>(t, o, item, alm, out, b, sm[warp], lane);
         else spin_fwd_item<1>(t, o, item, alm, out, b, sm[warp], lane);
     }
 }
@@ -245,61 +254,66 @@ __device__ void spin_adj_item(const SpinTables& t, const RingOut& o, const RingI
             p.y += __shfl_xor_sync(0xffffffffu, p.y, off);
         }
         if (lane == 0) {
-            const double N0 = sqrt((2.0 * l0 + 1) / (4 * M_PI));
+            const double N0 = t.lt[l0].w;
             atomicAdd(ad + 2 * sidx(l0, m, L), p.x * N0);
             atomicAdd(ad + 2 * sidx(l0, m, L) + 1, p.y * N0);
         }
     }
-    int steps = 0;
+    auto step = [&](int i) {
+        const SpinCoef c = sm.c[i];
+        double2 p = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const double dn = fma(fma(c.a1, x[r], -c.a2), d1[r], -(c.a0 * d0[r]));
+            d0[r] = d1[r];
+            d1[r] = dn;
+            p.x = fma(dn, gs[r].x, p.x);
+            p.y = fma(dn, gs[r].y, p.y);
+        }
+        sm.red[i][lane] = p;
+    };
     for (int lb = l0 + 1; lb <= L; lb += 32) {
         const int nl = min(32, L - lb + 1);
         __syncwarp();
-        if (lane < nl) sm.c[lane] = spin_coef(lb + lane, m, n);
+        if (lane < nl) sm.c[lane] = spin_coef(t.lt, lb + lane, m, n);
         __syncwarp();
-        for (int i = 0; i < nl; ++i) {
-            const SpinCoef c = sm.c[i];
-            double2 p = make_double2(0.0, 0.0);
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const double dn = fma(fma(c.a1, x[r], -c.a2), d1[r], -(c.a0 * d0[r]));
-                d0[r] = d1[r];
-                d1[r] = dn;
-                p.x = fma(dn, gs[r].x, p.x);
-                p.y = fma(dn, gs[r].y, p.y);
-            }
-            sm.red[i][lane] = p;
-            if (++steps == kSpinStride) {
-                steps = 0;
-#pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    const int sh = spin_renorm_shift(d1[r], d0[r]);
-                    if (sh != 0) {
-                        const double f = scalbn(1.0, -sh);
-                        d1[r] *= f;
-                        d0[r] *= f;
-                        E[r] += sh;
-                        gs[r] = make_double2(scalbn(g[r].x, E[r]), scalbn(g[r].y, E[r]));
-                    }
-                }
-            }
+        if (nl == 32) {
+#pragma unroll 8
+            for (int i = 0; i < 32; ++i) step(i);
+        } else {
+            for (int i = 0; i < nl; ++i) step(i);
         }
         __syncwarp();
         if (lane < nl) {
-            double sx = 0.0, sy = 0.0;
+            double sx0 = 0.0, sy0 = 0.0, sx1 = 0.0, sy1 = 0.0;
 #pragma unroll 8
-            for (int q = 0; q < 32; ++q) {
-                const double2 v = sm.red[lane][q];
-                sx += v.x;
-                sy += v.y;
+            for (int q = 0; q < 32; q += 2) {
+                const double2 v0 = sm.red[lane][q], v1 = sm.red[lane][q + 1];
+                sx0 += v0.x;
+                sy0 += v0.y;
+                sx1 += v1.x;
+                sy1 += v1.y;
             }
             const double N = sm.c[lane].N;
             const size_t e = 2 * sidx(lb + lane, m, L);
             if (item.flags & kItemSole) {
-                ad[e] = sx * N;
-                ad[e + 1] = sy * N;
+                ad[e] = (sx0 + sx1) * N;
+                ad[e + 1] = (sy0 + sy1) * N;
             } else {
-                atomicAdd(ad + e, sx * N);
-                atomicAdd(ad + e + 1, sy * N);
+                atomicAdd(ad + e, (sx0 + sx1) * N);
+                atomicAdd(ad + e + 1, (sy0 + sy1) * N);
+            }
+        }
+        // renormalise every 32 degrees (exact powers of two); the scaled ring values follow E
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int sh = spin_renorm_shift(d1[r], d0[r]);
+            if (sh != 0) {
+                const double f = scalbn(1.0, -sh);
+                d1[r] *= f;
+                d0[r] *= f;
+                E[r] += sh;
+                gs[r] = make_double2(scalbn(g[r].x, E[r]), scalbn(g[r].y, E[r]));
             }
         }
     }
@@ -315,7 +329,8 @@ spin_adj_kernel(SpinTables t, RingOut o, const RingItem* __restrict__ items, int
     const RingItem item = items[it];
     for (int b = 0; b < B; ++b) {
         const int reff = (item.n + 31) >> 5;
-        if (reff >= 2) spin_adj_item<2>(t, o, item, in, almd, b, sm[warp], lane);
+        if (reff >= 3) spin_adj_item<4>(t, o, item, in, almd, b, sm[warp], lane);
+        else if (reff == 2) spin_adj_item<2>(t, o, item, in, almd, b, sm[warp], lane);
         else spin_adj_item<1>(t, o, item, in, almd, b, sm[warp], lane);
     }
 }
@@ -446,6 +461,14 @@ int build_spin_tables(const std::vector<double>& theta_rings, bool reflect, int 
     PF_TRY(up(own.sg, sg.data(), sizeof(double) * nm));
     PF_TRY(up(own.pc, pc.data(), sizeof(int) * nm));
     PF_TRY(up(own.ps, ps.data(), sizeof(int) * nm));
+    // per degree (1/sqrt(l^2 - n^2), sqrt(l^2 - n^2), 1/l, N_l); the first two only for l > |n|
+    std::vector<double4> lt(L + 1);
+    for (int l = 0; l <= L; ++l) {
+        const double q = (double)l * l - (double)nn * nn;
+        lt[l] = make_double4(q > 0 ? 1.0 / std::sqrt(q) : 0.0, q > 0 ? std::sqrt(q) : 0.0,
+                             l > 0 ? 1.0 / l : 0.0, std::sqrt((2.0 * l + 1) / (4 * M_PI)));
+    }
+    PF_TRY(up(own.lt, lt.data(), sizeof(double4) * (L + 1)));
     PF_CUDA(cudaStreamSynchronize(s));
     own.t.cos_t = own.cos_t.as<double>();
     own.t.log2cos = own.log2cos.as<double>();
@@ -454,6 +477,7 @@ int build_spin_tables(const std::vector<double>& theta_rings, bool reflect, int 
     own.t.sg = own.sg.as<double>();
     own.t.pc = own.pc.as<int>();
     own.t.ps = own.ps.as<int>();
+    own.t.lt = own.lt.as<double4>();
     own.t.lmax = L;
     own.t.spin = spin;
     own.t.nrings = n;
