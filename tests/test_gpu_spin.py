@@ -157,3 +157,33 @@ def test_spin_rejections(pf, O, cuda):
     p0 = pf.Plan(th, ph, lmax=128, tol=1e-8, method="stretch", spin=0)
     assert p0.info["spin"] == 0 and p.info["spin"] == 1
     assert "spin=1" in repr(p)
+
+
+@pytest.mark.parametrize("method", ["stretch", "direct"])
+def test_spin_ntrans_columns_and_serving(pf, O, cuda, method):
+    # ntrans = 3: each column is the single-transform plan's result (src/Plan.jl:137-148 on
+    # (lmax+1, 2lmax+1, ntrans) arrays); a spin plan also runs in the serving loop
+    rng = np.random.default_rng(130)
+    L, s, B = 160, -2, 3
+    th, ph = cap_points(1500 if method == "stretch" else 300, rng=rng)
+    M = len(th)
+    p3 = pf.Plan(th, ph, lmax=L, tol=1e-8, method=method, spin=s, ntrans=B)
+    p1 = pf.Plan(th, ph, lmax=L, tol=1e-8, method=method, spin=s)
+    alm = O.rand_spin_alm(L, s, ntrans=B, rng=rng)
+    g = np.asfortranarray(cn(rng, M, B))
+    f3 = _fwd(p3, alm)
+    a3 = _adj(p3, g)
+    for b in range(B):
+        assert rel(f3[:, b], _fwd(p1, alm[:, :, b])) < 1e-13
+        assert _spin_rel(O, a3[:, :, b], _adj(p1, np.ascontiguousarray(g[:, b])), L, s) < 1e-13
+        assert dot_rel(f3[:, b], g[:, b], alm[:, :, b], a3[:, :, b]) < 1e-12
+    srv = pf.Server(hbm_budget_gb=4, nslots=2)
+    pid = srv.add(p1)
+    ah = pf.zeros_alm(L, device="pinned")
+    ah[...] = alm[:, :, 0]
+    out = pf.zeros_field(M, device="pinned")
+    srv.wait(srv.submit(pid, True, ah, out))
+    ref = pf.zeros_field(M, device="pinned")
+    p1.mul(ref, ah)
+    assert np.array_equal(out, ref)
+    srv.close()
