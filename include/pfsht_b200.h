@@ -83,7 +83,7 @@ typedef struct pfsht_opts {
     int32_t spin;               /* spin weight s, |s| <= lmax (src/Plan.jl:87,101-102): s != 0
                                    transforms spin-s fields with coefficients sa_lm at
                                    l + (lmax+1)(m+lmax) (src/Layout.jl:28-29), the ring pass in
-                                   FP64 whatever the precision mode; not in batches */
+                                   FP64 whatever the precision mode */
     int32_t reserved[2];
 } pfsht_opts;
 

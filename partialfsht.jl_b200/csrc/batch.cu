@@ -3,13 +3,14 @@
 //
 // One direction of a batch is one CUDA graph, captured on first use and replayed with a single
 // cudaGraphLaunch:
-//   forward : pointer table -> ring passes of all plans (one launch per kernel shape, items of
-//             all plans heaviest first) -> per plan, on one of several streams: FFT along Theta
-//             and NUFFT type 2 into the plan's own field buffer -> one copy kernel into the
-//             callers' fields
+//   forward : pointer table -> ring passes of all scalar plans (one launch per kernel shape,
+//             items of all plans heaviest first) -> per plan, on one of several streams: the
+//             spin ring pass of a spin plan, FFT along Theta and NUFFT type 2 into the plan's
+//             own field buffer -> one copy kernel into the callers' fields
 //   adjoint : pointer table -> one copy kernel from the callers' fields -> per plan on the
 //             streams: NUFFT type 1, inverse FFT along Theta, zeroing of the caller's
-//             coefficient array -> ring passes of all plans
+//             coefficient array (and a spin plan's own ring pass) -> ring passes of all scalar
+//             plans
 // Callers' arrays are reached through a device pointer table that the graph's first node
 // copies from pinned host memory, so new arrays on each call need no new capture.
 #include <cuda_runtime.h>
@@ -103,7 +104,15 @@ int record(pfsht_batch* b, bool fwd) {
         pfsht_plan* p = b->plans[i];
         cudaStream_t s = b->side[i % b->side.size()];
         if (fwd) {
+            if (p->spin)
+                PF_TRY(spin_ring_forward_ptr(p->spt.t, p->ro_cols, p->fwd_items.view, ptrs, i,
+                                             p->H.as<double2>(), p->B, s));
             PF_TRY(plan_forward_after_ring(p, p->st_f.as<double2>(), s));
+        } else if (p->spin) {
+            PF_TRY(plan_adjoint_before_ring(p, p->st_f.as<double2>(), s));
+            PF_TRY(alm_prepare_ptr(ptrs, i, p->L, p->B, nullptr, 0, s));
+            PF_TRY(spin_ring_adjoint_ptr(p->spt.t, p->ro_cols, p->fwd_items.view, p->H.as<double2>(),
+                                         ptrs, i, p->B, s));
         } else {
             PF_TRY(plan_adjoint_before_ring(p, p->st_f.as<double2>(), s));
             const int allow_sole = (p->B == 1 && p->adj_items.view.rmax >= 2) ? 1 : 0;
@@ -166,9 +175,6 @@ int batch_create(pfsht_plan* const* plans, int n, int nstreams, pfsht_batch** ou
         if (plans[i]->kind == kMultiBox)
             return fail(PFSHT_ERR_UNSUPPORTED, "a multi-box plan cannot join a batch; batch its boxes' "
                                                "geometries as plans of their own");
-        if (plans[i]->spin != 0)
-            return fail(PFSHT_ERR_UNSUPPORTED, "a spin plan cannot join a batch (the batched ring "
-                                               "pass is the scalar recurrence)");
     }
     const int dev = plans[0]->device;
     for (int i = 0; i < n; ++i) {
@@ -210,8 +216,11 @@ int batch_create(pfsht_plan* const* plans, int n, int nstreams, pfsht_batch** ou
         s.H = p->H.as<double2>();
         s.allow_sole = (p->B == 1 && p->adj_items.view.rmax >= 2) ? 1 : 0;
         s.ptr = i;
-        fw[i] = RingBatchPlan{&p->fwd_items.host, p->B, p->fwd_items.view.rmax, p->rt.mix};
-        ad[i] = RingBatchPlan{&p->adj_items.host, p->B, p->adj_items.view.rmax, p->rt.mix};
+        // spin plans run their own ring passes on the side streams (the merged launches are the
+        // scalar recurrence)
+        static const std::vector<RingItem> kNone;
+        fw[i] = RingBatchPlan{p->spin ? &kNone : &p->fwd_items.host, p->B, p->fwd_items.view.rmax, p->rt.mix};
+        ad[i] = RingBatchPlan{p->spin ? &kNone : &p->adj_items.host, p->B, p->adj_items.view.rmax, p->rt.mix};
         const int64_t tot = p->M * p->B;
         for (int64_t o = 0; o < tot; o += kFChunk) chunks.push_back(FChunk{i, o, std::min(kFChunk, tot - o)});
     }

@@ -228,6 +228,12 @@ int spin_ring_forward(const SpinTables& t, const RingOut& o, const RingItems& it
 // overwrites alm (entries below l = max(|m|, |s|) zero)
 int spin_ring_adjoint(const SpinTables& t, const RingOut& o, const RingItems& it,
                       const double2* in, double2* alm, int B, cudaStream_t s);
+// the same with the coefficient array at ptrs[ptr] (a batch's device pointer table); the adjoint
+// adds into that array, which the caller zeroes first
+int spin_ring_forward_ptr(const SpinTables& t, const RingOut& o, const RingItems& it,
+                          void* const* ptrs, int ptr, double2* out, int B, cudaStream_t s);
+int spin_ring_adjoint_ptr(const SpinTables& t, const RingOut& o, const RingItems& it,
+                          const double2* in, void* const* ptrs, int ptr, int B, cudaStream_t s);
 
 // ---------------------------------------------------------------------------------------
 // per-stage CUDA-event timing of applies (diagnostics; off unless a profile is active)

@@ -1128,6 +1128,7 @@ int build_ring_batch(const std::vector<RingBatchPlan>& plans, bool adjoint,
     }
     for (auto& kv : by) {
         auto& vec = kv.second;
+        if (vec.empty()) continue;  // plans without merged items (spin plans) make no launch
         std::stable_sort(vec.begin(), vec.end(),
                          [](const auto& a, const auto& b) { return a.first > b.first; });
         std::vector<BatchItem> items(vec.size());

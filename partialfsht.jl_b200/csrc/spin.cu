@@ -180,11 +180,13 @@ __device__ void spin_fwd_item(const SpinTables& t, const RingOut& o, const RingI
 __global__ void __launch_bounds__(kSpinWarps * 32)
 spin_fwd_kernel(SpinTables t, RingOut o, const RingItem* __restrict__ items, int nitems,
                 const int* __restrict__ jlo, const int* __restrict__ jhi, const double2* __restrict__ alm,
-                double2* __restrict__ out, int B) {
+                void* const* __restrict__ ptrs, int ptr, double2* __restrict__ out, int B) {
     __shared__ SpinFwdSmem sm[kSpinWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int it = blockIdx.x * kSpinWarps + warp;
     if (it >= nitems) return;
+    // in a batch the coefficient array is read from the batch's pointer table
+    if (ptrs) alm = static_cast<const double2*>(ptrs[ptr]);
     const RingItem item = items[it];
     const int m = item.m, am = abs(m);
     for (int b = 0; b < B; ++b) {
@@ -325,11 +327,13 @@ __device__ void spin_adj_item(const SpinTables& t, const RingOut& o, const RingI
 
 __global__ void __launch_bounds__(kSpinAdjWarps * 32)
 spin_adj_kernel(SpinTables t, RingOut o, const RingItem* __restrict__ items, int nitems,
-                const double2* __restrict__ in, double* __restrict__ almd, int B) {
+                const double2* __restrict__ in, double* __restrict__ almd, void* const* __restrict__ ptrs,
+                int ptr, int B) {
     __shared__ SpinAdjSmem sm[kSpinAdjWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int it = blockIdx.x * kSpinAdjWarps + warp;
     if (it >= nitems) return;
+    if (ptrs) almd = static_cast<double*>(ptrs[ptr]);
     const RingItem item = items[it];
     for (int b = 0; b < B; ++b) {
         const int reff = (item.n + 31) >> 5;
@@ -387,7 +391,15 @@ int spin_ring_forward(const SpinTables& t, const RingOut& o, const RingItems& it
                       double2* out, int B, cudaStream_t s) {
     if (it.nitems == 0) return 0;
     spin_fwd_kernel<<<(it.nitems + kSpinWarps - 1) / kSpinWarps, kSpinWarps * 32, 0, s>>>(
-        t, o, it.items, it.nitems, it.jlo, it.jhi, alm, out, B);
+        t, o, it.items, it.nitems, it.jlo, it.jhi, alm, nullptr, 0, out, B);
+    return check_launch("spin_fwd_kernel");
+}
+
+int spin_ring_forward_ptr(const SpinTables& t, const RingOut& o, const RingItems& it,
+                          void* const* ptrs, int ptr, double2* out, int B, cudaStream_t s) {
+    if (it.nitems == 0) return 0;
+    spin_fwd_kernel<<<(it.nitems + kSpinWarps - 1) / kSpinWarps, kSpinWarps * 32, 0, s>>>(
+        t, o, it.items, it.nitems, it.jlo, it.jhi, nullptr, ptrs, ptr, out, B);
     return check_launch("spin_fwd_kernel");
 }
 
@@ -397,7 +409,15 @@ int spin_ring_adjoint(const SpinTables& t, const RingOut& o, const RingItems& it
     PF_CUDA(cudaMemsetAsync(alm, 0, sizeof(double2) * (size_t)(t.lmax + 1) * (2 * t.lmax + 1) * B, s));
     if (it.nitems == 0) return 0;
     spin_adj_kernel<<<(it.nitems + kSpinAdjWarps - 1) / kSpinAdjWarps, kSpinAdjWarps * 32, 0, s>>>(
-        t, o, it.items, it.nitems, in, reinterpret_cast<double*>(alm), B);
+        t, o, it.items, it.nitems, in, reinterpret_cast<double*>(alm), nullptr, 0, B);
+    return check_launch("spin_adj_kernel");
+}
+
+int spin_ring_adjoint_ptr(const SpinTables& t, const RingOut& o, const RingItems& it,
+                          const double2* in, void* const* ptrs, int ptr, int B, cudaStream_t s) {
+    if (it.nitems == 0) return 0;
+    spin_adj_kernel<<<(it.nitems + kSpinAdjWarps - 1) / kSpinAdjWarps, kSpinAdjWarps * 32, 0, s>>>(
+        t, o, it.items, it.nitems, in, nullptr, ptrs, ptr, B);
     return check_launch("spin_adj_kernel");
 }
 
