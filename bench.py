@@ -784,7 +784,8 @@ def run_b200(args, world, rank, local):
                 "d2h_bytes_per_step": hb["d2h_forward"] + hb["d2h_adjoint"],
                 "note": "host-buffer C-ABI applies (pfsht_forward_host / pfsht_adjoint_host), "
                         "pinned memory, wall clock; the coefficient array crosses PCIe as its "
-                        "sph_mode staircase (valid rows, in blocks of orders), the field whole"},
+                        "sph_mode staircase of the retained orders m <= mmax (valid rows, in blocks of "
+                        "orders), the field whole"},
         "gpu_launches": launches,
         "clocks": clk,
     }

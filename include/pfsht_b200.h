@@ -127,8 +127,10 @@ pfsht_status pfsht_forward_host(pfsht_plan* plan, const void* alm, void* f);
 pfsht_status pfsht_adjoint_host(pfsht_plan* plan, const void* f, void* alm);
 
 /* Bytes the two host-buffer applies move across PCIe per call (no reference counterpart):
- * the coefficient array travels as its sph_mode staircase (rows 0..lmax-m of each order, in
- * blocks of orders; the adjoint zeroes the host padding itself), the field whole. */
+ * the coefficient array travels as the sph_mode staircase of the orders the plan retains
+ * (rows 0..lmax-m of each order m <= mmax, in blocks of orders; for a spin plan the columns of
+ * those orders), since the forward reads no other coefficient and the adjoint's others are zero,
+ * which the library writes into the host array itself; the field travels whole. */
 pfsht_status pfsht_host_bytes(const pfsht_plan* plan, int64_t* h2d_forward, int64_t* d2h_forward,
                               int64_t* h2d_adjoint, int64_t* d2h_adjoint);
 

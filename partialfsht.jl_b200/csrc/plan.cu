@@ -768,46 +768,67 @@ pfsht_status pfsht_adjoint(pfsht_plan* p, const void* f, void* alm, void* stream
 
 // The sph_mode coefficient array (src/Layout.jl:13-20) holds order m in the columns 2m - 1 and
 // 2m, rows 0 .. lmax - m: a staircase filling half of the (lmax + 1) x (2 lmax + 1) array.
-// Host copies move it as blocks of orders [m0, m1): the contiguous columns
+// Host copies move the orders up to the plan's highest retained order (host_mmax) as blocks of
+// orders [m0, m1): the contiguous columns
 // [max(0, 2 m0 - 1), 2 m1 - 1), rows 0 .. lmax - m0, one 2-D copy each. Blocks of about
 // (lmax + 1) / 16 orders keep both the number of copies and the padding they carry small.
 struct AlmBlock {
     int c0, c1, rows;
 };
-static std::vector<AlmBlock> alm_blocks(int L) {
+// blocks of the orders 0 .. mu
+static std::vector<AlmBlock> alm_blocks(int L, int mu) {
     const int G = std::max(32, (L + 1 + 15) / 16);
     std::vector<AlmBlock> v;
-    for (int m0 = 0; m0 <= L; m0 += G) {
-        const int m1 = std::min(L + 1, m0 + G);
+    for (int m0 = 0; m0 <= mu; m0 += G) {
+        const int m1 = std::min(mu + 1, m0 + G);
         v.push_back(AlmBlock{m0 == 0 ? 0 : 2 * m0 - 1, 2 * m1 - 1, L + 1 - m0});
     }
     return v;
 }
 
-// bytes a host apply moves: the coefficient blocks (the whole array for a spin plan, whose
-// (l, m + lmax) layout has no staircase) and the field
+// The highest order a plan's applies read or write: the retained orders of the polar truncation
+// (src/Legendre.jl:48-57); the forward reads no coefficient of a higher order and the adjoint
+// writes zeros there, so host applies move only the orders up to it and zero the rest on the host
+static int host_mmax(const pfsht_plan* p) {
+    if (p->kind == kMultiBox) {
+        int mu = 0;
+        for (const auto& c : p->boxes) mu = std::max(mu, host_mmax(c.get()));
+        return mu;
+    }
+    if (p->kind == kDirect) return p->L;
+    return std::min(p->L, p->leaf.mmax);
+}
+
+// bytes a host apply moves: the coefficient blocks of the orders up to host_mmax (for a spin
+// plan, whose (l, m + lmax) layout has no staircase, the columns of those orders) and the field
 static void host_bytes(const pfsht_plan* p, int64_t* alm_bytes, int64_t* f_bytes) {
     int64_t a = 0;
-    if (p->spin != 0) a = (int64_t)(p->L + 1) * (2 * p->L + 1);
+    const int mu = host_mmax(p);
+    if (p->spin != 0) a = (int64_t)(p->L + 1) * (2 * mu + 1);
     else
-        for (const AlmBlock& b : alm_blocks(p->L)) a += (int64_t)b.rows * (b.c1 - b.c0);
+        for (const AlmBlock& b : alm_blocks(p->L, mu)) a += (int64_t)b.rows * (b.c1 - b.c0);
     *alm_bytes = a * (int64_t)sizeof(double2) * p->B;
     *f_bytes = (int64_t)sizeof(double2) * p->M * p->B;
 }
 
 static int alm_copy(pfsht_plan* p, void* host, bool to_device, cudaStream_t s) {
     const int L = p->L;
+    const int mu = host_mmax(p);
     const size_t col = sizeof(double2) * (size_t)(L + 1);
     const size_t tr = col * (2 * L + 1);
     char* h = static_cast<char*>(host);
     char* d = p->st_alm.as<char>();
     if (p->spin != 0) {
-        if (to_device) PF_CUDA(cudaMemcpyAsync(d, h, tr * p->B, cudaMemcpyHostToDevice, s));
-        else PF_CUDA(cudaMemcpyAsync(h, d, tr * p->B, cudaMemcpyDeviceToHost, s));
+        // columns m + lmax for m = -mu .. mu, contiguous in each transform
+        const size_t off = col * (size_t)(L - mu), n = col * (size_t)(2 * mu + 1);
+        for (int b = 0; b < p->B; ++b) {
+            if (to_device) PF_CUDA(cudaMemcpyAsync(d + tr * b + off, h + tr * b + off, n, cudaMemcpyHostToDevice, s));
+            else PF_CUDA(cudaMemcpyAsync(h + tr * b + off, d + tr * b + off, n, cudaMemcpyDeviceToHost, s));
+        }
         return 0;
     }
     for (int b = 0; b < p->B; ++b) {
-        for (const AlmBlock& k : alm_blocks(L)) {
+        for (const AlmBlock& k : alm_blocks(L, mu)) {
             const size_t off = tr * b + col * k.c0;
             const size_t width = sizeof(double2) * (size_t)k.rows;
             if (to_device)
@@ -821,15 +842,18 @@ static int alm_copy(pfsht_plan* p, void* host, bool to_device, cudaStream_t s) {
     return 0;
 }
 
-// zero the padding rows of the host array that the block copies leave out (rows past each
-// block's height), on host threads while the copies run
+// zero what the block copies leave out of the host array (rows past each block's height, and the
+// columns of orders above host_mmax), on host threads while the copies run
 static void alm_zero_host_padding(const pfsht_plan* p, void* host) {
-    if (p->spin != 0) return;  // copied whole
     const int L = p->L;
-    const std::vector<AlmBlock> blocks = alm_blocks(L);
-    std::vector<int> rows(2 * L + 1);
-    for (const AlmBlock& k : blocks)
-        for (int c = k.c0; c < k.c1; ++c) rows[c] = k.rows;
+    const int mu = host_mmax(p);
+    std::vector<int> rows(2 * L + 1, 0);
+    if (p->spin != 0) {
+        for (int c = L - mu; c <= L + mu; ++c) rows[c] = L + 1;  // copied whole
+    } else {
+        for (const AlmBlock& k : alm_blocks(L, mu))
+            for (int c = k.c0; c < k.c1; ++c) rows[c] = k.rows;
+    }
     double2* h = static_cast<double2*>(host);
     const int64_t ncol = (int64_t)(2 * L + 1) * p->B;
 #pragma omp parallel for schedule(static) num_threads(16) if (ncol > 512)

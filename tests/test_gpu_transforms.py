@@ -164,6 +164,10 @@ def test_host_buffers_equal_device_applies(pf, O, cuda, L, B):
     pad = ~O.valid_mask(L)
     dirty = alm.copy(order="F")
     dirty[pad] = np.nan
+    # orders above the plan's retained maximum are not read either (the polar truncation)
+    mu = ps.info["mmax"]
+    assert mu < L
+    dirty[:, 2 * mu + 1:] = np.nan
     a_in = np.asfortranarray(dirty if B > 1 else dirty[:, :, 0])
     f_host = pf.zeros_field(len(th), ntrans=B, device="cpu")
     ps.mul(f_host, a_in)
@@ -178,9 +182,12 @@ def test_host_buffers_equal_device_applies(pf, O, cuda, L, B):
     assert np.all(a3[pad] == 0)
     # the adjoint adds some partial sums atomically: equal up to the order of those additions
     assert O.alm_reldiff(a_host, a_dev, L) < 1e-14
+    assert np.all(a3[:, 2 * mu + 1:] == 0)
+    # the coefficient staircase of the orders up to mmax crosses PCIe, in blocks of orders
     hb = ps.host_bytes()
-    valid = (L + 1) ** 2 * 16 * B
+    valid = ((L + 1) + 2 * sum(L + 1 - m for m in range(1, mu + 1))) * 16 * B
     assert valid <= hb["h2d_forward"] < 1.15 * valid
+    assert hb["d2h_adjoint"] == hb["h2d_forward"]
     assert hb["d2h_forward"] == hb["h2d_adjoint"] == len(th) * 16 * B
 
 
