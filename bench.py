@@ -719,6 +719,30 @@ def run_b200(args, world, rank, local):
                  "note": "FP64 recurrence and exponents, FP32 compensated ring sums, FP32 "
                          "NUFFT (w=7); same points, inputs and timing as the headline"}
         del pm
+    # the workload's two other readings, timed once to show they do not change the speed:
+    # coefficients in the m >= 0 slots only, and points theta* sqrt(u) (the reference's
+    # benchmark/calibrate.jl:56 draw) instead of cos(theta) uniform
+    variants = None
+    if not args.no_variants and world == 1:
+        nv = max(20, min(args.steps, 50))
+        apos = []
+        for a in alms:
+            b = a.clone()
+            b[:, 1::2] = 0  # columns 2|m| - 1 hold m < 0
+            apos.append(b)
+        Tp, _ = time_applies(pf, plan, apos, fins, fout, aout, nv, args.warmup, stream)
+        rs = np.random.default_rng(4096)
+        th2 = THETA_STAR * np.sqrt(rs.random(M))
+        ph2 = 2 * np.pi * rs.random(M)
+        p2 = pf.Plan(th2, ph2, lmax=args.lmax, tol=args.tol, precision=args.precision, device=local,
+                     fft_lengths=fft_lengths_arg(args.fft_lengths))
+        Ts, _ = time_applies(pf, p2, alms, fins, fout, aout, nv, args.warmup, stream)
+        variants = {"steps": nv,
+                    "alm_m_nonneg_ms_per_step": Tp / nv,
+                    "points_theta_sqrt_u_ms_per_step": Ts / nv,
+                    "points_theta_sqrt_u_ring_work": p2.info["ring_work"],
+                    "headline_ms_per_step": T / args.steps}
+        del p2
     serve = None
     if not args.no_serve and world == 1:
         serve = measure_serving(pf)
@@ -777,6 +801,7 @@ def run_b200(args, world, rank, local):
         "accuracy": {"tol": args.tol, "l2_rel_vs_direct": err, "dot_rel": dot,
                      "sample": "4096 seeded points, FP64 direct evaluation on the device"},
         "mixed": mixed,
+        "variants": variants,
         "serve": serve,
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_ms / world, "unit": "ms",
@@ -807,6 +832,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-form measurement")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving measurement")
+    ap.add_argument("--no-variants", action="store_true",
+                    help="skip the m >= 0 and theta* sqrt(u) workload variants")
     ap.add_argument("--config", default="headline",
                     choices=["headline", "batch", "serve", "solve", "spin"],
                     help="headline (default): the lmax 2048 cap; batch: 64 plans in one graph; "
