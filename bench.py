@@ -220,7 +220,40 @@ def stage_work(info, stage, B=1):
         return 8.0 * M * w * w * B, U + pts + M * 16 * B
     if stage == "spread":
         return 8.0 * M * w * w * B, U + pts + M * 16 * B
+    P = nf1 * ncols * 16 * B       # the padded dim-1 grid
+    K = nrows * ncols * 16 * B     # its kept rows, mode columns only
+    if stage == "nufft_pad":       # mode columns in, padded grid out (zeros included)
+        return 0.0, H + P
+    if stage == "nufft_unpad":     # the modes read back out of the padded grid
+        return 0.0, 2 * H
+    if stage == "rows_fwd":        # kept rows of the mode columns in, fine rows out
+        return 0.0, K + U
+    if stage == "rows_adj":        # fine rows' mode columns in, kept rows out
+        return 0.0, 2 * K
     return 0.0, 0.0
+
+
+def stage_rooflines(info, stages, fp64_peak, hbm):
+    """Per stage of our own kernels: time per launch, algorithmic FP64 rate and bytes rate against
+    the measured peaks, and the DRAM rate from the ncu traffic per launch where one is recorded."""
+    traffic = load_traffic()
+    out = {}
+    for k, (tot, n) in stages.items():
+        if k.startswith("fft_"):
+            continue
+        ms = tot / n
+        fl, by = stage_work(info, k)
+        r = {"ms": round(ms, 4)}
+        if fl:
+            r["fp64_tflops"] = round(fl / (ms * 1e-3) / 1e12, 2)
+            r["frac_fp64"] = round(fl / (ms * 1e-3) / 1e12 / fp64_peak, 3)
+        if by:
+            r["alg_gbs"] = round(by / (ms * 1e-3) / 1e9, 1)
+            r["frac_hbm"] = round(by / (ms * 1e-3) / 1e9 / hbm, 3)
+        if k in traffic:
+            r["dram_gbs"] = round(traffic[k] / (ms * 1e-3) / 1e9, 1)
+        out[k] = r
+    return out
 
 
 def time_applies(pf, plan, alms, fins, fout, aout, steps, warmup, stream):
@@ -798,6 +831,7 @@ def run_b200(args, world, rank, local):
         "plan_build_s": build_s,
         "roofline": roof,
         "stages_ms": stage_ms,
+        "stages_roofline": stage_rooflines(info, stages, fp64_peak, hbm),
         "accuracy": {"tol": args.tol, "l2_rel_vs_direct": err, "dot_rel": dot,
                      "sample": "4096 seeded points, FP64 direct evaluation on the device"},
         "mixed": mixed,
