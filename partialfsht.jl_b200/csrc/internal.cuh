@@ -192,8 +192,11 @@ int build_ring_segments(const RingTables& t, const std::vector<int>& jlo,
 // launchers: B transforms, alm complex (lmax+1, 2lmax+1, B); the adjoint writes all of alm
 int ring_forward(const RingTables& t, const RingOut& o, const RingItems& it, const double2* alm,
                  double2* out, int B, cudaStream_t s);
+// prepare = false: the caller has run ring_adjoint_prepare on alm (zeroing what the pass does
+// not store), e.g. on another stream ahead of the pass
 int ring_adjoint(const RingTables& t, const RingOut& o, const RingItems& it, const double2* in,
-                 double2* alm, int B, cudaStream_t s);
+                 double2* alm, int B, cudaStream_t s, bool prepare = true);
+int ring_adjoint_prepare(const RingTables& t, const RingItems& it, double2* alm, int B, cudaStream_t s);
 
 // ---------------------------------------------------------------------------------------
 // spin-weighted ring pass (spin.cu): G[j, m] = sum_l sa_{lm} N_l d^l_{m,-s}(theta_j) for
@@ -225,9 +228,9 @@ int build_spin_items(const std::vector<int>& jlo, const std::vector<int>& jhi, i
                      int rings_per_tile, RingItemsOwner& own, cudaStream_t s);
 int spin_ring_forward(const SpinTables& t, const RingOut& o, const RingItems& it,
                       const double2* alm, double2* out, int B, cudaStream_t s);
-// overwrites alm (entries below l = max(|m|, |s|) zero)
+// overwrites alm (entries below l = max(|m|, |s|) zero); clear = false: the caller has zeroed it
 int spin_ring_adjoint(const SpinTables& t, const RingOut& o, const RingItems& it,
-                      const double2* in, double2* alm, int B, cudaStream_t s);
+                      const double2* in, double2* alm, int B, cudaStream_t s, bool clear = true);
 // the same with the coefficient array at ptrs[ptr] (a batch's device pointer table); the adjoint
 // adds into that array, which the caller zeroes first
 int spin_ring_forward_ptr(const SpinTables& t, const RingOut& o, const RingItems& it,

@@ -562,6 +562,9 @@ int plan_create(const double* theta, const double* phi, int64_t npts, int lmax, 
     p->seg_degrees = o.ring_segment_degrees;
     p->spin = o.spin;
     PF_CUDA(cudaStreamCreateWithFlags(&p->st_stream, cudaStreamNonBlocking));
+    PF_CUDA(cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking));
+    PF_CUDA(cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming));
+    PF_CUDA(cudaEventCreateWithFlags(&p->ev_join, cudaEventDisableTiming));
     cudaStream_t s = p->st_stream;
 
     // host and device copies of the points
@@ -682,12 +685,25 @@ int apply_forward(pfsht_plan* p, const double2* alm, double2* f, cudaStream_t s)
 
 int apply_adjoint(pfsht_plan* p, const double2* f, double2* alm, cudaStream_t s) {
     if (p->kind == kMultiBox) return multibox_adjoint(p, f, alm, s);
+    // zero what the ring pass will not store on the side stream, overlapped with the NUFFT and
+    // Theta-FFT stages (a bandwidth-bound fill beside compute-bound kernels); joined before the pass
+    PF_CUDA(cudaEventRecord(p->ev_fork, s));
+    PF_CUDA(cudaStreamWaitEvent(p->side, p->ev_fork, 0));
+    if (p->spin != 0)
+        PF_CUDA(cudaMemsetAsync(alm, 0, sizeof(double2) * (size_t)(p->L + 1) * (2 * p->L + 1) * p->B,
+                                p->side));
+    else
+        PF_TRY(ring_adjoint_prepare(p->rt, p->adj_items.view, alm, p->B, p->side));
+    PF_CUDA(cudaEventRecord(p->ev_join, p->side));
     clock_begin(&p->clk, s);
     PF_TRY(plan_adjoint_before_ring(p, f, s));
+    PF_CUDA(cudaStreamWaitEvent(s, p->ev_join, 0));
     if (p->spin != 0)
-        PF_TRY(spin_ring_adjoint(p->spt.t, p->ro_cols, p->fwd_items.view, p->H.as<double2>(), alm, p->B, s));
+        PF_TRY(spin_ring_adjoint(p->spt.t, p->ro_cols, p->fwd_items.view, p->H.as<double2>(), alm, p->B,
+                                 s, false));
     else
-        PF_TRY(ring_adjoint(p->rt, p->ro_cols, p->adj_items.view, p->H.as<double2>(), alm, p->B, s));
+        PF_TRY(ring_adjoint(p->rt, p->ro_cols, p->adj_items.view, p->H.as<double2>(), alm, p->B, s,
+                            false));
     clock_mark(&p->clk, p->kind == kDirect ? kStDirect : kStRingAdj, s);
     return 0;
 }

@@ -45,6 +45,9 @@ struct pfsht_plan {
     // host-buffer staging
     DevBuf st_alm, st_f;
     cudaStream_t st_stream = nullptr;
+    // the adjoint zeroes its output on `side` while the NUFFT and Theta-FFT stages run
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     // MultiBox (src/MultiBox.jl): one stretched-leaf plan per box; gidx holds the boxes' point
     // indices one box after the other (box i at [box_off[i], box_off[i + 1])), fg the boxes'
     // fields in the same order (box i at B box_off[i]), acc one coefficient array for the sum
@@ -56,6 +59,9 @@ struct pfsht_plan {
     ~pfsht_plan() {
         if (have_fth) cufftDestroy(fth);
         if (st_stream) cudaStreamDestroy(st_stream);
+        if (side) cudaStreamDestroy(side);
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
         for (cudaEvent_t e : clk.ev) cudaEventDestroy(e);
     }
 };

@@ -1021,12 +1021,18 @@ static int ring_adjoint_t(const RingTables& t, const RingOut& o, const RingItems
     return 0;
 }
 
+// a single transform with the item's own tile shape stores sole orders directly; the
+// multi-transform kernels split items into passes and always add
+static int adjoint_allow_sole(const RingItems& it, int B) { return (B == 1 && it.rmax >= 2) ? 1 : 0; }
+
+int ring_adjoint_prepare(const RingTables& t, const RingItems& it, double2* alm, int B, cudaStream_t s) {
+    return alm_prepare(alm, t.lmax, B, it.sole_m, adjoint_allow_sole(it, B), s);
+}
+
 int ring_adjoint(const RingTables& t, const RingOut& o, const RingItems& it, const double2* in,
-                 double2* alm, int B, cudaStream_t s) {
-    // a single transform with the item's own tile shape stores sole orders directly; the
-    // multi-transform kernels split items into passes and always add
-    const int allow_sole = (B == 1 && it.rmax >= 2) ? 1 : 0;
-    PF_TRY(alm_prepare(alm, t.lmax, B, it.sole_m, allow_sole, s));
+                 double2* alm, int B, cudaStream_t s, bool prepare) {
+    const int allow_sole = adjoint_allow_sole(it, B);
+    if (prepare) PF_TRY(alm_prepare(alm, t.lmax, B, it.sole_m, allow_sole, s));
     if (it.nitems <= 0) return 0;
     return t.mix ? ring_adjoint_t<true>(t, o, it, in, alm, B, allow_sole, s)
                  : ring_adjoint_t<false>(t, o, it, in, alm, B, allow_sole, s);

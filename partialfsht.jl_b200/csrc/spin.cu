@@ -404,9 +404,10 @@ int spin_ring_forward_ptr(const SpinTables& t, const RingOut& o, const RingItems
 }
 
 int spin_ring_adjoint(const SpinTables& t, const RingOut& o, const RingItems& it, const double2* in,
-                      double2* alm, int B, cudaStream_t s) {
+                      double2* alm, int B, cudaStream_t s, bool clear) {
     // the adjoint overwrites alm: clear it, then every (l, m) the walk reaches is added
-    PF_CUDA(cudaMemsetAsync(alm, 0, sizeof(double2) * (size_t)(t.lmax + 1) * (2 * t.lmax + 1) * B, s));
+    if (clear)
+        PF_CUDA(cudaMemsetAsync(alm, 0, sizeof(double2) * (size_t)(t.lmax + 1) * (2 * t.lmax + 1) * B, s));
     if (it.nitems == 0) return 0;
     spin_adj_kernel<<<(it.nitems + kSpinAdjWarps - 1) / kSpinAdjWarps, kSpinAdjWarps * 32, 0, s>>>(
         t, o, it.items, it.nitems, in, reinterpret_cast<double*>(alm), nullptr, 0, B);
