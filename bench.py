@@ -503,8 +503,7 @@ def measure_serving(pf, nreq=160, loads=(0.7, 1.0, 1.5), seed=6):
     srv.close()
     return {"plans": len(plans), "requests_per_rate": nreq, "hbm_budget_gb": 120,
             "resident_gb": resident / 1e9, "unbatched_service_ms": service * 1e3,
-            "plan_build_s": build_s,
-        "plan_build_warm_s": build_warm_s, "rates": out,
+            "plan_build_s": build_s, "rates": out,
             "workload": "32 resident plans (lmax 128..2048, cap 5-30 deg, M = 4 (lmax theta*)^2, "
                         "fp64 at 1e-8 / mixed at 1e-6), Poisson arrivals, half synthesis half "
                         "adjoint, host buffers in pinned memory; unbatched = synchronous "
