@@ -187,14 +187,20 @@ def fft_lengths_arg(v):
 
 
 def config_dict(args, M):
+    B = getattr(args, "ntrans", 1)
     return {"workload": f"stretched-leaf fwd+adj, lmax={args.lmax}, 20deg polar cap, M={M}, "
-                        f"tol={args.tol:g}, {args.precision}, ntrans=1",
+                        f"tol={args.tol:g}, {args.precision}, ntrans={B}",
             "lmax": args.lmax, "npts": M, "cap_deg": 20.0, "tol": args.tol,
-            "precision": args.precision, "ntrans": 1,
+            "precision": args.precision, "ntrans": B,
             "alm": "complex N(0,1)/(l+1) in valid sph_mode slots",
             "points": "cos(theta) uniform on the cap, phi uniform, 1% on the boundary",
             "l2": "3 rotating input sets, each apply's buffers larger than L2",
             "parallelism": f"replicas x{args.gpus}"}
+
+
+# the stages of the forward apply (the others are the adjoint's)
+FWD_STAGES = ("ring_fwd", "fft_theta_fwd", "nufft_pad", "fft_fine1_fwd", "rows_fwd", "fft_fine2_fwd",
+              "interp")
 
 
 def load_traffic():
@@ -233,7 +239,7 @@ def stage_work(info, stage, B=1):
     return 0.0, 0.0
 
 
-def stage_rooflines(info, stages, fp64_peak, hbm):
+def stage_rooflines(info, stages, fp64_peak, hbm, B=1):
     """Per stage of our own kernels: time per launch, algorithmic FP64 rate and bytes rate against
     the measured peaks, and the DRAM rate from the ncu traffic per launch where one is recorded."""
     traffic = load_traffic()
@@ -242,7 +248,7 @@ def stage_rooflines(info, stages, fp64_peak, hbm):
         if k.startswith("fft_"):
             continue
         ms = tot / n
-        fl, by = stage_work(info, k)
+        fl, by = stage_work(info, k, B)
         r = {"ms": round(ms, 4)}
         if fl:
             r["fp64_tflops"] = round(fl / (ms * 1e-3) / 1e12, 2)
@@ -661,16 +667,17 @@ def run_b200(args, world, rank, local):
     fp64_peak = fl.value / 1e12
 
     M, theta, phi, rng = workload(args.lmax)
+    B = args.ntrans
     t0 = time.perf_counter()
     plan = pf.Plan(theta, phi, lmax=args.lmax, tol=args.tol, precision=args.precision,
-                   device=local, fft_lengths=fft_lengths_arg(args.fft_lengths))
+                   device=local, fft_lengths=fft_lengths_arg(args.fft_lengths), ntrans=B)
     torch.cuda.synchronize()
     build_s = time.perf_counter() - t0
     # a second build of the same plan: without the process's one-time costs (library loading,
     # the fine-grid FFT length timing, which is cached per process and shape)
     t0 = time.perf_counter()
     p_again = pf.Plan(theta, phi, lmax=args.lmax, tol=args.tol, precision=args.precision,
-                      device=local, fft_lengths=fft_lengths_arg(args.fft_lengths))
+                      device=local, fft_lengths=fft_lengths_arg(args.fft_lengths), ntrans=B)
     torch.cuda.synchronize()
     build_warm_s = time.perf_counter() - t0
     del p_again
@@ -678,12 +685,14 @@ def run_b200(args, world, rank, local):
     nset = 3
     alms, fins = [], []
     for _ in range(nset):
-        ah = rand_alm_host(args.lmax, rng)
-        alms.append(torch.from_numpy(ah).to(dev).permute(2, 1, 0)[:, :, 0])
-        fh = (rng.standard_normal(M) + 1j * rng.standard_normal(M)) / np.sqrt(2)
-        fins.append(torch.from_numpy(fh).to(dev))
-    fout = pf.zeros_field(M, device=dev)
-    aout = pf.zeros_alm(args.lmax, device=dev)
+        ah = rand_alm_host(args.lmax, rng, B)
+        a3 = torch.from_numpy(ah).to(dev).permute(2, 1, 0)
+        alms.append(a3[:, :, 0] if B == 1 else a3)
+        fh = (rng.standard_normal((B, M)) + 1j * rng.standard_normal((B, M))) / np.sqrt(2)
+        f2 = torch.from_numpy(fh).to(dev).T  # (M, B), column-major
+        fins.append(f2[:, 0] if B == 1 else f2)
+    fout = pf.zeros_field(M, B, device=dev)
+    aout = pf.zeros_alm(args.lmax, B, device=dev)
     stream = torch.cuda.current_stream(dev)
 
     def step(i):
@@ -724,11 +733,14 @@ def run_b200(args, world, rank, local):
         launches = int(c.item())
 
     # end to end through the public API with pinned host buffers
-    ah = torch.from_numpy(rand_alm_host(args.lmax, rng)).pin_memory()
-    a_host = ah.numpy().transpose(2, 1, 0)[:, :, 0]
-    f_in = torch.from_numpy((rng.standard_normal(M) + 1j * rng.standard_normal(M))).pin_memory().numpy()
-    f_out = torch.zeros(M, dtype=torch.complex128).pin_memory().numpy()
-    a_out = torch.zeros(ah.shape, dtype=torch.complex128).pin_memory().numpy().transpose(2, 1, 0)[:, :, 0]
+    ah = torch.from_numpy(rand_alm_host(args.lmax, rng, B)).pin_memory()
+    sq = (lambda x: x[:, :, 0]) if B == 1 else (lambda x: x)
+    a_host = sq(ah.numpy().transpose(2, 1, 0))
+    fq = (lambda x: x[:, 0]) if B == 1 else (lambda x: x)
+    f_in = fq(torch.from_numpy(rng.standard_normal((B, M)) + 1j * rng.standard_normal((B, M)))
+              .pin_memory().numpy().T)
+    f_out = fq(torch.zeros((B, M), dtype=torch.complex128).pin_memory().numpy().T)
+    a_out = sq(torch.zeros(ah.shape, dtype=torch.complex128).pin_memory().numpy().transpose(2, 1, 0))
     for _ in range(2):
         plan.mul(f_out, a_host)
         plan.mul_adjoint(a_out, f_in)
@@ -746,9 +758,17 @@ def run_b200(args, world, rank, local):
 
     # accuracy of this form, then the mixed form at tol 1e-6 on the same points and inputs
     acc_rng = np.random.default_rng(7)
-    err, dot = accuracy(pf, plan, theta, phi, args.lmax, alms[0], fins[0], 4096, acc_rng)
+    if B == 1:
+        err, dot = accuracy(pf, plan, theta, phi, args.lmax, alms[0], fins[0], 4096, acc_rng)
+    else:
+        # several transforms: the dot test of every column (the l2 error is a B = 1 figure)
+        err = None
+        fB, aB = plan * alms[0], plan.H * fins[0]
+        dot = max(abs(torch.vdot(fB[:, b], fins[0][:, b]).item()
+                      - torch.vdot(alms[0][:, :, b].T.reshape(-1), aB[:, :, b].T.reshape(-1)).item())
+                  / abs(torch.vdot(fB[:, b], fins[0][:, b]).item()) for b in range(B))
     mixed = None
-    if not args.no_mixed and args.precision == "fp64":
+    if not args.no_mixed and args.precision == "fp64" and B == 1:
         pm = pf.Plan(theta, phi, lmax=args.lmax, tol=1e-6, precision="mixed", device=local)
         Tm, st_m = time_applies(pf, pm, alms, fins, fout, aout, args.steps, args.warmup, stream)
         em, dm = accuracy(pf, pm, theta, phi, args.lmax, alms[0], fins[0], 4096,
@@ -764,7 +784,7 @@ def run_b200(args, world, rank, local):
     # coefficients in the m >= 0 slots only, and points theta* sqrt(u) (the reference's
     # benchmark/calibrate.jl:56 draw) instead of cos(theta) uniform
     variants = None
-    if not args.no_variants and world == 1:
+    if not args.no_variants and world == 1 and B == 1:
         nv = max(20, min(args.steps, 50))
         apos = []
         for a in alms:
@@ -785,7 +805,7 @@ def run_b200(args, world, rank, local):
                     "headline_ms_per_step": T / args.steps}
         del p2
     serve = None
-    if not args.no_serve and world == 1:
+    if not args.no_serve and world == 1 and B == 1:
         serve = measure_serving(pf)
     if world > 1:
         import torch.distributed as dist
@@ -800,7 +820,7 @@ def run_b200(args, world, rank, local):
     ours = {k: v for k, v in stages.items() if not k.startswith("fft_")}
     dom = max(ours, key=lambda k: ours[k][0])
     dom_ms = ours[dom][0] / ours[dom][1]
-    flops, byts = stage_work(info, dom)
+    flops, byts = stage_work(info, dom, B)
     hbm = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs", 6650.0) \
         if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else 6650.0
     traffic = load_traffic().get(dom)
@@ -834,13 +854,15 @@ def run_b200(args, world, rank, local):
         "data": "synthetic",
         "config": dict(config_dict(args, M), nufft_lengths=[info["nf1"], info["nf2"]],
                        fft_lengths=args.fft_lengths),
-        "ns_per_triple": ms_per_step * 1e6 / info["ring_work"],
+        "ns_per_triple": ms_per_step * 1e6 / (info["ring_work"] * B),
+        "ms_forward": sum(v[0] / v[1] for k, v in stages.items() if k in FWD_STAGES),
+        "ms_adjoint": sum(v[0] / v[1] for k, v in stages.items() if k not in FWD_STAGES),
         "ring_work": info["ring_work"],
         "plan_build_s": build_s,
         "plan_build_warm_s": build_warm_s,
         "roofline": roof,
         "stages_ms": stage_ms,
-        "stages_roofline": stage_rooflines(info, stages, fp64_peak, hbm),
+        "stages_roofline": stage_rooflines(info, stages, fp64_peak, hbm, B),
         "accuracy": {"tol": args.tol, "l2_rel_vs_direct": err, "dot_rel": dot,
                      "sample": "4096 seeded points, FP64 direct evaluation on the device"},
         "mixed": mixed,
@@ -870,6 +892,7 @@ def main():
     ap.add_argument("--lmax", type=int, default=2048)
     ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--ntrans", type=int, default=1, help="transforms per plan (headline config)")
     ap.add_argument("--fft-lengths", default="timed",
                     help='NUFFT fine-grid FFT lengths: "timed" (plan default), "minimal" or N1xN2')
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")

@@ -115,7 +115,7 @@ int record(pfsht_batch* b, bool fwd) {
                                          ptrs, i, p->B, s));
         } else {
             PF_TRY(plan_adjoint_before_ring(p, p->st_f.as<double2>(), s));
-            const int allow_sole = (p->B == 1 && p->adj_items.view.rmax >= 2) ? 1 : 0;
+            const int allow_sole = p->adj_items.view.rmax >= 2 ? 1 : 0;
             PF_TRY(alm_prepare_ptr(ptrs, i, p->L, p->B, p->adj_items.view.sole_m, allow_sole, s));
         }
     }
@@ -214,7 +214,7 @@ int batch_create(pfsht_plan* const* plans, int n, int nstreams, pfsht_batch** ou
         s.jlo = p->adj_items.view.jlo;
         s.jhi = p->adj_items.view.jhi;
         s.H = p->H.as<double2>();
-        s.allow_sole = (p->B == 1 && p->adj_items.view.rmax >= 2) ? 1 : 0;
+        s.allow_sole = p->adj_items.view.rmax >= 2 ? 1 : 0;
         s.ptr = i;
         // spin plans run their own ring passes on the side streams (the merged launches are the
         // scalar recurrence)
