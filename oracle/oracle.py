@@ -427,7 +427,7 @@ def mode_k(i0, n, modeord=1):
 
 
 def nufft_direct(typ, n1, n2, iflag, x, y, inp):
-    """DirectSum NUFFT (src/NUFFT.jl:155-199). type 2: modes (n1,n2,B) -> (M,B);
+    """DirectSum NUFFT (src/NUFFT.jl:85-129). type 2: modes (n1,n2,B) -> (M,B);
     type 1: (M,B) -> (n1,n2,B)."""
     x = _f64(x)
     y = _f64(y)

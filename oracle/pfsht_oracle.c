@@ -854,7 +854,7 @@ void orc_fft_rows(double* a, int n1, int n2, int sign, int nthreads) {
 }
 
 /* ------------------------------------------------------------------------------------ */
-/* NUFFT: mode order and DirectSum (src/NUFFT.jl:144-199)                                */
+/* NUFFT: mode order and DirectSum (src/NUFFT.jl:85-129)                                */
 /* ------------------------------------------------------------------------------------ */
 int orc_mode_k(int i0, int n, int modeord) {
     if (modeord == 0) return i0 - n / 2;
@@ -1212,7 +1212,7 @@ void orc_direct_destroy(orc_direct* d) {
     free(d);
 }
 
-/* synthesize_direct! (src/Direct.jl:279-305) */
+/* synthesize_direct! (src/Direct.jl:60-86) */
 void orc_direct_forward(orc_direct* d, const double* alm, double* f, int nthreads) {
     const int L = d->L, B = d->B;
     const int64_t M = d->M;
@@ -1244,7 +1244,7 @@ void orc_direct_forward(orc_direct* d, const double* alm, double* f, int nthread
     }
 }
 
-/* adjoint_direct! (src/Direct.jl:313-336), summed over point blocks */
+/* adjoint_direct! (src/Direct.jl:94-117), summed over point blocks */
 void orc_direct_adjoint(orc_direct* d, const double* f, double* alm, int nthreads) {
     const int L = d->L, B = d->B;
     const int64_t M = d->M;

@@ -81,7 +81,7 @@ void orc_fft_rows(double* a, int n1, int n2, int sign, int nthreads);   /* along
 
 /* ---- NUFFT (src/NUFFT.jl) ---- */
 int orc_mode_k(int i0 /* 0-based */, int n, int modeord);
-/* DirectSum (src/NUFFT.jl:155-199): exact O(M n1 n2); modes in FFT order (modeord=1) */
+/* DirectSum (src/NUFFT.jl:85-129): exact O(M n1 n2); modes in FFT order (modeord=1) */
 void orc_nufft_direct(int type, int n1, int n2, int iflag, int ntrans, const double* x,
                       const double* y, int64_t M, const double* in, double* out);
 /* ES-kernel NUFFT (the published FINUFFT algorithm: exponential-of-semicircle kernel,

@@ -9,7 +9,9 @@
 // breaks. The host keeps one iteration in flight: it launches iteration i, then waits for the
 // state copied out after iteration i - 1, and stops when that says done (the iteration in flight
 // is then a frozen no-op). Dot products reduce in a fixed order (per-block partials, then one
-// block), so a solve is bit-reproducible.
+// block); the adjoint apply inside an iteration adds floating-point atomically (ring tiles of one
+// order, spread rows shared by neighbouring bins), so two solves agree to round-off, not bit for
+// bit.
 #include <cuda_runtime.h>
 
 #include <algorithm>

@@ -22,7 +22,7 @@ def _adj(plan, g):
 
 
 def test_two_caps_against_direct(pf, O, cuda):
-    # test/test_transforms.jl:212-227
+    # test/test_transforms.jl:210-224
     rng = np.random.default_rng(37)
     L, tol = 256, 1e-8
     th, ph = _caps(rng, 80, 0.25)

@@ -26,7 +26,7 @@ def test_host_arrays_are_column_major(pf):
 
 
 def test_plan_argument_errors_before_any_device_use(pf):
-    # src/Plan.jl:98-102 and src/Layout.jl:251-272
+    # src/Plan.jl:98-102 and src/Layout.jl:35-56
     th, ph = np.full(10, 0.1), np.zeros(10)
     with pytest.raises(pf.DimensionMismatch):
         pf.Plan(th, ph[:9], lmax=8)

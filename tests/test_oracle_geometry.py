@@ -7,7 +7,7 @@ from helpers import cap_points
 
 
 def test_derived_relations(O):
-    # test/test_geometry_windows.jl:279-290
+    # test/test_geometry_windows.jl:55-66
     for (thhi, L, eps) in ((0.35, 512, 1e-8), (0.6, 1024, 1e-10), (1.0, 2048, 1e-6)):
         g = O.stretch_geometry(0.0, thhi, L, eps)
         beta = O.es_beta(eps)
@@ -20,7 +20,7 @@ def test_derived_relations(O):
 
 
 def test_window_contract(O):
-    # test/test_geometry_windows.jl:292-301
+    # test/test_geometry_windows.jl:68-77
     g = O.stretch_geometry(0.0, 0.35, 512, 1e-8)
     for Th in np.linspace(0, g.Theta1, 50):
         assert g.window(Th) == 1.0
@@ -30,7 +30,7 @@ def test_window_contract(O):
 
 
 def test_es_cdf_converged_and_monotone(O):
-    # test/test_geometry_windows.jl:303-316
+    # test/test_geometry_windows.jl:79-92
     beta = O.es_beta(1e-8)
     for u in (-1.0, -0.3, 0.0, 0.7, np.pi / 2):
         assert np.isfinite(O.es_cdf(beta, u))
@@ -45,7 +45,7 @@ def test_es_cdf_converged_and_monotone(O):
 
 
 def test_coordinate_maps_invert(O):
-    # test/test_geometry_windows.jl:318-326
+    # test/test_geometry_windows.jl:94-102
     for (lo, hi, L) in ((0.0, 0.4, 512), (0.8, 1.2, 1024), (0.0, np.pi, 256)):
         g = O.stretch_geometry(lo, hi, L, 1e-8)
         for th in np.linspace(max(lo, 1e-6), hi, 20):
@@ -53,7 +53,7 @@ def test_coordinate_maps_invert(O):
 
 
 def test_interior_never_pads_across_a_pole(O):
-    # test/test_geometry_windows.jl:328-339
+    # test/test_geometry_windows.jl:104-115
     for (lo, hi, L) in ((0.02, 0.35, 256), (0.01, 0.5, 512), (2.7, 3.13, 512)):
         g = O.stretch_geometry(lo, hi, L, 1e-8)
         if g.kind == "interior":
@@ -63,7 +63,7 @@ def test_interior_never_pads_across_a_pole(O):
 
 
 def test_degenerate_geometry_refused(O):
-    # test/test_geometry_windows.jl:341-345
+    # test/test_geometry_windows.jl:117-121
     with pytest.raises(ValueError):
         O.stretch_geometry(0.0, 0.05, 32, 1e-10)
     with pytest.raises(ValueError):
@@ -71,7 +71,7 @@ def test_degenerate_geometry_refused(O):
 
 
 def test_full_sphere(O):
-    # test/test_geometry_windows.jl:347-352
+    # test/test_geometry_windows.jl:123-128
     g = O.stretch_geometry(0.0, np.pi, 256, 1e-8)
     assert g.kind == "full"
     assert g.K == 256
@@ -86,7 +86,7 @@ def _smooth(n):
 
 
 def test_grid_sizes_smooth_and_even(O):
-    # test/test_geometry_windows.jl:355-378
+    # test/test_geometry_windows.jl:131-154
     for n in (1, 2, 7, 100, 122, 227, 1000, 4097):
         assert O.next_smooth(n) >= n and _smooth(O.next_smooth(n))
         e = O.next_smooth_even(n)

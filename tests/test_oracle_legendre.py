@@ -52,7 +52,7 @@ def test_closed_form_ylm(O):
 
 
 def test_polar_truncation_bounds_dropped_content(O):
-    # test/test_legendre.jl:116-131
+    # test/test_legendre.jl:52-67
     for (L, th, eps) in ((512, 0.4, 1e-8), (1024, 0.6, 1e-8), (2048, 0.35, 1e-6)):
         mm = O.polar_mmax(th, L, eps)
         if mm >= L:
@@ -65,7 +65,7 @@ def test_polar_truncation_bounds_dropped_content(O):
 
 
 def test_ring_engine_dot_test(O):
-    # test/test_legendre.jl:133-149: <R a, g> = <a, R^T g> to round-off
+    # test/test_legendre.jl:69-85: <R a, g> = <a, R^T g> to round-off
     rng = np.random.default_rng(11)
     for L in (16, 64):
         th = np.sort(0.05 + 0.9 * rng.random(37))
@@ -80,7 +80,7 @@ def test_ring_engine_dot_test(O):
 
 
 def test_ring_engine_matches_per_point_alf(O):
-    # test/test_legendre.jl:151-162
+    # test/test_legendre.jl:87-98
     L = 48
     th = np.sort([0.02, 0.11, 0.37, 0.8, 1.4, 2.7])
     eng = O.Rings(th, L, 1e-13)
@@ -93,7 +93,7 @@ def test_ring_engine_matches_per_point_alf(O):
 
 
 def test_ring_work_counted_and_reduced(O):
-    # test/test_legendre.jl:164-171
+    # test/test_legendre.jl:100-107
     L = 512
     th = np.linspace(1e-3, 0.5, 120)
     w_opt, _ = O.counted_ring_work(th, L, 1e-8)
@@ -103,7 +103,7 @@ def test_ring_work_counted_and_reduced(O):
 
 
 def test_nested_ranges_equal_brute_force(O):
-    # test/test_legendre.jl:173-192, including ring sets that straddle the equator
+    # test/test_legendre.jl:109-128, including ring sets that straddle the equator
     for (lo, hi, L) in ((1e-3, 0.4, 256), (1.2, 2.0, 256), (0.5, 2.6, 512)):
         th = np.linspace(lo, hi, 77)
         mlim = [O.polar_mmax(t, L, 1e-8) for t in th]
