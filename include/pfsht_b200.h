@@ -3,7 +3,7 @@
  * partial-sky spherical harmonic synthesis and its exact adjoint.
  *
  * The entry points are what a PartialFSHT.jl device extension would ccall in place of the
- * reference's Julia leaf (see INTEGRATION.md for the binding). Plain pointers and sizes only.
+ * reference's Julia leaf. Plain pointers and sizes only.
  *
  * Layouts are the reference's, column-major:
  *   alm : (lmax+1) x (2lmax+1) x ntrans complex double, FastSphericalHarmonics sph_mode
@@ -29,7 +29,7 @@ extern "C" {
 typedef enum {
     PFSHT_OK = 0,
     PFSHT_ERR_ARGUMENT = 1,       /* Julia ArgumentError (src/Plan.jl:98-102) */
-    PFSHT_ERR_DIMENSION = 2,      /* Julia DimensionMismatch (src/Layout.jl:251-272) */
+    PFSHT_ERR_DIMENSION = 2,      /* Julia DimensionMismatch (src/Layout.jl:35-56) */
     PFSHT_ERR_REFUSED = 3,        /* degenerate stretch geometry (src/Windows.jl:66-75) */
     PFSHT_ERR_CUDA = 4,           /* a CUDA or cuFFT call failed */
     PFSHT_ERR_OUT_OF_MEMORY = 5,  /* device allocation failed, or a budget was exceeded */
@@ -302,13 +302,16 @@ const char* pfsht_stage_name(int32_t stage);
 /* Direct synthesis without any allocation (no counterpart in the reference): for callers
  * that cannot allocate device memory at the call (a framework owning the device's memory
  * through its own pool, memory reserved in advance, or calls too small to pay for a plan).
- * Computes f_i = sum_lm a_lm Y_lm(theta_i, phi_i) (the Direct leaf, src/Direct.jl:279-305)
+ * Computes f_i = sum_lm a_lm Y_lm(theta_i, phi_i) exactly, as a Direct plan's synthesis does,
  * for device arrays theta, phi (npts), alm ((lmax+1) x (2lmax+1)) and f (npts), with all
  * intermediates in one fixed 32 MiB array the library declares in device memory; it makes no
  * cudaMalloc, cudaFree or other allocating call. Sizes needing more (about
- * npts (2 lmax + 1) 16 bytes) are rejected with PFSHT_ERR_ARGUMENT. The first call on a
- * device looks up the array's address and should come before any stream capture. Calls share
- * the array: calls that overlap on the GPU race and must be serialised by the caller. */
+ * npts (2 lmax + 1) 16 bytes), and lmax above 2048, are rejected with PFSHT_ERR_ARGUMENT.
+ * The first call on a device looks up the array's address and should come before any stream
+ * capture; the address is kept per device for the device's primary context (the CUDA
+ * runtime's), so the call is not for other driver-API contexts or after cudaDeviceReset.
+ * Calls share the array: calls that overlap on the GPU race and must be serialised by the
+ * caller. */
 pfsht_status pfsht_direct_forward_noalloc(const double* theta, const double* phi, int64_t npts,
                                           int32_t lmax, const void* alm, void* f, void* stream);
 

@@ -147,7 +147,7 @@ class PFSHTError(RuntimeError):
 
 
 class DimensionMismatch(ValueError):
-    """Julia's DimensionMismatch (src/Layout.jl:251-272)."""
+    """Julia's DimensionMismatch (src/Layout.jl:35-56)."""
 
 
 class RefusedGeometry(ValueError):

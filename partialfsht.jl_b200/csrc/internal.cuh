@@ -315,7 +315,7 @@ int leaf_points(const Geom& g, bool flip, const double* theta, const double* phi
                 double* Theta, double* phi_out, cudaStream_t s);
 int minmax_device(const double* x, int64_t M, double* mn, double* mx, cudaStream_t s);
 
-// Direct leaf helpers (src/Direct.jl:279-336) on the device
+// Direct leaf helpers (src/Direct.jl:60-117) on the device
 int direct_phase_sum(const double2* G, const double* phi, int64_t M, int lmax, int B,
                      double2* f, cudaStream_t s);
 int direct_phase_spread(const double2* f, const double* phi, int64_t M, int lmax, int B,

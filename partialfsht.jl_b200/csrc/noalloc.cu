@@ -6,7 +6,7 @@
 // graph or another process has reserved in advance, or small utility calls for which a
 // plan's allocations and their cudaMalloc/cudaFree synchronisation cost more than the work.
 // This entry point evaluates f_i = sum_lm a_lm Y_lm(theta_i, phi_i) for a small point set
-// (the reference's Direct leaf, src/Direct.jl:279-305) with every intermediate held in one
+// (the Direct leaf's synthesis, src/Direct.jl:60-86) with every intermediate held in one
 // fixed array of device memory that the library declares at file scope, so it makes no
 // cudaMalloc, cudaFree or other allocating call at all. The caller still passes the points,
 // the coefficients and the output buffer, all on the device.
@@ -17,7 +17,11 @@
 //     call whose sizes need more is rejected with PFSHT_ERR_ARGUMENT before any launch;
 //   - every device that loads the library holds this array until the process exits;
 //   - the first call on a device looks up the array's device address (cudaGetSymbolAddress)
-//     with that device current; make that first call before any stream capture;
+//     with that device current; make that first call before any stream capture. The address
+//     is kept per device ordinal, which assumes the device's primary context (the one the CUDA
+//     runtime uses); after cudaDeviceReset, or from another driver-API context on the same
+//     device, the kept address is stale and the entry point must not be called;
+//   - lmax is at most kNoAllocMaxLmax (the recurrence table alone would not fit above it);
 //   - all calls share the one array and the array keeps the last call's contents, so calls
 //     that overlap on the GPU (different streams, or different host threads on one device)
 //     race and must be serialised by the caller. Every region a call reads is written by the
@@ -36,6 +40,7 @@ namespace pf {
 
 static constexpr size_t kNoAllocScratchBytes = 32u << 20;  // 32 MiB
 static constexpr int kNoAllocTile = 64;                    // rings (points) per work item
+static constexpr int kNoAllocMaxLmax = 2048;               // its (beta, g) table alone nearly fills the array
 
 // the scratch array: host code must not take its address directly (see below)
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
@@ -75,19 +80,22 @@ struct NoAllocLayout {
 
 static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
-static NoAllocLayout noalloc_layout(int64_t M, int L) {
+// all sizes in 64-bit arithmetic: callers bound lmax <= kNoAllocMaxLmax and npts < 2^31, so
+// no product below can overflow, and the total decides whether the call fits
+static NoAllocLayout noalloc_layout(int64_t M, int64_t L) {
     NoAllocLayout y;
-    const int64_t nab = L >= 1 ? (int64_t)L * (L - 1) / 2 + 1 : 1;  // sum over m of max(0, L-m-1)
+    const int64_t nab = L >= 1 ? L * (L - 1) / 2 + 1 : 1;  // sum over m of max(0, L-m-1)
     const int64_t ntile = (M + kNoAllocTile - 1) / kNoAllocTile;
-    y.nitems = (int)((L + 1) * ntile);
+    const int64_t nitems = (L + 1) * ntile;
+    y.nitems = nitems > INT32_MAX ? -1 : (int)nitems;
     size_t o = 0;
-    y.cos_t = o; o = align256(o + sizeof(double) * M);
-    y.log2sin = o; o = align256(o + sizeof(double) * M);
-    y.log2c = o; o = align256(o + sizeof(double) * (L + 1));
-    y.aboff = o; o = align256(o + sizeof(int64_t) * (L + 1));
-    y.ab = o; o = align256(o + sizeof(double2) * nab);
-    y.items = o; o = align256(o + sizeof(RingItem) * (size_t)y.nitems);
-    y.G = o; o = align256(o + sizeof(double2) * (size_t)M * (2 * L + 1));
+    y.cos_t = o; o = align256(o + sizeof(double) * (size_t)M);
+    y.log2sin = o; o = align256(o + sizeof(double) * (size_t)M);
+    y.log2c = o; o = align256(o + sizeof(double) * (size_t)(L + 1));
+    y.aboff = o; o = align256(o + sizeof(int64_t) * (size_t)(L + 1));
+    y.ab = o; o = align256(o + sizeof(double2) * (size_t)nab);
+    y.items = o; o = align256(o + sizeof(RingItem) * (size_t)nitems);
+    y.G = o; o = align256(o + sizeof(double2) * (size_t)M * (size_t)(2 * L + 1));
     y.total = o;
     return y;
 }
@@ -133,7 +141,7 @@ __global__ void noalloc_prep_kernel(const double* __restrict__ theta, int64_t M,
 static int direct_forward_noalloc(const double* theta, const double* phi, int64_t M, int L,
                                   const double2* alm, double2* f, cudaStream_t s) {
     const NoAllocLayout y = noalloc_layout(M, L);
-    if (y.total > kNoAllocScratchBytes) {
+    if (y.total > kNoAllocScratchBytes || y.nitems < 0) {
         set_error("pfsht_direct_forward_noalloc: npts = " + std::to_string(M) + " at lmax = " +
                   std::to_string(L) + " needs " + std::to_string(y.total) +
                   " bytes of scratch, above the fixed " + std::to_string(kNoAllocScratchBytes) +
@@ -192,6 +200,12 @@ extern "C" pfsht_status pfsht_direct_forward_noalloc(const double* theta, const 
     }
     if (npts < 1 || lmax < 0 || npts > INT32_MAX) {
         pf::set_error("pfsht_direct_forward_noalloc: need npts >= 1 and lmax >= 0");
+        return PFSHT_ERR_ARGUMENT;
+    }
+    if (lmax > pf::kNoAllocMaxLmax) {
+        pf::set_error("pfsht_direct_forward_noalloc: lmax = " + std::to_string(lmax) +
+                      " is above the fixed scratch's limit of " +
+                      std::to_string(pf::kNoAllocMaxLmax) + "; use a plan instead");
         return PFSHT_ERR_ARGUMENT;
     }
     return (pfsht_status)pf::direct_forward_noalloc(theta, phi, npts, lmax, (const double2*)alm,

@@ -1,7 +1,7 @@
 // 2-D NUFFT of the stretched leaf and the NUFFT seam, on sm_100a: an exponential-of-
 // semicircle (ES) kernel NUFFT with upsampling 2 (the published FINUFFT algorithm that the
 // reference calls through ext/PartialFSHTFINUFFTExt.jl and ext/PartialFSHTcuFINUFFTExt.jl;
-// its exact semantics are DirectSum's, src/NUFFT.jl:155-199).
+// its exact semantics are DirectSum's, src/NUFFT.jl:85-129).
 //
 // Type 2 (modes -> values), per transform:
 //   pad   : mode columns (n1 x ncols, FFT order along dim 1) times the per-mode factors
@@ -1135,7 +1135,7 @@ int nufft_type1(const NufftGrid& g, NufftDev& d, const double2* f, double2* mode
 }
 
 // ---------------------------------------------------------------------------------------
-// Direct leaf phases (src/Direct.jl:287-333): exact cis(m phi) per (point, order)
+// Direct leaf phases (src/Direct.jl:74-84,102-114): exact cis(m phi) per (point, order)
 // ---------------------------------------------------------------------------------------
 __global__ void direct_sum_kernel(const double2* __restrict__ G, const double* __restrict__ phi,
                                   int64_t M, int L, int B, double2* __restrict__ f) {

@@ -309,7 +309,7 @@ int build_stretch(pfsht_plan* p, const double* d_theta, const double* d_phi, con
 }
 
 // the Direct leaf's ring set: every point a ring, every order on every point (eps = 0,
-// src/Direct.jl:262-263)
+// src/Direct.jl:43-44)
 int build_direct_rings(pfsht_plan* p, const double* h_theta, cudaStream_t s) {
     const int L = p->L;
     const int64_t M = p->M;

@@ -33,7 +33,7 @@ def test_ring_pass_matches_oracle(pf, O, cuda, L):
 @pytest.mark.parametrize("L", [128, 256, 512])
 def test_stretch_apply_matches_oracle(pf, O, cuda, L):
     rng = np.random.default_rng(12)
-    M = 4 * int(round((L * np.deg2rad(20)) ** 2))
+    M = int(round(4 * (L * np.deg2rad(20)) ** 2))  # 31,941 at lmax 256: the workload's M
     th, ph = cap_points(M, rng=rng)
     plan = pf.Plan(th, ph, lmax=L, tol=1e-8)
     ref = O.Stretch(th, ph, L, 1e-8, nufft="es", nufft_grid=plan_grid(plan))

@@ -237,7 +237,7 @@ def test_direct_plan_adjoint_segments(pf, O, cuda):
 
 @pytest.mark.parametrize("typ", [1, 2])
 def test_nufft_seam_matches_direct_sum(pf, O, cuda, typ):
-    # src/NUFFT.jl:17-25 seam against the DirectSum backend (src/NUFFT.jl:155-199)
+    # src/NUFFT.jl:17-25 seam against the DirectSum backend (src/NUFFT.jl:85-129)
     rng = np.random.default_rng(44)
     n1, n2, M, tol = 40, 30, 500, 1e-9
     x = 2 * np.pi * rng.random(M) - np.pi
