@@ -203,6 +203,19 @@ FWD_STAGES = ("ring_fwd", "fft_theta_fwd", "nufft_pad", "fft_fine1_fwd", "rows_f
               "interp")
 
 
+def hbm_peak():
+    """HBM bandwidth denominator: MEASURED_PEAKS.json's hbm_gbs (of measured) when present, else
+    the pool's earlier measurement of 6650 GB/s (of fallback)."""
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        v = json.load(open(p)).get("hbm_gbs")
+        if v:
+            return float(v), "MEASURED_PEAKS.json hbm_gbs (of measured)"
+    except (OSError, ValueError):
+        pass
+    return 6650.0, "6650 GB/s (of fallback: MEASURED_PEAKS.json absent)"
+
+
 def load_traffic():
     p = os.path.join(ROOT, "profiles", "traffic_per_launch.json")
     try:
@@ -804,6 +817,27 @@ def run_b200(args, world, rank, local):
                     "points_theta_sqrt_u_ring_work": p2.info["ring_work"],
                     "headline_ms_per_step": T / args.steps}
         del p2
+    # the benchmark's smaller configurations (lmax 256 and 1024 on the same cap, M = round(4
+    # (lmax theta*)^2)), timed the same way on their own plans
+    other_workloads = None
+    if not args.no_variants and world == 1 and B == 1 and args.lmax == 2048:
+        other_workloads = {}
+        for Lw in (256, 1024):
+            Mw, thw, phw, rw = workload(Lw)
+            pw = pf.Plan(thw, phw, lmax=Lw, tol=args.tol, precision=args.precision, device=local)
+            aw = [torch.from_numpy(rand_alm_host(Lw, rw)).to(dev).permute(2, 1, 0)[:, :, 0]
+                  for _ in range(nset)]
+            fw = [torch.from_numpy((rw.standard_normal(Mw) + 1j * rw.standard_normal(Mw))
+                                   / np.sqrt(2)).to(dev) for _ in range(nset)]
+            fo = pf.zeros_field(Mw, device=dev)
+            ao = pf.zeros_alm(Lw, device=dev)
+            nw = 100
+            Tw, stw = time_applies(pf, pw, aw, fw, fo, ao, nw, args.warmup, stream)
+            other_workloads[f"lmax{Lw}"] = {
+                "npts": Mw, "ms_per_step": Tw / nw, "steps": nw, "ring_work": pw.info["ring_work"],
+                "ns_per_triple": Tw / nw * 1e6 / pw.info["ring_work"],
+                "stages_ms": {k: round(v[0] / v[1], 4) for k, v in stw.items()}}
+            del pw
     serve = None
     if not args.no_serve and world == 1 and B == 1:
         serve = measure_serving(pf)
@@ -815,14 +849,14 @@ def run_b200(args, world, rank, local):
         return 0
 
     ms_per_step = T / args.steps
-    value = ms_per_step / world
+    # each rank runs its own replica of the workload: the time of one fwd+adj (max over ranks)
+    value = ms_per_step
     # roofline of the dominant stage of our kernels
     ours = {k: v for k, v in stages.items() if not k.startswith("fft_")}
     dom = max(ours, key=lambda k: ours[k][0])
     dom_ms = ours[dom][0] / ours[dom][1]
     flops, byts = stage_work(info, dom, B)
-    hbm = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs", 6650.0) \
-        if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else 6650.0
+    hbm, hbm_source = hbm_peak()
     traffic = load_traffic().get(dom)
     if flops / (fp64_peak * 1e12) >= byts / (hbm * 1e9):
         achieved = flops / (dom_ms * 1e-3) / 1e12
@@ -833,18 +867,39 @@ def run_b200(args, world, rank, local):
         roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm}
     roof.update({"kernel": dom, "ms_per_launch": dom_ms, "traffic": traffic,
+                 "traffic_source": "stored ncu figure (profiles/traffic_per_launch.json: "
+                                   "dram__bytes_read.sum + dram__bytes_write.sum per launch of "
+                                   "this kernel at this workload), not measured in this run"
+                 if traffic is not None else None,
                  "peak_source": "FP64 FMA microbenchmark pfsht_fma_peak run in this bench "
                                 "(MEASURED_PEAKS.json has no FP64 figure)"
-                 if roof["bound"] == "fp64" else "MEASURED_PEAKS.json hbm_gbs (measured)"})
+                 if roof["bound"] == "fp64" else hbm_source})
     stage_ms = {k: round(v[0] / v[1], 4) for k, v in stages.items()}
 
     cpu = None
+    acc_oracle = None
     if world == 1 and not args.no_cpu:
         nthreads = os.cpu_count() or 1
         t_cpu, _, _ = cpu_port_apply_time(args.lmax, args.tol, nthreads, napply=2)
+        t_ser, _, _ = cpu_port_apply_time(args.lmax, args.tol, 1, napply=1)
         cpu = {"value": t_cpu * 1e3, "unit": "ms", "cores": nthreads, "kind": "port",
-               "sample": "full workload (lmax 2048, M 2.04e6), best of 2 fwd+adj applies of the "
-                         "C restatement of the reference's CPU apply, OpenMP"}
+               "sample": f"full workload (lmax {args.lmax}, M {M}), best of 2 fwd+adj applies of "
+                         "the C restatement of the reference's CPU apply, OpenMP",
+               "serial_ms": t_ser * 1e3,
+               "serial_sample": "the same workload, one fwd+adj apply on 1 thread",
+               "published_reference": {
+                   "synthesis_only_ms": {"serial": 538.0, "threads_4": 245.0},
+                   "source": "README.md:44 of the reference (lmax 2048, M 2.0e6, tol 1e-8, "
+                             "FINUFFT, 4 physical cores; synthesis alone, no adjoint)"}}
+        # the oracle checks the device result: FP64 direct evaluation of the same coefficients
+        # on a seeded subsample (the CPU leg is where the oracle runs)
+        if B == 1:
+            from oracle import oracle as O
+            sub = np.sort(np.random.default_rng(11).choice(M, 1024, replace=False))
+            a_h = np.asfortranarray(alms[0].cpu().numpy())[:, :, None]
+            fd = O.Direct(theta[sub], phi[sub], args.lmax).forward(a_h, nthreads=nthreads)[:, 0]
+            fs = (plan * alms[0]).cpu().numpy()[sub]
+            acc_oracle = float(np.linalg.norm(fs - fd) / np.linalg.norm(fd))
 
     hb = plan.host_bytes()
     line = {
@@ -864,12 +919,15 @@ def run_b200(args, world, rank, local):
         "stages_ms": stage_ms,
         "stages_roofline": stage_rooflines(info, stages, fp64_peak, hbm, B),
         "accuracy": {"tol": args.tol, "l2_rel_vs_direct": err, "dot_rel": dot,
-                     "sample": "4096 seeded points, FP64 direct evaluation on the device"},
+                     "sample": "4096 seeded points, FP64 direct evaluation on the device",
+                     "l2_rel_vs_oracle_direct": acc_oracle,
+                     "oracle_sample": "1024 seeded points, the CPU oracle's Direct leaf"},
+        "workloads": other_workloads,
         "mixed": mixed,
         "variants": variants,
         "serve": serve,
         "cpu_baseline": cpu,
-        "e2e": {"value": e2e_ms / world, "unit": "ms",
+        "e2e": {"value": e2e_ms, "unit": "ms",
                 "h2d_bytes_per_step": hb["h2d_forward"] + hb["h2d_adjoint"],
                 "d2h_bytes_per_step": hb["d2h_forward"] + hb["d2h_adjoint"],
                 "note": "host-buffer C-ABI applies (pfsht_forward_host / pfsht_adjoint_host), "
