@@ -275,6 +275,12 @@ struct NufftGrid {
     int nsbc = 0, nisb = 0;    // groups per bin row; non-empty groups
     int fp32 = 0;              // fine grids, FFTs, spreading and interpolation in FP32
     int64_t M = 0;
+    // spreading in bin colours: bins (br, bc) of one colour (br mod rcol, bc mod ccol) have
+    // disjoint tiles, so launching the colours one after the other lets every tile add its rows
+    // with plain loads and stores, in a fixed order (a deterministic type-1 NUFFT); 0 colours: the
+    // grid does not allow it and rows add atomically
+    int ncolors = 0;
+    std::vector<int> color_off;  // ncolors + 1 offsets into NufftDev::sorder
 };
 
 struct NufftDev {
@@ -283,6 +289,7 @@ struct NufftDev {
     DevBuf binstart;  // int32 nbins + 1
     DevBuf binorder;  // int32 nbusy: non-empty bins, most points first
     DevBuf iorder;    // int32 nisb: non-empty interpolation groups, most points first
+    DevBuf sorder;    // int32 nbusy: non-empty bins by spreading colour, most points first in each
     DevBuf colp2;     // int32 ncols: fine column of each mode column
     DevBuf p2col;     // int32 nf2: mode column of each fine column or -1
     DevBuf mult1;     // double2 n1: per-mode complex factor along dim 1 (deconv incl.)
