@@ -210,6 +210,7 @@ int batch_create(pfsht_plan* const* plans, int n, int nstreams, pfsht_batch** ou
         stf[i] = p->st_f.as<double2>();
         RingSlot& s = slots[i];
         s.t = p->rt;
+        s.tf = p->rt_fwd;
         s.o = p->ro_cols;
         s.jlo = p->adj_items.view.jlo;
         s.jhi = p->adj_items.view.jhi;
@@ -219,7 +220,7 @@ int batch_create(pfsht_plan* const* plans, int n, int nstreams, pfsht_batch** ou
         // spin plans run their own ring passes on the side streams (the merged launches are the
         // scalar recurrence)
         static const std::vector<RingItem> kNone;
-        fw[i] = RingBatchPlan{p->spin ? &kNone : &p->fwd_items.host, p->B, p->fwd_items.view.rmax, p->rt.mix};
+        fw[i] = RingBatchPlan{p->spin ? &kNone : &p->fwd_items.host, p->B, p->fwd_items.view.rmax, p->rt_fwd.mix};
         ad[i] = RingBatchPlan{p->spin ? &kNone : &p->adj_items.host, p->B, p->adj_items.view.rmax, p->rt.mix};
         const int64_t tot = p->M * p->B;
         for (int64_t o = 0; o < tot; o += kFChunk) chunks.push_back(FChunk{i, o, std::min(kFChunk, tot - o)});

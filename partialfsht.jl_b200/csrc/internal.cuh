@@ -137,7 +137,8 @@ struct RingItemsOwner {
 
 // one plan of a batched ring pass, as the batched kernels read it from device memory
 struct RingSlot {
-    RingTables t;
+    RingTables t;   // the adjoint's tables
+    RingTables tf;  // the forward's (the mixed form's forward runs in FP64 on its own table)
     RingOut o;
     const int* jlo = nullptr;
     const int* jhi = nullptr;
@@ -182,7 +183,7 @@ std::vector<RingItem> make_ring_items(const std::vector<int>& jlo, const std::ve
                                       const RingSegments* seg = nullptr);
 int build_ring_items(const std::vector<int>& jlo, const std::vector<int>& jhi, int lmax, int mmax,
                      int rmax, RingItemsOwner& own, cudaStream_t s,
-                     const RingSegments* seg = nullptr);
+                     const RingSegments* seg = nullptr, int tile = 0);
 // choose the degree segments for a ring set (seg_degrees > 0: target length; 0: none) and
 // save the recurrence state at every segment start; t.ab/aboff must be built. Returns the
 // segments unused (nseg all 1) when the state would exceed max_bytes.

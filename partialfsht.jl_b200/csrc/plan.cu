@@ -202,24 +202,30 @@ void fill_info(pfsht_plan* p) {
                             &p->adj_seg.ck_p, &p->adj_seg.ck_E,
                             &p->H, &p->phi_pts, &p->nd.pts, &p->nd.perm, &p->nd.binstart,
                             &p->nd.colp2, &p->nd.p2col, &p->nd.mult1, &p->nd.dec2, &p->nd.pad,
-                            &p->nd.U, &p->st_alm, &p->st_f})
+                            &p->nd.U, &p->st_alm, &p->st_f, &p->ab_fwd})
         bytes += (int64_t)b->bytes;
     in.device_bytes = bytes;
 }
 
-// Adjoint items: tiles of 32 * R rings, each order split into degree segments of about
-// seg_degrees when the unsplit items would give fewer than ~8 warps per resident warp slot
-// (12 per SM at the adjoint's register count). The saved recurrence state is bounded by
-// 512 MiB; past that, or with seg_degrees < 0, the items stay whole.
+// Adjoint items: all retained rings of an order in one item when no order retains more than
+// four tiles of 32 * R rings (the warp walks them tile after tile and adds each tile's sums to
+// the previous ones in order: a deterministic pass without atomics), else tiles of 32 * R rings
+// whose sums add atomically; each order split into degree segments of about seg_degrees when the
+// unsplit items would give fewer than ~8 warps per resident warp slot (12 per SM at the
+// adjoint's register count). The saved recurrence state is bounded by 512 MiB; past that, or
+// with seg_degrees < 0, the items stay whole.
 int build_adjoint_items(pfsht_plan* p, const std::vector<int>& jlo, const std::vector<int>& jhi,
                         int mmax, cudaStream_t s) {
     const int L = p->L;
     const int rmax = p->R > 0 ? p->R : 4;
+    int maxret = 0;
+    for (int m = 0; m <= std::min(mmax, L); ++m) maxret = std::max(maxret, jhi[m] - jlo[m] + 1);
+    const int tile = maxret <= 4 * 32 * rmax ? std::max(maxret, 1) : 32 * rmax;
     int seg = p->seg_degrees;
     if (seg == 0) {
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device);
-        const size_t whole = make_ring_items(jlo, jhi, L, mmax, 32 * rmax).size();
+        const size_t whole = make_ring_items(jlo, jhi, L, mmax, tile).size();
         seg = whole >= (size_t)sms * 12 * 8 ? -1 : 256;
     }
     if (seg > 0) {
@@ -228,7 +234,7 @@ int build_adjoint_items(pfsht_plan* p, const std::vector<int>& jlo, const std::v
         p->rt.ck_E = p->adj_seg.ck_E.as<int>();
     }
     return build_ring_items(jlo, jhi, L, mmax, rmax, p->adj_items, s,
-                            p->adj_seg.seg_degrees > 0 ? &p->adj_seg : nullptr);
+                            p->adj_seg.seg_degrees > 0 ? &p->adj_seg : nullptr, tile);
 }
 
 int build_stretch(pfsht_plan* p, const double* d_theta, const double* d_phi, const pfsht_opts& o,
@@ -262,8 +268,15 @@ int build_stretch(pfsht_plan* p, const double* d_theta, const double* d_phi, con
         // forward tiles of 64 rings in the FP64 form (more warps) and of 128 in the mixed form
         // (measured faster), adjoint tiles of 128 (amortises its reduction), split along the
         // degree axis when the tiles alone leave the GPU under-filled
-        PF_TRY(build_ring_items(lf.jlo, lf.jhi, L, lf.mmax, p->R > 0 ? p->R : (mix ? 4 : 2),
-                                p->fwd_items, s));
+        p->rt_fwd = p->rt;
+        if (mix) {
+            DevBuf off_unused;  // the offsets equal p->aboff (they depend on lmax and mmax only)
+            PF_TRY(build_ab_table(L, lf.mmax, 64, p->ab_fwd, off_unused, s));
+            p->rt_fwd.ab = p->ab_fwd.as<double2>();
+            p->rt_fwd.mix = 0;
+            p->rt_fwd.stride = 64;
+        }
+        PF_TRY(build_ring_items(lf.jlo, lf.jhi, L, lf.mmax, p->R > 0 ? p->R : 2, p->fwd_items, s));
         PF_TRY(build_adjoint_items(p, lf.jlo, lf.jhi, lf.mmax, s));
     }
     p->ncols = 2 * lf.mmax + 1;
@@ -346,6 +359,7 @@ int build_direct_rings(pfsht_plan* p, const double* h_theta, cudaStream_t s) {
     p->rt.aboff = p->aboff.as<int64_t>();
     p->rt.lmax = L;
     p->rt.nrings = (int)M;
+    p->rt_fwd = p->rt;
     PF_TRY(build_ring_items(jlo, jhi, L, L, p->R > 0 ? p->R : 2, p->fwd_items, s));
     return build_adjoint_items(p, jlo, jhi, L, s);
 }
@@ -678,7 +692,7 @@ int apply_forward(pfsht_plan* p, const double2* alm, double2* f, cudaStream_t s)
     if (p->spin != 0)
         PF_TRY(spin_ring_forward(p->spt.t, p->ro_cols, p->fwd_items.view, alm, p->H.as<double2>(), p->B, s));
     else
-        PF_TRY(ring_forward(p->rt, p->ro_cols, p->fwd_items.view, alm, p->H.as<double2>(), p->B, s));
+        PF_TRY(ring_forward(p->rt_fwd, p->ro_cols, p->fwd_items.view, alm, p->H.as<double2>(), p->B, s));
     if (p->kind != kDirect) clock_mark(&p->clk, kStRingFwd, s);
     return plan_forward_after_ring(p, f, s);
 }
@@ -950,7 +964,7 @@ pfsht_status pfsht_ring_forward(pfsht_plan* p, const void* alm, void* G, void* s
         return (pfsht_status)fail(PFSHT_ERR_UNSUPPORTED, "a multi-box plan has one ring set per box");
     DeviceGuard dg(p->device);
     cudaStream_t s = (cudaStream_t)stream;
-    RingTables t = p->rt;
+    RingTables t = p->rt_fwd;
     t.w = nullptr;
     RingOut o;
     o.ld = p->nrings;

@@ -28,6 +28,11 @@ struct pfsht_plan {
     RingSegments adj_seg;  // degree segments of the adjoint items
     int seg_degrees = 0;   // requested segment length (0 = auto, < 0 = none)
     RingTables rt;
+    // the forward ring pass's tables: rt itself, except in the mixed form, whose forward runs the
+    // FP64 pass (FP32 accumulation saves nothing there: each ring value's conversion costs as
+    // much as the FP64 multiply-adds) on its own (beta, g) table of 64-degree blocks
+    RingTables rt_fwd;
+    DevBuf ab_fwd;
     // spin weight s (src/Spin.jl): s != 0 runs the Wigner-d ring pass on spt with the items in
     // fwd_items for both directions; coefficients in the (l, m + lmax) layout
     int spin = 0;

@@ -273,11 +273,12 @@ int build_ring_segments(const RingTables& t, const std::vector<int>& jlo,
 // ---------------------------------------------------------------------------------------
 template <bool MIX> using CoefT = std::conditional_t<MIX, float2, double2>;
 
+// one warp's staging (a block holds one per warp)
 template <int NB, bool MIX>
 struct FwdSmem {
-    double2 bg[kWarpsPerBlock][32];               // (beta_l, g_l) of the chunk's degrees
-    CoefT<MIX> ap[kWarpsPerBlock][NB][32];        // g_l a_{l,+m}
-    CoefT<MIX> am[kWarpsPerBlock][NB][32];        // g_l (-1)^m a_{l,-m}
+    double2 bg[32];               // (beta_l, g_l) of the chunk's degrees
+    CoefT<MIX> ap[NB][32];        // g_l a_{l,+m}
+    CoefT<MIX> am[NB][32];        // g_l (-1)^m a_{l,-m}
 };
 
 // accumulator of one (ring, +-m, transform): FP64, or FP32 blocks into a two-sum total
@@ -421,7 +422,7 @@ __device__ __forceinline__ void ring_fwd_item(const RingTables& t, const RingOut
         lstart = m + 2;
     }
     auto step = [&](int i) {
-        const double beta = sm.bg[warp][i].x;
+        const double beta = sm.bg[i].x;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const double qn = fma(x[r], q1[r], -(beta * q2[r]));
@@ -435,8 +436,8 @@ __device__ __forceinline__ void ring_fwd_item(const RingTables& t, const RingOut
         }
 #pragma unroll
         for (int b = 0; b < NB; ++b) {
-            const CoefT<MIX> ap = sm.ap[warp][b][i];
-            const CoefT<MIX> am = sm.am[warp][b][i];
+            const CoefT<MIX> ap = sm.ap[b][i];
+            const CoefT<MIX> am = sm.am[b][i];
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 if constexpr (MIX) {
@@ -482,12 +483,12 @@ __device__ __forceinline__ void ring_fwd_item(const RingTables& t, const RingOut
             __syncwarp();
             if (lane < nl) {
                 const double g = bg_n.y;
-                sm.bg[warp][lane] = bg_n;
+                sm.bg[lane] = bg_n;
 #pragma unroll
                 for (int b = 0; b < NB; ++b) {
-                    sm.ap[warp][b][lane] = to_coef<MIX>(make_double2(ap_n[b].x * g, ap_n[b].y * g));
+                    sm.ap[b][lane] = to_coef<MIX>(make_double2(ap_n[b].x * g, ap_n[b].y * g));
                     const double gs = g * sgn;
-                    sm.am[warp][b][lane] = to_coef<MIX>(make_double2(am_n[b].x * gs, am_n[b].y * gs));
+                    sm.am[b][lane] = to_coef<MIX>(make_double2(am_n[b].x * gs, am_n[b].y * gs));
                 }
             }
             __syncwarp();
@@ -501,7 +502,7 @@ __device__ __forceinline__ void ring_fwd_item(const RingTables& t, const RingOut
                     steps = 0;
                     if (l0 + blk * 8 + 7 < L) {
                         // leave the block: scale the state by g of its last degree, renormalise
-                        const double G = sm.bg[warp][blk * 8 + 7].y;
+                        const double G = sm.bg[blk * 8 + 7].y;
 #pragma unroll
                         for (int r = 0; r < R; ++r) {
                             q1[r] *= G;
@@ -599,11 +600,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
 ring_fwd_kernel(RingTables t, RingOut o, const RingItem* __restrict__ items, int nitems,
                 const int* __restrict__ jlo, const int* __restrict__ jhi,
                 const double2* __restrict__ alm, double2* __restrict__ out, int b0) {
-    __shared__ FwdSmem<NB, MIX> sm;
+    __shared__ FwdSmem<NB, MIX> sm[kWarpsPerBlock];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int it = blockIdx.x * kWarpsPerBlock + warp;
     if (it >= nitems) return;
-    ring_fwd_body<RMAX, NB, MIX>(t, o, items[it], jlo, jhi, alm, out, b0, sm, warp, lane);
+    ring_fwd_body<RMAX, NB, MIX>(t, o, items[it], jlo, jhi, alm, out, b0, sm[warp], warp, lane);
 }
 
 // the forward ring passes of many plans: item i belongs to plan items[i].slot
@@ -611,17 +612,17 @@ template <int RMAX, int NB, bool MIX>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32)
 ring_fwd_batch_kernel(const RingSlot* __restrict__ slots, const BatchItem* __restrict__ items,
                       int nitems, void* const* __restrict__ ptrs) {
-    __shared__ FwdSmem<NB, MIX> sm;
+    __shared__ FwdSmem<NB, MIX> sm[kWarpsPerBlock];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int it = blockIdx.x * kWarpsPerBlock + warp;
     if (it >= nitems) return;
     const BatchItem bi = items[it];
     const RingSlot& sl = slots[bi.slot];
-    const RingTables t = sl.t;
+    const RingTables t = sl.tf;
     const RingOut o = sl.o;
     ring_fwd_body<RMAX, NB, MIX>(t, o, bi.it, sl.jlo, sl.jhi,
-                                 static_cast<const double2*>(ptrs[sl.ptr]), sl.H, bi.b0, sm, warp,
-                                 lane);
+                                 static_cast<const double2*>(ptrs[sl.ptr]), sl.H, bi.b0, sm[warp],
+                                 warp, lane);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -630,17 +631,24 @@ ring_fwd_batch_kernel(const RingSlot* __restrict__ slots, const BatchItem* __res
 template <bool MIX> using RedT = std::conditional_t<MIX, float, double>;
 template <bool MIX> using RingDataT = std::conditional_t<MIX, float2, double2>;
 
-template <bool MIX>
+// One warp's staging (a block holds one per warp). SHF (one transform per pass): each degree's
+// four partial sums go through two shuffle stages first (lanes l, l ^ 16, then l ^ 8), after
+// which lane l holds component l >> 3 summed over the four lanes that share l & 7, and only that
+// value is staged: red8[degree slot][(l & 7) 4 + (l >> 3)], rows of 36 so that both the staging
+// and the reduction's reads fill each bank once
+template <bool MIX, bool SHF>
 struct AdjSmem {
-    RedT<MIX> red[kAdjWarps][32][33];
-    double2 bg[kAdjWarps][32];
+    RedT<MIX> red[SHF ? 1 : 32][33];
+    RedT<MIX> red8[SHF ? 8 : 1][36];
+    double2 bg[32];
 };
 
-template <int R, int NB, bool MIX>
+template <int R, int NB, bool MIX, bool SHF>
 __device__ __forceinline__ void ring_adj_item(const RingTables& t, const RingOut& o,
                                               const RingItem& item, const double2* __restrict__ in,
-                                              double* __restrict__ almd, int b0, bool sole,
-                                              AdjSmem<MIX>& sm, int warp, int lane) {
+                                              double* __restrict__ almd, int b0, int wmode,
+                                              AdjSmem<MIX, SHF>& sm, int warp, int lane) {
+    static_assert(!SHF || NB == 1, "the shuffle staging serves one transform per pass");
     constexpr int STRIDE = MIX ? 16 : 64;
     constexpr int NV = 4 * NB;   // (+m re, +m im, -m re, -m im) per transform
     constexpr int LB = 32 / NV;  // degrees per reduction block
@@ -755,8 +763,20 @@ __device__ __forceinline__ void ring_adj_item(const RingTables& t, const RingOut
                 }
             }
         }
+        if constexpr (SHF) {
+            const bool hi16 = (lane & 16) != 0, b8 = (lane & 8) != 0;
+            RT k0 = hi16 ? part[2] : part[0], k1 = hi16 ? part[3] : part[1];
+            const RT s0 = hi16 ? part[0] : part[2], s1 = hi16 ? part[1] : part[3];
+            k0 += __shfl_xor_sync(0xffffffffu, s0, 16);
+            k1 += __shfl_xor_sync(0xffffffffu, s1, 16);
+            RT kk = b8 ? k1 : k0;
+            const RT ss = b8 ? k0 : k1;
+            kk += __shfl_xor_sync(0xffffffffu, ss, 8);
+            sm.red8[slot][(lane & 7) * 4 + (lane >> 3)] = kk;
+        } else {
 #pragma unroll
-        for (int v = 0; v < NV; ++v) sm.red[warp][slot * NV + v][lane] = part[v];
+            for (int v = 0; v < NV; ++v) sm.red[slot * NV + v][lane] = part[v];
+        }
     };
     // reduce the staged degrees [lfirst, lfirst + cnt) over the lanes and write alm; degree
     // lfirst + i carries the factor g of its chunk slot gslot0 + i (1 for the seed degrees)
@@ -764,23 +784,37 @@ __device__ __forceinline__ void ring_adj_item(const RingTables& t, const RingOut
         __syncwarp();
         if (lane < cnt * NV) {
             const int li = lane / NV, v = lane % NV;
-            // four independent partial sums: the chain of dependent adds is 8 long, not 32
             RT s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+            if constexpr (SHF) {
+                // the eight lane groups' sums of component v of degree slot li
 #pragma unroll
-            for (int q = 0; q < 32; q += 4) {
-                s0 += sm.red[warp][lane][q];
-                s1 += sm.red[warp][lane][q + 1];
-                s2 += sm.red[warp][lane][q + 2];
-                s3 += sm.red[warp][lane][q + 3];
+                for (int k = 0; k < 8; k += 4) {
+                    s0 += sm.red8[li][k * 4 + v];
+                    s1 += sm.red8[li][(k + 1) * 4 + v];
+                    s2 += sm.red8[li][(k + 2) * 4 + v];
+                    s3 += sm.red8[li][(k + 3) * 4 + v];
+                }
+            } else {
+                // four independent partial sums: the chain of dependent adds is 8 long, not 32
+#pragma unroll
+                for (int q = 0; q < 32; q += 4) {
+                    s0 += sm.red[lane][q];
+                    s1 += sm.red[lane][q + 1];
+                    s2 += sm.red[lane][q + 2];
+                    s3 += sm.red[lane][q + 3];
+                }
             }
             double s = (double)((s0 + s1) + (s2 + s3));
-            if (gslot0 >= 0) s *= sm.bg[warp][gslot0 + li].y;
+            if (gslot0 >= 0) s *= sm.bg[gslot0 + li].y;
             const int l = lfirst + li;
             const int b = v >> 2, comp = v & 3;
             if (comp < 2 || m > 0) {
                 const int64_t idx = (l - m) + (comp < 2 ? cp : cm) + albs * (b0 + b);
                 double* dst = almd + 2 * idx + (comp & 1);
-                if (sole) *dst = s;
+                // 0: the only writer; 1: this warp wrote the value before (an earlier ring
+                // tile of the same item, the same lane): add in order; 2: other warps add too
+                if (wmode == 0) *dst = s;
+                else if (wmode == 1) *dst += s;
                 else atomicAdd(dst, s);
             }
         }
@@ -808,7 +842,7 @@ __device__ __forceinline__ void ring_adj_item(const RingTables& t, const RingOut
         lstart = m + 2;
     }
     auto rec = [&](int i) {
-        const double beta = sm.bg[warp][i].x;
+        const double beta = sm.bg[i].x;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const double qn = fma(x[r], q1[r], -(beta * q2[r]));
@@ -824,7 +858,7 @@ __device__ __forceinline__ void ring_adj_item(const RingTables& t, const RingOut
     for (int l0 = lstart; l0 <= item.lend; l0 += 32) {
         const int nl = min(32, item.lend - l0 + 1);
         __syncwarp();
-        if (lane < nl) sm.bg[warp][lane] = bg_next;
+        if (lane < nl) sm.bg[lane] = bg_next;
         __syncwarp();
         if (l0 + 32 + lane <= item.lend) bg_next = abm[l0 + 32 + lane - m - 2];
         const int nblk = nl / LB;
@@ -840,7 +874,7 @@ __device__ __forceinline__ void ring_adj_item(const RingTables& t, const RingOut
                 steps = 0;
                 if (l0 + blk * LB + LB - 1 < L) {
                     // leave the block: scale the state by g of its last degree, renormalise
-                    const double G = sm.bg[warp][blk * LB + LB - 1].y;
+                    const double G = sm.bg[blk * LB + LB - 1].y;
 #pragma unroll
                     for (int r = 0; r < R; ++r) {
                         q1[r] *= G;
@@ -882,35 +916,38 @@ __device__ __forceinline__ void ring_adj_item(const RingTables& t, const RingOut
     }
 }
 
-template <int RMAX, int NB, bool MIX>
+template <int RMAX, int NB, bool MIX, bool SHF>
 __device__ __forceinline__ void ring_adj_body(const RingTables& t, const RingOut& o,
                                               const RingItem& item, const double2* __restrict__ in,
                                               double* __restrict__ almd, int b0, int allow_sole,
-                                              AdjSmem<MIX>& sm, int warp, int lane) {
-    const bool multi = item.n > 32 * RMAX;
-    const bool sole = allow_sole && (item.flags & kItemSole) && !multi;
+                                              AdjSmem<MIX, SHF>& sm, int warp, int lane) {
+    // an item holding all retained rings of its order writes its degrees alone: its first ring
+    // tile stores them and the later ones add in order (deterministic); an order split over
+    // several items adds atomically into zeros
+    const bool whole = allow_sole && (item.flags & kItemSole);
     for (int base = 0; base < item.n; base += 32 * RMAX) {
+        const int wmode = whole ? (base == 0 ? 0 : 1) : 2;
         RingItem sub = item;
         sub.j0 = item.j0 + base;
         sub.n = min(32 * RMAX, item.n - base);
         if (sub.ck >= 0) sub.ck += base;
         const int reff = (sub.n + 31) >> 5;
-        if (RMAX >= 8 && reff >= 5) ring_adj_item<(RMAX >= 8 ? 8 : 1), NB, MIX>(t, o, sub, in, almd, b0, sole, sm, warp, lane);
-        else if (RMAX >= 4 && reff >= 3) ring_adj_item<(RMAX >= 4 ? 4 : 1), NB, MIX>(t, o, sub, in, almd, b0, sole, sm, warp, lane);
-        else if (RMAX >= 2 && reff == 2) ring_adj_item<(RMAX >= 2 ? 2 : 1), NB, MIX>(t, o, sub, in, almd, b0, sole, sm, warp, lane);
-        else ring_adj_item<1, NB, MIX>(t, o, sub, in, almd, b0, sole, sm, warp, lane);
+        if (RMAX >= 8 && reff >= 5) ring_adj_item<(RMAX >= 8 ? 8 : 1), NB, MIX, SHF>(t, o, sub, in, almd, b0, wmode, sm, warp, lane);
+        else if (RMAX >= 4 && reff >= 3) ring_adj_item<(RMAX >= 4 ? 4 : 1), NB, MIX, SHF>(t, o, sub, in, almd, b0, wmode, sm, warp, lane);
+        else if (RMAX >= 2 && reff == 2) ring_adj_item<(RMAX >= 2 ? 2 : 1), NB, MIX, SHF>(t, o, sub, in, almd, b0, wmode, sm, warp, lane);
+        else ring_adj_item<1, NB, MIX, SHF>(t, o, sub, in, almd, b0, wmode, sm, warp, lane);
     }
 }
 
-template <int RMAX, int NB, bool MIX>
+template <int RMAX, int NB, bool MIX, bool SHF>
 __global__ void __launch_bounds__(kAdjWarps * 32)
 ring_adj_kernel(RingTables t, RingOut o, const RingItem* __restrict__ items, int nitems,
                 const double2* __restrict__ in, double* __restrict__ almd, int b0, int allow_sole) {
-    __shared__ AdjSmem<MIX> sm;
+    __shared__ AdjSmem<MIX, SHF> sm[kAdjWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int it = blockIdx.x * kAdjWarps + warp;
     if (it >= nitems) return;
-    ring_adj_body<RMAX, NB, MIX>(t, o, items[it], in, almd, b0, allow_sole, sm, warp, lane);
+    ring_adj_body<RMAX, NB, MIX, SHF>(t, o, items[it], in, almd, b0, allow_sole, sm[warp], warp, lane);
 }
 
 // the adjoint ring passes of many plans: item i belongs to plan items[i].slot
@@ -918,7 +955,8 @@ template <int RMAX, int NB, bool MIX>
 __global__ void __launch_bounds__(kAdjWarps * 32)
 ring_adj_batch_kernel(const RingSlot* __restrict__ slots, const BatchItem* __restrict__ items,
                       int nitems, void* const* __restrict__ ptrs) {
-    __shared__ AdjSmem<MIX> sm;
+    constexpr bool SHF = NB == 1;
+    __shared__ AdjSmem<MIX, SHF> sm[kAdjWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int it = blockIdx.x * kAdjWarps + warp;
     if (it >= nitems) return;
@@ -926,8 +964,8 @@ ring_adj_batch_kernel(const RingSlot* __restrict__ slots, const BatchItem* __res
     const RingSlot& sl = slots[bi.slot];
     const RingTables t = sl.t;
     const RingOut o = sl.o;
-    ring_adj_body<RMAX, NB, MIX>(t, o, bi.it, sl.H, static_cast<double*>(ptrs[sl.ptr]), bi.b0,
-                                 sl.allow_sole, sm, warp, lane);
+    ring_adj_body<RMAX, NB, MIX, SHF>(t, o, bi.it, sl.H, static_cast<double*>(ptrs[sl.ptr]), bi.b0,
+                                      sl.allow_sole, sm[warp], warp, lane);
 }
 
 // zero what the adjoint does not overwrite: padding rows of every column, the orders the
@@ -959,8 +997,12 @@ template <int RMAX, int NB, bool MIX>
 static int launch_adj(const RingTables& t, const RingOut& o, const RingItem* items, int nitems,
                       const double2* in, double2* alm, int b0, int allow_sole, cudaStream_t s) {
     const int grid = (nitems + kAdjWarps - 1) / kAdjWarps;
-    ring_adj_kernel<RMAX, NB, MIX><<<grid, kAdjWarps * 32, 0, s>>>(
-        t, o, items, nitems, in, reinterpret_cast<double*>(alm), b0, allow_sole);
+    if (NB == 1 && !getenv("PFSHT_ADJ_OLD"))
+        ring_adj_kernel<RMAX, NB, MIX, NB == 1><<<grid, kAdjWarps * 32, 0, s>>>(
+            t, o, items, nitems, in, reinterpret_cast<double*>(alm), b0, allow_sole);
+    else
+        ring_adj_kernel<RMAX, NB, MIX, false><<<grid, kAdjWarps * 32, 0, s>>>(
+            t, o, items, nitems, in, reinterpret_cast<double*>(alm), b0, allow_sole);
     return check_launch("ring_adj_kernel");
 }
 
@@ -1035,8 +1077,9 @@ int ring_adjoint(const RingTables& t, const RingOut& o, const RingItems& it, con
 
 // item lists of one ring set: tiles of 32 * rmax rings, the order flags, the device tables
 int build_ring_items(const std::vector<int>& jlo, const std::vector<int>& jhi, int L, int mmax,
-                     int rmax, RingItemsOwner& own, cudaStream_t s, const RingSegments* seg) {
-    std::vector<RingItem> items = make_ring_items(jlo, jhi, L, mmax, 32 * rmax, seg);
+                     int rmax, RingItemsOwner& own, cudaStream_t s, const RingSegments* seg,
+                     int tile) {
+    std::vector<RingItem> items = make_ring_items(jlo, jhi, L, mmax, tile > 0 ? tile : 32 * rmax, seg);
     std::vector<unsigned char> sole(L + 1, 0);
     for (const RingItem& r : items)
         if (r.flags & kItemSole) sole[r.m] = 1;

@@ -46,3 +46,21 @@ def test_stretch_apply_matches_oracle(pf, O, cuda, L):
     a_ref = ref.adjoint(g, nthreads=8)[:, :, 0]
     assert O.alm_reldiff(a, a_ref, L) < 1e-10
     assert dot_rel(f, g, alm[:, :, 0], a) < 1e-12
+
+
+def test_ring_adjoint_is_deterministic(pf, O, cuda):
+    # the reference's threaded adjoint ring pass equals its serial one bit for bit
+    # (test/test_backends.jl:202-259): here every order's retained rings sit in one item whose
+    # warp adds its ring tiles' sums in a fixed order, so two passes agree bit for bit
+    rng = np.random.default_rng(13)
+    L = 1024
+    th, ph = cap_points(100000, rng=rng)
+    plan = pf.Plan(th, ph, lmax=L, tol=1e-8)
+    n = plan.info["nrings"]
+    Gr = to_dev(np.asfortranarray(cn(rng, n, 2 * L + 1, 1)))
+    out = []
+    for _ in range(2):
+        a = to_dev(np.zeros((L + 1, 2 * L + 1, 1), np.complex128, order="F"))
+        pf.ring_adjoint(plan, Gr, a)
+        out.append(to_host(a))
+    assert np.array_equal(out[0], out[1])

@@ -191,6 +191,21 @@ def test_host_buffers_equal_device_applies(pf, O, cuda, L, B):
     assert hb["d2h_forward"] == hb["h2d_adjoint"] == len(th) * 16 * B
 
 
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-8), ("mixed", 1e-6)])
+def test_adjoint_is_deterministic(pf, O, cuda, precision, tol):
+    # spreading runs its bins in colours whose tiles are disjoint (plain adds, fixed order) and
+    # the ring pass holds each order's rings in one warp: two adjoints agree bit for bit, as the
+    # reference's threaded and serial adjoints do (test/test_backends.jl:202-259)
+    rng = np.random.default_rng(43)
+    L = 512
+    th, ph = cap_points(50000, rng=rng)
+    ps = pf.Plan(th, ph, lmax=L, tol=tol, precision=precision)
+    g = to_dev(cn(rng, len(th)))
+    a1 = to_host(ps.H * g)
+    a2 = to_host(ps.H * g)
+    assert np.array_equal(a1, a2)
+
+
 def test_forward_is_deterministic(pf, O, cuda):
     # the forward path has no atomics: two applies agree bit for bit
     rng = np.random.default_rng(41)
