@@ -84,7 +84,9 @@ typedef struct pfsht_opts {
                                    transforms spin-s fields with coefficients sa_lm at
                                    l + (lmax+1)(m+lmax) (src/Layout.jl:28-29), the ring pass in
                                    FP64 whatever the precision mode */
-    int32_t reserved[2];
+    int32_t nufft_transpose;    /* NUFFT fine-row transposes: 0 = TMA-staged tiles where the grid
+                                   layout allows (plain loads for the rest), 1 = plain loads only */
+    int32_t reserved[1];
 } pfsht_opts;
 
 typedef struct pfsht_plan pfsht_plan;
@@ -314,6 +316,11 @@ const char* pfsht_stage_name(int32_t stage);
  * caller. */
 pfsht_status pfsht_direct_forward_noalloc(const double* theta, const double* phi, int64_t npts,
                                           int32_t lmax, const void* alm, void* f, void* stream);
+
+/* Number of bounded device-side waits (the TMA tile loads of the NUFFT row transposes) that gave
+ * up on the current device since the library was loaded (no reference counterpart). A kernel
+ * whose wait runs out records it here, skips that tile and returns; 0 means every wait ended. */
+pfsht_status pfsht_wait_timeouts(int32_t* count);
 
 /* Thread-local message of the last failing call; returns its length. */
 size_t pfsht_last_error(char* buf, size_t len);

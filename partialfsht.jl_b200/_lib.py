@@ -25,7 +25,7 @@ class Opts(C.Structure):
                 ("oversample_phi", C.c_double), ("eps_apo_max", C.c_double),
                 ("ring_segment_degrees", C.c_int32), ("nufft_fft_lengths", C.c_int32),
                 ("nufft_nf1", C.c_int32), ("nufft_nf2", C.c_int32), ("maxboxes", C.c_int32),
-                ("spin", C.c_int32), ("reserved", C.c_int32 * 2)]
+                ("spin", C.c_int32), ("nufft_transpose", C.c_int32), ("reserved", C.c_int32 * 1)]
 
 
 class Box(C.Structure):
@@ -60,6 +60,7 @@ SIGNATURES = {
     "pfsht_adjoint": (C.c_int, [_vp, _vp, _vp, _vp]),
     "pfsht_forward_host": (C.c_int, [_vp, _vp, _vp]),
     "pfsht_adjoint_host": (C.c_int, [_vp, _vp, _vp]),
+    "pfsht_wait_timeouts": (C.c_int, [C.POINTER(C.c_int32)]),
     "pfsht_ring_forward": (C.c_int, [_vp, _vp, _vp, _vp]),
     "pfsht_ring_adjoint": (C.c_int, [_vp, _vp, _vp, _vp]),
     "pfsht_ring_work": (C.c_int64, [_vp]),

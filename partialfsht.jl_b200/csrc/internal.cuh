@@ -1,5 +1,6 @@
 // Internal declarations shared by the CUDA sources of libpfsht_b200.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <cufft.h>
 
@@ -282,6 +283,10 @@ struct NufftGrid {
     // grid does not allow it and rows add atomically
     int ncolors = 0;
     std::vector<int> color_off;  // ncolors + 1 offsets into NufftDev::sorder
+    // the fine columns that hold no mode column: one run [gap_lo, gap_hi) (gap_ok), which the
+    // TMA row transposes zero directly
+    int gap_lo = 0, gap_hi = 0, gap_ok = 0;
+    int plain_transpose = 0;   // 1: the plain-load transposes only
 };
 
 struct NufftDev {
@@ -299,8 +304,15 @@ struct NufftDev {
     DevBuf U;         // double2 nrows x nf2 x B
     cufftHandle f1 = 0, f2 = 0;
     bool have_f1 = false, have_f2 = false;
+    // 2-D tensor maps of pad (nf1 x ncols B) and U (nf2 x nrows B) for the TMA row transposes
+    alignas(64) CUtensorMap pad_map;
+    alignas(64) CUtensorMap U_map;
+    bool have_maps = false;
     ~NufftDev();
 };
+
+// bounded device-side waits that gave up (the TMA row transposes), on the current device
+int tma_timeouts(int* out);
 
 // transform points (x = stretched colatitude, y = longitude; both radians) into grid
 // coordinates, sort them into bins, fill pts/perm/binstart. x,y are device arrays.

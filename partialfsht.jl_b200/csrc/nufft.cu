@@ -27,6 +27,7 @@
 
 #include "es_horner_table.h"
 #include "internal.cuh"
+#include "tma.cuh"
 
 namespace pf {
 
@@ -406,6 +407,11 @@ int nufft_alloc(NufftGrid& g, NufftDev& d, int B) {
     int n2[1] = {g.nf2};
     PF_CUFFT(cufftPlanMany(&d.f2, 1, n2, n2, 1, g.nf2, n2, 1, g.nf2, ty, g.nrows * B));
     d.have_f2 = true;
+    // tensor maps for the TMA row transposes (the plain kernels serve when the driver has no
+    // encoder or the layout does not fit one)
+    d.have_maps = g.gap_ok && !g.plain_transpose &&
+                  make_tile_map(&d.pad_map, d.pad.p, (int)el, g.nf1, (int64_t)g.ncols * B, 128 / (int)el, 32) == 0 &&
+                  make_tile_map(&d.U_map, d.U.p, (int)el, g.nf2, (int64_t)g.nrows * B, 128 / (int)el, 32) == 0;
     return 0;
 }
 
@@ -545,6 +551,151 @@ __global__ void rows_adj_kernel(const cx<T>* __restrict__ U, int nf1, int ncols,
         const int p1 = p0 + threadIdx.x;
         if (c < ncols && p1 < nf1) pb[p1 + (int64_t)nf1 * c] = tile[threadIdx.x][k];
     }
+}
+
+// ---------------------------------------------------------------------------------------
+// the same transposes with TMA-staged tiles: a block per 32 x 32 tile loads it into shared
+// memory with 2-D tensor copies (128-byte lines, 128-byte swizzle so that the transposed reads
+// fill each bank once), waits on an mbarrier (bounded) and writes the transposed tile with
+// coalesced stores. Tiles whose rows wrap around the fine grid, or whose columns are not one
+// contiguous run (or, for 8-byte elements, start on an odd element), are read with plain loads.
+// ---------------------------------------------------------------------------------------
+constexpr int kTmaWaitLimit = 1 << 20;
+
+// U[r, p2] = pad[(row0 + r) mod nf1, p2col[p2]]; blocks past the tiles zero the fine columns
+// [gap_lo, gap_hi) that hold no mode column (the only such columns)
+template <class T>
+__global__ void __launch_bounds__(256)
+rows_fwd_tma_kernel(const __grid_constant__ CUtensorMap pmap, const cx<T>* __restrict__ pad,
+                    int nf1, int ncols, int row0, int nrows, int nf2,
+                    const int* __restrict__ colp2, int gap_lo, int gap_hi, int ntc, int ntr,
+                    cx<T>* __restrict__ U) {
+    constexpr int E = sizeof(cx<T>);  // 16 (FP64) or 8 (FP32) bytes
+    constexpr int SUB = 128 / E;       // fine rows per 128-byte line
+    constexpr int NSUB = 32 / SUB;     // line blocks per 32-row tile
+    __shared__ __align__(1024) unsigned char tile[NSUB][32 * 128];
+    __shared__ __align__(8) uint64_t bar;
+    const int b = blockIdx.z, tx = threadIdx.x, ty = threadIdx.y;
+    cx<T>* ub = U + (int64_t)nrows * nf2 * b;
+    const int ntiles = ntc * ntr;
+    if ((int)blockIdx.x >= ntiles) {
+        const int zr = ((int)blockIdx.x - ntiles) * 32;
+        const cx<T> z = Cx<T>::make(0, 0);
+        for (int r = zr + ty; r < min(zr + 32, nrows); r += 8)
+            for (int p2 = gap_lo + tx; p2 < gap_hi; p2 += 32) ub[(int64_t)r * nf2 + p2] = z;
+        return;
+    }
+    const int c0 = ((int)blockIdx.x % ntc) * 32, r0 = ((int)blockIdx.x / ntc) * 32;
+    const int p0 = row0 + r0;
+    const bool tma = p0 >= 0 && p0 + 32 <= nf1 && (E == 16 || (p0 & 1) == 0);
+    if (tma) {
+        if (tx == 0 && ty == 0) {
+            mbar_init(&bar, 1);
+            mbar_expect_tx(&bar, NSUB * 32 * 128);
+#pragma unroll
+            for (int j = 0; j < NSUB; ++j)
+                tma_load_2d(tile[j], &pmap, &bar, (p0 + j * SUB) * (E / 8), c0 + ncols * b);
+        }
+        __syncthreads();
+        if (!mbar_wait_bounded(&bar, 0, kTmaWaitLimit)) return;
+    }
+    const int c = c0 + tx;
+    if (c >= ncols) return;
+    const int p2 = colp2[c];
+    for (int rr = ty; rr < 32; rr += 8) {
+        const int r = r0 + rr;
+        if (r >= nrows) break;
+        cx<T> v;
+        if (tma) {
+            v = *reinterpret_cast<const cx<T>*>(tile[rr / SUB] + swz128(tx, (rr % SUB) * E));
+        } else {
+            int p1 = (row0 + r) % nf1;
+            if (p1 < 0) p1 += nf1;
+            v = pad[p1 + (int64_t)nf1 * (c + (int64_t)ncols * b)];
+        }
+        ub[(int64_t)r * nf2 + p2] = v;
+    }
+}
+
+// pad[p1, c] = U[(p1 - row0) mod nf1, colp2[c]] when that row is kept, else 0
+template <class T>
+__global__ void __launch_bounds__(256)
+rows_adj_tma_kernel(const __grid_constant__ CUtensorMap umap, const cx<T>* __restrict__ U,
+                    int nf1, int ncols, int row0, int nrows, int nf2,
+                    const int* __restrict__ colp2, int ntc, cx<T>* __restrict__ pad) {
+    constexpr int E = sizeof(cx<T>);
+    constexpr int SUB = 128 / E;  // fine columns per 128-byte line
+    constexpr int NSUB = 32 / SUB;
+    __shared__ __align__(1024) unsigned char tile[NSUB][32 * 128];
+    __shared__ __align__(8) uint64_t bar;
+    const int b = blockIdx.z, tx = threadIdx.x, ty = threadIdx.y;
+    const int c0 = ((int)blockIdx.x % ntc) * 32, p0 = ((int)blockIdx.x / ntc) * 32;
+    // kept rows of the tile: r = (p1 - row0) mod nf1, one run when it does not wrap
+    int rf = (p0 - row0) % nf1;
+    if (rf < 0) rf += nf1;
+    const int ncv = min(32, ncols - c0);
+    const int q0 = colp2[c0];
+    // the tile's columns are one run of fine columns
+    const bool run = __syncthreads_and(tx >= ncv || colp2[c0 + tx] == q0 + tx) != 0;
+    const bool tma = run && rf + 32 <= nf1 && rf < nrows && (E == 16 || (q0 & 1) == 0);
+    if (tma) {
+        if (tx == 0 && ty == 0) {
+            mbar_init(&bar, 1);
+            mbar_expect_tx(&bar, NSUB * 32 * 128);
+#pragma unroll
+            for (int j = 0; j < NSUB; ++j)
+                tma_load_2d(tile[j], &umap, &bar, (q0 + j * SUB) * (E / 8), rf + nrows * b);
+        }
+        __syncthreads();
+        if (!mbar_wait_bounded(&bar, 0, kTmaWaitLimit)) return;
+    }
+    const int p1 = p0 + tx;
+    if (p1 >= nf1) return;
+    const int r = tma ? rf + tx : ((p1 - row0) % nf1 + nf1) % nf1;
+    const cx<T>* ub = U + (int64_t)nrows * nf2 * b;
+    for (int k = ty; k < ncv; k += 8) {
+        const int c = c0 + k;
+        cx<T> v = Cx<T>::make(0, 0);
+        if (r < nrows) {
+            if (tma) v = *reinterpret_cast<const cx<T>*>(tile[k / SUB] + swz128(tx, (k % SUB) * E));
+            else v = ub[(int64_t)r * nf2 + colp2[c]];
+        }
+        pad[p1 + (int64_t)nf1 * (c + (int64_t)ncols * b)] = v;
+    }
+}
+
+int tma_timeouts(int* out) {
+    PF_CUDA(cudaMemcpyFromSymbol(out, g_tma_timeouts, sizeof(int)));
+    return 0;
+}
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                   const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                   const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+int make_tile_map(CUtensorMap* map, void* base, int esize, int64_t inner, int64_t outer,
+                  int box_inner, int box_outer) {
+    static EncodeTiledFn fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<EncodeTiledFn>(f);
+    }();
+    if (!fn || esize % 8 != 0 || ((uintptr_t)base & 15) != 0) return 1;
+    // 8-byte units: the complex values move as (re, im) pairs of 8-byte words
+    const int u = esize / 8;
+    const cuuint64_t dims[2] = {(cuuint64_t)(inner * u), (cuuint64_t)outer};
+    const cuuint64_t strides[1] = {(cuuint64_t)(inner * esize)};
+    const cuuint32_t box[2] = {(cuuint32_t)(box_inner * u), (cuuint32_t)box_outer};
+    const cuuint32_t estr[2] = {1, 1};
+    if (strides[0] % 16 != 0 || box[0] * 8 != 128) return 1;
+    return fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, base, dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS
+               ? 0 : 1;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -1455,7 +1606,15 @@ static int type2_impl(const NufftGrid& g, NufftDev& d, const double2* modes, dou
     PF_CUFFT(cufftSetStream(d.f1, s));
     PF_TRY(fine_fft(d.f1, d.pad.p, g.fp32, dir));
     clock_mark(clk, kStFft1Fwd, s);
-    {
+    if (d.have_maps) {
+        const int ntc = (g.ncols + 31) / 32, ntr = (g.nrows + 31) / 32;
+        const int nz = g.gap_hi > g.gap_lo ? ntr : 0;
+        dim3 grid(ntc * ntr + nz, 1, B);
+        rows_fwd_tma_kernel<T><<<grid, dim3(32, 8), 0, s>>>(
+            d.pad_map, d.pad.as<cx<T>>(), g.nf1, g.ncols, g.row0, g.nrows, g.nf2,
+            d.colp2.as<int>(), g.gap_lo, g.gap_hi, ntc, ntr, d.U.as<cx<T>>());
+        PF_TRY(check_launch("rows_fwd_tma_kernel"));
+    } else {
         dim3 grid((g.nf2 + 31) / 32, (g.nrows + 31) / 32, B);
         rows_fwd_kernel<T><<<grid, dim3(32, 8), 0, s>>>(d.pad.as<cx<T>>(), g.nf1, g.ncols, g.row0,
                                                         g.nrows, g.nf2, d.p2col.as<int>(),
@@ -1480,7 +1639,14 @@ static int type1_impl(const NufftGrid& g, NufftDev& d, const double2* f, double2
     PF_CUFFT(cufftSetStream(d.f2, s));
     PF_TRY(fine_fft(d.f2, d.U.p, g.fp32, dir));
     clock_mark(clk, kStFft2Adj, s);
-    {
+    if (d.have_maps) {
+        const int ntc = (g.ncols + 31) / 32, ntp = (g.nf1 + 31) / 32;
+        dim3 grid(ntc * ntp, 1, B);
+        rows_adj_tma_kernel<T><<<grid, dim3(32, 8), 0, s>>>(
+            d.U_map, d.U.as<cx<T>>(), g.nf1, g.ncols, g.row0, g.nrows, g.nf2, d.colp2.as<int>(),
+            ntc, d.pad.as<cx<T>>());
+        PF_TRY(check_launch("rows_adj_tma_kernel"));
+    } else {
         dim3 grid((g.ncols + 31) / 32, (g.nf1 + 31) / 32, B);
         rows_adj_kernel<T><<<grid, dim3(32, 8), 0, s>>>(d.U.as<cx<T>>(), g.nf1, g.ncols, g.row0,
                                                         g.nrows, g.nf2, d.colp2.as<int>(),

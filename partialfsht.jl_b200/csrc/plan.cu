@@ -132,6 +132,20 @@ int setup_nufft_grid(NufftGrid& g, NufftDev& d, int n1, int nmodes2, const std::
         colp2[c] = p2;
         p2col[p2] = c;
     }
+    // the fine columns without a mode column form one run when the mode columns are the two
+    // ends of the fine grid (non-negative k2 first, negative k2 last)
+    {
+        int lo = g.nf2, hi = -1, n = 0;
+        for (int q = 0; q < g.nf2; ++q)
+            if (p2col[q] < 0) {
+                lo = std::min(lo, q);
+                hi = std::max(hi, q);
+                ++n;
+            }
+        g.gap_lo = n ? lo : 0;
+        g.gap_hi = n ? hi + 1 : 0;
+        g.gap_ok = (n == 0 || hi + 1 - lo == n) ? 1 : 0;
+    }
     PF_TRY(upload(d.mult1, mult1, s));
     PF_TRY(upload(d.dec2, dec2, s));
     PF_TRY(upload(d.colp2, colp2, s));
@@ -317,6 +331,7 @@ int build_stretch(pfsht_plan* p, const double* d_theta, const double* d_phi, con
                             p->precision == PFSHT_PRECISION_MIXED, o.nufft_fft_lengths, o.nufft_nf1,
                             o.nufft_nf2, s));
     PF_TRY(nufft_setpts(p->ng, p->nd, Th.as<double>(), ph.as<double>(), s));
+    p->ng.plain_transpose = o.nufft_transpose == 1 ? 1 : 0;
     PF_TRY(nufft_alloc(p->ng, p->nd, B));
     return 0;
 }
@@ -955,6 +970,14 @@ pfsht_status pfsht_forward_host(pfsht_plan* p, const void* alm, void* f) {
 pfsht_status pfsht_adjoint_host(pfsht_plan* p, const void* f, void* alm) {
     if (!p || !alm || !f) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "NULL argument");
     return (pfsht_status)host_apply(p, f, alm, false);
+}
+
+pfsht_status pfsht_wait_timeouts(int32_t* count) {
+    if (!count) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "NULL argument");
+    int n = 0;
+    const int r = tma_timeouts(&n);
+    *count = n;
+    return (pfsht_status)r;
 }
 
 pfsht_status pfsht_ring_forward(pfsht_plan* p, const void* alm, void* G, void* stream) {

@@ -206,6 +206,26 @@ def test_adjoint_is_deterministic(pf, O, cuda, precision, tol):
     assert np.array_equal(a1, a2)
 
 
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-8), ("mixed", 1e-6)])
+def test_tma_transposes_equal_plain_ones(pf, O, cuda, precision, tol):
+    # the NUFFT's fine-row transposes with TMA-staged tiles move the same values as the plain-load
+    # kernels: both applies agree bit for bit; every bounded tile wait ended
+    import ctypes as C
+    rng = np.random.default_rng(45)
+    L = 700
+    th, ph = cap_points(60000, rng=rng)
+    pt = pf.Plan(th, ph, lmax=L, tol=tol, precision=precision)
+    pp = pf.Plan(th, ph, lmax=L, tol=tol, precision=precision, transpose="plain")
+    assert pt.info["nf1"] == pp.info["nf1"] and pt.info["nf2"] == pp.info["nf2"]
+    alm = O.rand_alm(L, rng=rng)
+    g = cn(rng, len(th))
+    assert np.array_equal(_fwd(pt, alm), _fwd(pp, alm))
+    assert np.array_equal(_adj(pt, g), _adj(pp, g))
+    n = C.c_int32(-1)
+    assert pf._lib.load().pfsht_wait_timeouts(C.byref(n)) == 0
+    assert n.value == 0
+
+
 def test_forward_is_deterministic(pf, O, cuda):
     # the forward path has no atomics: two applies agree bit for bit
     rng = np.random.default_rng(41)
