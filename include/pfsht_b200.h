@@ -124,9 +124,23 @@ pfsht_status pfsht_forward(pfsht_plan* plan, const void* alm, void* f, void* str
 pfsht_status pfsht_adjoint(pfsht_plan* plan, const void* f, void* alm, void* stream);
 
 /* The same two applies on host buffers: copies in, apply, copies out, synchronous.
- * The plan keeps staging buffers for this (src/Stretch.jl:393-410 role). */
+ * The plan keeps staging buffers for this (src/Stretch.jl:393-410 role), one set per direction.
+ * The coefficients cross in blocks of orders, and the ring pass of a block runs while the next
+ * block is copied (in for the forward, out for the adjoint). */
 pfsht_status pfsht_forward_host(pfsht_plan* plan, const void* alm, void* f);
 pfsht_status pfsht_adjoint_host(pfsht_plan* plan, const void* f, void* alm);
+
+/* The host-buffer applies without waiting for them (no reference counterpart; mul! on host
+ * arrays returns with the result, these let a caller with independent inputs keep the link busy):
+ * the compute is enqueued on `stream` (NULL = the plan's own stream) and the copies on the plan's
+ * two copy streams, one per direction, so a forward's field copy out can run beside an adjoint's
+ * field copy in and compute. The outputs are complete, and the inputs free for reuse, once
+ * pfsht_host_sync returns. Host buffers must be page-locked (cudaHostAlloc / cudaHostRegister) for
+ * the copies to overlap. One plan's host applies run in the order issued. */
+pfsht_status pfsht_forward_host_async(pfsht_plan* plan, const void* alm, void* f, void* stream);
+pfsht_status pfsht_adjoint_host_async(pfsht_plan* plan, const void* f, void* alm, void* stream);
+/* Waits for every host-buffer apply of the plan issued so far. */
+pfsht_status pfsht_host_sync(pfsht_plan* plan);
 
 /* Bytes the two host-buffer applies move across PCIe per call (no reference counterpart):
  * the coefficient array travels as the sph_mode staircase of the orders the plan retains

@@ -348,6 +348,30 @@ class Plan:
             _lib.check(lib.pfsht_adjoint_host(self._h, _ptr(f), _ptr(alm)), "mul!")
         return alm
 
+    def mul_async(self, f, alm):
+        """mul!(f, plan, alm) on page-locked host arrays without waiting: the result is in f
+        once host_sync() returns (pfsht_forward_host_async)."""
+        _check_array(alm, _coeff_shapes(self.lmax, self.ntrans), "coefficient array")
+        _check_array(f, _field_shapes(self.npts, self.ntrans), "field")
+        if (_is_torch(alm) and alm.is_cuda) or (_is_torch(f) and f.is_cuda):
+            raise ValueError("mul_async takes host arrays")
+        _lib.check(_lib.load().pfsht_forward_host_async(self._h, _ptr(alm), _ptr(f), None), "mul!")
+        return f
+
+    def mul_adjoint_async(self, alm, f):
+        """mul!(alm, plan', f) on page-locked host arrays without waiting; alm is complete once
+        host_sync() returns (pfsht_adjoint_host_async)."""
+        _check_array(alm, _coeff_shapes(self.lmax, self.ntrans), "coefficient array")
+        _check_array(f, _field_shapes(self.npts, self.ntrans), "field")
+        if (_is_torch(alm) and alm.is_cuda) or (_is_torch(f) and f.is_cuda):
+            raise ValueError("mul_adjoint_async takes host arrays")
+        _lib.check(_lib.load().pfsht_adjoint_host_async(self._h, _ptr(f), _ptr(alm), None), "mul!")
+        return alm
+
+    def host_sync(self):
+        """Waits for the plan's host-buffer applies issued so far (pfsht_host_sync)."""
+        _lib.check(_lib.load().pfsht_host_sync(self._h), "host_sync")
+
     def __mul__(self, alm):
         """plan * alm (src/Plan.jl:190-193)."""
         dev = alm.device if (_is_torch(alm) and alm.is_cuda) else "cpu"

@@ -60,6 +60,9 @@ SIGNATURES = {
     "pfsht_adjoint": (C.c_int, [_vp, _vp, _vp, _vp]),
     "pfsht_forward_host": (C.c_int, [_vp, _vp, _vp]),
     "pfsht_adjoint_host": (C.c_int, [_vp, _vp, _vp]),
+    "pfsht_forward_host_async": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "pfsht_adjoint_host_async": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "pfsht_host_sync": (C.c_int, [_vp]),
     "pfsht_wait_timeouts": (C.c_int, [C.POINTER(C.c_int32)]),
     "pfsht_ring_forward": (C.c_int, [_vp, _vp, _vp, _vp]),
     "pfsht_ring_adjoint": (C.c_int, [_vp, _vp, _vp, _vp]),

@@ -179,7 +179,7 @@ void fill_info(pfsht_plan* p) {
             in.device_bytes += c->info.device_bytes;
         }
         in.device_bytes += (int64_t)(p->gidx.bytes + p->fg.bytes + p->acc.bytes + p->st_alm.bytes +
-                                     p->st_f.bytes);
+                                     p->st_f.bytes + p->st_alm2.bytes + p->st_f2.bytes);
         return;
     }
     if (p->kind == kDirect) {
@@ -216,7 +216,8 @@ void fill_info(pfsht_plan* p) {
                             &p->adj_seg.ck_p, &p->adj_seg.ck_E,
                             &p->H, &p->phi_pts, &p->nd.pts, &p->nd.perm, &p->nd.binstart,
                             &p->nd.colp2, &p->nd.p2col, &p->nd.mult1, &p->nd.dec2, &p->nd.pad,
-                            &p->nd.U, &p->st_alm, &p->st_f, &p->ab_fwd})
+                            &p->nd.U, &p->st_alm, &p->st_f, &p->ab_fwd, &p->st_alm2,
+                            &p->st_f2, &p->blk_fwd_items, &p->blk_adj_items})
         bytes += (int64_t)b->bytes;
     in.device_bytes = bytes;
 }
@@ -856,13 +857,13 @@ static void host_bytes(const pfsht_plan* p, int64_t* alm_bytes, int64_t* f_bytes
     *f_bytes = (int64_t)sizeof(double2) * p->M * p->B;
 }
 
-static int alm_copy(pfsht_plan* p, void* host, bool to_device, cudaStream_t s) {
+static int alm_copy(pfsht_plan* p, void* host, double2* dev, bool to_device, cudaStream_t s) {
     const int L = p->L;
     const int mu = host_mmax(p);
     const size_t col = sizeof(double2) * (size_t)(L + 1);
     const size_t tr = col * (2 * L + 1);
     char* h = static_cast<char*>(host);
-    char* d = p->st_alm.as<char>();
+    char* d = reinterpret_cast<char*>(dev);
     if (p->spin != 0) {
         // columns m + lmax for m = -mu .. mu, contiguous in each transform
         const size_t off = col * (size_t)(L - mu), n = col * (size_t)(2 * mu + 1);
@@ -913,27 +914,174 @@ static void alm_zero_host_padding(const pfsht_plan* p, void* host) {
 
 namespace pf {
 
+// copy order block k of the coefficient staircase (all transforms) between host and device
+static int alm_copy_block(pfsht_plan* p, const AlmBlock& k, void* host, double2* dev, bool to_device,
+                          cudaStream_t s) {
+    const int L = p->L;
+    const size_t col = sizeof(double2) * (size_t)(L + 1);
+    const size_t tr = col * (2 * L + 1);
+    char* h = static_cast<char*>(host);
+    char* d = reinterpret_cast<char*>(dev);
+    for (int b = 0; b < p->B; ++b) {
+        const size_t off = tr * b + col * k.c0;
+        const size_t width = sizeof(double2) * (size_t)k.rows;
+        if (to_device)
+            PF_CUDA(cudaMemcpy2DAsync(d + off, col, h + off, col, width, k.c1 - k.c0,
+                                      cudaMemcpyHostToDevice, s));
+        else
+            PF_CUDA(cudaMemcpy2DAsync(h + off, col, d + off, col, width, k.c1 - k.c0,
+                                      cudaMemcpyDeviceToHost, s));
+    }
+    return 0;
+}
+
+// ring items grouped by the order blocks of the host copies, each group in its launch order
+static int group_items_by_block(pfsht_plan* p, const std::vector<RingItem>& items,
+                                const std::vector<AlmBlock>& blocks, DevBuf& out,
+                                std::vector<int>& off) {
+    std::vector<RingItem> v;
+    v.reserve(items.size());
+    off.assign(blocks.size() + 1, 0);
+    for (size_t k = 0; k < blocks.size(); ++k) {
+        const int m0 = (blocks[k].c0 + 1) / 2, m1 = (blocks[k].c1 + 1) / 2;
+        for (const RingItem& it : items)
+            if (it.m >= m0 && it.m < m1) v.push_back(it);
+        off[k + 1] = (int)v.size();
+    }
+    if (v.size() != items.size()) return fail(PFSHT_ERR_ARGUMENT, "ring items outside the copied orders");
+    PF_TRY(out.alloc(sizeof(RingItem) * std::max<size_t>(v.size(), 1)));
+    if (!v.empty())
+        PF_CUDA(cudaMemcpyAsync(out.p, v.data(), sizeof(RingItem) * v.size(), cudaMemcpyHostToDevice,
+                                p->st_stream));
+    PF_CUDA(cudaStreamSynchronize(p->st_stream));
+    return 0;
+}
+
 int plan_host_staging(pfsht_plan* p) {
     const size_t na = sizeof(double2) * (size_t)(p->L + 1) * (2 * p->L + 1) * p->B;
     const size_t nf = sizeof(double2) * (size_t)p->M * p->B;
     if (!p->st_alm.p) PF_TRY(p->st_alm.alloc(na));
     if (!p->st_f.p) PF_TRY(p->st_f.alloc(nf));
+    if (!p->st_alm2.p) PF_TRY(p->st_alm2.alloc(na));
+    if (!p->st_f2.p) PF_TRY(p->st_f2.alloc(nf));
+    if (!p->h2d) {
+        PF_CUDA(cudaStreamCreateWithFlags(&p->h2d, cudaStreamNonBlocking));
+        PF_CUDA(cudaStreamCreateWithFlags(&p->d2h, cudaStreamNonBlocking));
+        for (cudaEvent_t* e : {&p->ev_alm_in_free, &p->ev_f_out_free, &p->ev_f_in_free,
+                               &p->ev_alm_out_free, &p->ev_fwd_done, &p->ev_f_in_ready, &p->ev_copied})
+            PF_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    }
+    // the blocked ring passes: stretched scalar leaves (spin, Direct and MultiBox plans copy
+    // whole and apply on the compute stream)
+    const bool blocked = p->kind != kDirect && p->kind != kMultiBox && p->spin == 0;
+    if (blocked && !p->host_pipeline) {
+        const std::vector<AlmBlock> blocks = alm_blocks(p->L, host_mmax(p));
+        PF_TRY(group_items_by_block(p, p->fwd_items.host, blocks, p->blk_fwd_items, p->blk_fwd_off));
+        PF_TRY(group_items_by_block(p, p->adj_items.host, blocks, p->blk_adj_items, p->blk_adj_off));
+        p->ev_blk.assign(blocks.size(), nullptr);
+        for (cudaEvent_t& e : p->ev_blk) PF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        p->host_pipeline = true;
+    }
     return 0;
 }
 
-int plan_host_enqueue(pfsht_plan* p, const void* in, void* out, bool fwd, cudaStream_t s) {
+// the forward from host coefficients: each order block's copy on h2d, joined by an event before
+// the ring items of its orders on s; the field copied back on d2h once the forward ends
+static int host_forward_pipelined(pfsht_plan* p, const void* in, void* out, cudaStream_t s) {
+    const std::vector<AlmBlock> blocks = alm_blocks(p->L, host_mmax(p));
+    const size_t nf = sizeof(double2) * (size_t)p->M * p->B;
+    double2* alm = p->st_alm.as<double2>();
+    // the previous forward's ring pass has finished reading the staging coefficients
+    PF_CUDA(cudaStreamWaitEvent(p->h2d, p->ev_alm_in_free, 0));
+    for (size_t k = 0; k < blocks.size(); ++k) {
+        PF_TRY(alm_copy_block(p, blocks[k], const_cast<void*>(in), alm, true, p->h2d));
+        PF_CUDA(cudaEventRecord(p->ev_blk[k], p->h2d));
+    }
+    clock_begin(&p->clk, s);
+    for (size_t k = 0; k < blocks.size(); ++k) {
+        PF_CUDA(cudaStreamWaitEvent(s, p->ev_blk[k], 0));
+        RingItems v = p->fwd_items.view;
+        v.items = p->blk_fwd_items.as<RingItem>() + p->blk_fwd_off[k];
+        v.nitems = p->blk_fwd_off[k + 1] - p->blk_fwd_off[k];
+        PF_TRY(ring_forward(p->rt_fwd, p->ro_cols, v, alm, p->H.as<double2>(), p->B, s));
+    }
+    clock_mark(&p->clk, kStRingFwd, s);
+    PF_CUDA(cudaEventRecord(p->ev_alm_in_free, s));
+    // the previous forward's field has left the staging buffer
+    PF_CUDA(cudaStreamWaitEvent(s, p->ev_f_out_free, 0));
+    PF_TRY(plan_forward_after_ring(p, p->st_f.as<double2>(), s));
+    PF_CUDA(cudaEventRecord(p->ev_fwd_done, s));
+    PF_CUDA(cudaStreamWaitEvent(p->d2h, p->ev_fwd_done, 0));
+    PF_CUDA(cudaMemcpyAsync(out, p->st_f.p, nf, cudaMemcpyDeviceToHost, p->d2h));
+    PF_CUDA(cudaEventRecord(p->ev_f_out_free, p->d2h));
+    return 0;
+}
+
+// the adjoint to host coefficients: the field copied in on h2d; each order block's ring items on
+// s, then that block's coefficients copied out on d2h while the next block computes
+static int host_adjoint_pipelined(pfsht_plan* p, const void* in, void* out, cudaStream_t s) {
+    const std::vector<AlmBlock> blocks = alm_blocks(p->L, host_mmax(p));
+    const size_t nf = sizeof(double2) * (size_t)p->M * p->B;
+    double2* alm = p->st_alm2.as<double2>();
+    PF_CUDA(cudaStreamWaitEvent(p->h2d, p->ev_f_in_free, 0));
+    PF_CUDA(cudaMemcpyAsync(p->st_f2.p, in, nf, cudaMemcpyHostToDevice, p->h2d));
+    PF_CUDA(cudaEventRecord(p->ev_f_in_ready, p->h2d));
+    // the output zero fill on the side stream, once the previous adjoint's copies have left
+    PF_CUDA(cudaEventRecord(p->ev_fork, s));
+    PF_CUDA(cudaStreamWaitEvent(p->side, p->ev_fork, 0));
+    PF_CUDA(cudaStreamWaitEvent(p->side, p->ev_alm_out_free, 0));
+    PF_TRY(ring_adjoint_prepare(p->rt, p->adj_items.view, alm, p->B, p->side));
+    PF_CUDA(cudaEventRecord(p->ev_join, p->side));
+    clock_begin(&p->clk, s);
+    PF_CUDA(cudaStreamWaitEvent(s, p->ev_f_in_ready, 0));
+    PF_TRY(plan_adjoint_before_ring(p, p->st_f2.as<double2>(), s));
+    PF_CUDA(cudaEventRecord(p->ev_f_in_free, s));
+    PF_CUDA(cudaStreamWaitEvent(s, p->ev_join, 0));
+    for (size_t k = 0; k < blocks.size(); ++k) {
+        RingItems v = p->adj_items.view;
+        v.items = p->blk_adj_items.as<RingItem>() + p->blk_adj_off[k];
+        v.nitems = p->blk_adj_off[k + 1] - p->blk_adj_off[k];
+        PF_TRY(ring_adjoint(p->rt, p->ro_cols, v, p->H.as<double2>(), alm, p->B, s, false));
+        PF_CUDA(cudaEventRecord(p->ev_blk[k], s));
+        PF_CUDA(cudaStreamWaitEvent(p->d2h, p->ev_blk[k], 0));
+        PF_TRY(alm_copy_block(p, blocks[k], out, alm, false, p->d2h));
+    }
+    clock_mark(&p->clk, kStRingAdj, s);
+    PF_CUDA(cudaEventRecord(p->ev_alm_out_free, p->d2h));
+    return 0;
+}
+
+int plan_host_enqueue(pfsht_plan* p, const void* in, void* out, bool fwd, cudaStream_t s,
+                      bool order_on_s) {
     PF_TRY(plan_host_staging(p));
     const size_t nf = sizeof(double2) * (size_t)p->M * p->B;
-    if (fwd) {
-        // the forward reads rows 0 .. lmax - m of each order only
-        PF_TRY(alm_copy(p, const_cast<void*>(in), true, s));
-        PF_TRY(apply_forward(p, p->st_alm.as<double2>(), p->st_f.as<double2>(), s));
-        PF_CUDA(cudaMemcpyAsync(out, p->st_f.p, nf, cudaMemcpyDeviceToHost, s));
+    if (p->host_pipeline) {
+        if (fwd) {
+            PF_TRY(host_forward_pipelined(p, in, out, s));
+        } else {
+            PF_TRY(host_adjoint_pipelined(p, in, out, s));
+            alm_zero_host_padding(p, out);
+        }
     } else {
-        PF_CUDA(cudaMemcpyAsync(p->st_f.p, in, nf, cudaMemcpyHostToDevice, s));
-        PF_TRY(apply_adjoint(p, p->st_f.as<double2>(), p->st_alm.as<double2>(), s));
-        PF_TRY(alm_copy(p, out, false, s));
-        alm_zero_host_padding(p, out);
+        // whole copies around the apply on the compute stream
+        PF_CUDA(cudaStreamWaitEvent(s, p->ev_copied, 0));
+        if (fwd) {
+            PF_TRY(alm_copy(p, const_cast<void*>(in), p->st_alm.as<double2>(), true, s));
+            PF_TRY(apply_forward(p, p->st_alm.as<double2>(), p->st_f.as<double2>(), s));
+            PF_CUDA(cudaMemcpyAsync(out, p->st_f.p, nf, cudaMemcpyDeviceToHost, s));
+        } else {
+            PF_CUDA(cudaMemcpyAsync(p->st_f2.p, in, nf, cudaMemcpyHostToDevice, s));
+            PF_TRY(apply_adjoint(p, p->st_f2.as<double2>(), p->st_alm2.as<double2>(), s));
+            PF_TRY(alm_copy(p, out, p->st_alm2.as<double2>(), false, s));
+            alm_zero_host_padding(p, out);
+        }
+        // the plan's d2h stream marks the end of every host apply
+        PF_CUDA(cudaEventRecord(p->ev_copied, s));
+        PF_CUDA(cudaStreamWaitEvent(p->d2h, p->ev_copied, 0));
+    }
+    if (order_on_s) {
+        PF_CUDA(cudaEventRecord(p->ev_copied, p->d2h));
+        PF_CUDA(cudaStreamWaitEvent(s, p->ev_copied, 0));
     }
     return 0;
 }
@@ -970,6 +1118,34 @@ pfsht_status pfsht_forward_host(pfsht_plan* p, const void* alm, void* f) {
 pfsht_status pfsht_adjoint_host(pfsht_plan* p, const void* f, void* alm) {
     if (!p || !alm || !f) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "NULL argument");
     return (pfsht_status)host_apply(p, f, alm, false);
+}
+
+static int host_apply_async(pfsht_plan* p, const void* in, void* out, bool fwd, void* stream) {
+    DeviceGuard dg(p->device);
+    cudaStream_t s = stream ? (cudaStream_t)stream : p->st_stream;
+    return plan_host_enqueue(p, in, out, fwd, s, false);
+}
+
+pfsht_status pfsht_forward_host_async(pfsht_plan* p, const void* alm, void* f, void* stream) {
+    if (!p || !alm || !f) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "NULL argument");
+    return (pfsht_status)host_apply_async(p, alm, f, true, stream);
+}
+
+pfsht_status pfsht_adjoint_host_async(pfsht_plan* p, const void* f, void* alm, void* stream) {
+    if (!p || !alm || !f) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "NULL argument");
+    return (pfsht_status)host_apply_async(p, f, alm, false, stream);
+}
+
+static int host_sync(pfsht_plan* p) {
+    if (!p->d2h) return 0;  // no host apply was issued
+    DeviceGuard dg(p->device);
+    PF_CUDA(cudaStreamSynchronize(p->d2h));
+    return 0;
+}
+
+pfsht_status pfsht_host_sync(pfsht_plan* p) {
+    if (!p) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "NULL plan");
+    return (pfsht_status)host_sync(p);
 }
 
 pfsht_status pfsht_wait_timeouts(int32_t* count) {

@@ -47,9 +47,23 @@ struct pfsht_plan {
     NufftDev nd;
     // direct leaf
     DevBuf phi_pts;
-    // host-buffer staging
-    DevBuf st_alm, st_f;
+    // host-buffer staging: st_alm / st_f serve the forward (coefficients in, field out),
+    // st_alm2 / st_f2 the adjoint (field in, coefficients out), so that a forward's output copy
+    // and an adjoint's input copy (or the next call's) can be in flight while the other computes
+    DevBuf st_alm, st_f, st_alm2, st_f2;
     cudaStream_t st_stream = nullptr;
+    // host copies run on their own streams, one per direction of the link, ordered against the
+    // compute stream by events; blk_* hold the ring items grouped by the order blocks in which
+    // the coefficients cross (items of block k at [off[k], off[k + 1]), heaviest first in each),
+    // so the ring pass of one block runs while the next block is copied
+    cudaStream_t h2d = nullptr, d2h = nullptr;
+    cudaEvent_t ev_alm_in_free = nullptr, ev_f_out_free = nullptr, ev_f_in_free = nullptr,
+                ev_alm_out_free = nullptr, ev_fwd_done = nullptr, ev_f_in_ready = nullptr,
+                ev_copied = nullptr;
+    std::vector<cudaEvent_t> ev_blk;
+    DevBuf blk_fwd_items, blk_adj_items;
+    std::vector<int> blk_fwd_off, blk_adj_off;
+    bool host_pipeline = false;  // the blocked host path is set up
     // the adjoint zeroes its output on `side` while the NUFFT and Theta-FFT stages run
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
@@ -67,6 +81,12 @@ struct pfsht_plan {
         if (side) cudaStreamDestroy(side);
         if (ev_fork) cudaEventDestroy(ev_fork);
         if (ev_join) cudaEventDestroy(ev_join);
+        if (h2d) cudaStreamDestroy(h2d);
+        if (d2h) cudaStreamDestroy(d2h);
+        for (cudaEvent_t e : {ev_alm_in_free, ev_f_out_free, ev_f_in_free, ev_alm_out_free,
+                              ev_fwd_done, ev_f_in_ready, ev_copied})
+            if (e) cudaEventDestroy(e);
+        for (cudaEvent_t e : ev_blk) cudaEventDestroy(e);
         for (cudaEvent_t e : clk.ev) cudaEventDestroy(e);
     }
 };
@@ -91,10 +111,13 @@ int plan_forward_after_ring(pfsht_plan* p, double2* f, cudaStream_t s);
 int plan_adjoint_before_ring(pfsht_plan* p, const double2* f, cudaStream_t s);
 
 // The host-buffer apply without its final synchronisation: copies in (the coefficient
-// staircase or the field), applies on the plan's staging buffers and copies out, all on `s`;
-// for the adjoint it also zeroes the host array's padding rows on host threads before it
-// returns. The host arrays must stay valid until `s` reaches this point.
-int plan_host_enqueue(pfsht_plan* p, const void* in, void* out, bool fwd, cudaStream_t s);
+// staircase or the field), applies on the plan's staging buffers and copies out. The compute
+// runs on `s`, the copies on the plan's h2d / d2h streams; with order_on_s the end of the output
+// copy is ordered before whatever is enqueued on `s` afterwards, otherwise only the plan's d2h
+// stream (pfsht_host_sync) marks it. For the adjoint it also zeroes the host array's padding rows
+// on host threads before it returns. The host arrays must stay valid until the copies end.
+int plan_host_enqueue(pfsht_plan* p, const void* in, void* out, bool fwd, cudaStream_t s,
+                      bool order_on_s = true);
 // allocate the plan's staging buffers for host-buffer applies
 int plan_host_staging(pfsht_plan* p);
 

@@ -4,12 +4,14 @@
 // A server owns `nslots` streams. Plans are registered against an HBM budget: a plan counts
 // its own device memory and the staging buffers that requests on host arrays go through, and a
 // registration that would exceed the budget is refused. Requests queue in arrival order; a
-// worker thread admits a request as soon as a stream is free and its plan is idle (requests for
-// the same plan share its buffers, so they run one after the other; requests for different
-// plans overlap: one's copies in with another's kernels and a third's copies out). Each admitted
-// request is enqueued on its stream as copy in -> apply -> copy out, followed by a host callback
-// that marks it done, frees its stream and plan and wakes the worker, so requests that arrive
-// while others are on the GPU start as soon as resources free up.
+// worker thread admits a request as soon as a stream is free and its plan is idle, together with
+// the requests for the same plan queued behind it (up to kMaxGroup): the group's applies run on
+// one stream one after the other, since they share the plan's buffers, while their copies run on
+// the plan's own copy streams, so one request's copies in and out overlap its neighbours' kernels
+// (requests for different plans overlap as well: one's copies with another's kernels). Each
+// admitted request is enqueued as copy in -> apply -> copy out, and a host callback on the plan's
+// copy-out stream marks it done; the group's last one frees its stream and plan and wakes the
+// worker, so requests that arrive while others are on the GPU start as soon as resources free up.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -37,6 +39,7 @@ struct pfsht_server {
     std::vector<pfsht_plan*> plans;
     std::vector<int64_t> plan_bytes;
     std::vector<char> plan_busy;
+    std::vector<int> plan_left;  // requests of the plan's admitted group still running
     std::vector<cudaStream_t> slots;
     std::vector<char> slot_busy;
     std::deque<Request*> pending;
@@ -58,6 +61,7 @@ namespace {
 using namespace pf;
 
 enum { kPending = 0, kRunning = 1, kDone = 2, kFailed = 3 };
+constexpr int kMaxGroup = 8;  // same-plan requests admitted together
 
 struct Request {
     pfsht_server* srv = nullptr;
@@ -84,20 +88,24 @@ void CUDART_CB request_done(void* arg) {
         std::lock_guard<std::mutex> lk(s->mu);
         r->t_done = s->now();
         r->state = kDone;
-        s->plan_busy[r->plan] = 0;
-        s->slot_busy[r->slot] = 0;
         s->running -= 1;
         s->completed += 1;
+        if (--s->plan_left[r->plan] == 0) {
+            s->plan_busy[r->plan] = 0;
+            s->slot_busy[r->slot] = 0;
+        }
     }
     s->cv_work.notify_one();
     s->cv_done.notify_all();
 }
 
+// one request of an admitted group: the apply on the group's stream, the copies on the plan's
+// copy streams, and the completion after the request's copy out (on the plan's copy-out stream)
 int launch(pfsht_server* s, Request* r) {
     pfsht_plan* p = s->plans[r->plan];
     cudaStream_t st = s->slots[r->slot];
-    PF_TRY(plan_host_enqueue(p, r->in, r->out, r->fwd != 0, st));
-    PF_CUDA(cudaLaunchHostFunc(st, request_done, r));
+    PF_TRY(plan_host_enqueue(p, r->in, r->out, r->fwd != 0, st, false));
+    PF_CUDA(cudaLaunchHostFunc(p->d2h, request_done, r));
     return 0;
 }
 
@@ -105,7 +113,8 @@ void worker_main(pfsht_server* s) {
     cudaSetDevice(s->device);
     std::unique_lock<std::mutex> lk(s->mu);
     for (;;) {
-        // admit in arrival order, skipping requests whose plan is busy
+        // admit in arrival order, skipping requests whose plan is busy; an admitted request
+        // takes the requests queued behind it for the same plan along
         for (auto it = s->pending.begin(); it != s->pending.end();) {
             const auto fs = std::find(s->slot_busy.begin(), s->slot_busy.end(), 0);
             if (fs == s->slot_busy.end()) break;
@@ -114,26 +123,46 @@ void worker_main(pfsht_server* s) {
                 ++it;
                 continue;
             }
-            it = s->pending.erase(it);
-            r->slot = (int)(fs - s->slot_busy.begin());
-            s->slot_busy[r->slot] = 1;
+            const int slot = (int)(fs - s->slot_busy.begin());
+            std::vector<Request*> group;
+            for (auto jt = it; jt != s->pending.end() && (int)group.size() < kMaxGroup;) {
+                if ((*jt)->plan == r->plan) {
+                    group.push_back(*jt);
+                    jt = s->pending.erase(jt);
+                } else {
+                    ++jt;
+                }
+            }
+            s->slot_busy[slot] = 1;
             s->plan_busy[r->plan] = 1;
-            s->running += 1;
-            r->state = kRunning;
-            r->t_start = s->now();
+            s->plan_left[r->plan] = (int)group.size();
+            s->running += (int)group.size();
+            const double t = s->now();
+            for (Request* g : group) {
+                g->slot = slot;
+                g->state = kRunning;
+                g->t_start = t;
+            }
             lk.unlock();
-            const int rc = launch(s, r);
+            size_t k = 0;
+            int rc = 0;
+            for (; k < group.size() && !rc; ++k) rc = launch(s, group[k]);
             std::string msg = rc ? get_error() : std::string();
             lk.lock();
             if (rc) {
-                // nothing of this request will run the callback: release it here
-                r->status = rc;
-                r->err = msg;
-                r->state = kFailed;
-                r->t_done = s->now();
-                s->plan_busy[r->plan] = 0;
-                s->slot_busy[r->slot] = 0;
-                s->running -= 1;
+                // the failed request and those after it run no callback: release them here
+                for (size_t q = k - 1; q < group.size(); ++q) {
+                    Request* g = group[q];
+                    g->status = rc;
+                    g->err = msg;
+                    g->state = kFailed;
+                    g->t_done = s->now();
+                    s->running -= 1;
+                    if (--s->plan_left[g->plan] == 0) {
+                        s->plan_busy[g->plan] = 0;
+                        s->slot_busy[g->slot] = 0;
+                    }
+                }
                 s->cv_done.notify_all();
             }
             it = s->pending.begin();  // the lock was released: start over
@@ -168,7 +197,8 @@ int server_add(pfsht_server* s, pfsht_plan* p, int32_t* id) {
     std::lock_guard<std::mutex> lk(s->mu);
     for (pfsht_plan* q : s->plans)
         if (q == p) return fail(PFSHT_ERR_ARGUMENT, "the plan is registered already");
-    const int64_t staging = (int64_t)sizeof(double2) *
+    // one coefficient array and one field per direction of the host copies
+    const int64_t staging = 2 * (int64_t)sizeof(double2) *
                             ((int64_t)(p->L + 1) * (2 * p->L + 1) + p->M) * p->B;
     const int64_t bytes = p->info.device_bytes + (p->st_alm.p ? 0 : staging);
     if (s->used + bytes > s->budget)
@@ -179,6 +209,7 @@ int server_add(pfsht_server* s, pfsht_plan* p, int32_t* id) {
     s->plans.push_back(p);
     s->plan_bytes.push_back(bytes);
     s->plan_busy.push_back(0);
+    s->plan_left.push_back(0);
     s->used += bytes;
     *id = (int32_t)(s->plans.size() - 1);
     return 0;

@@ -71,6 +71,31 @@ def test_results_alone_equal_results_in_the_mix(pf, O, cuda):
     srv.close()
 
 
+def test_requests_on_one_plan_run_as_a_group(pf, O, cuda):
+    # requests queued for one plan are admitted together and pipelined through the plan's copy
+    # streams (copies of one overlapping the kernels of its neighbours); each result equals the
+    # plan's own host-buffer apply of its input
+    rng = np.random.default_rng(72)
+    th, ph = cap_points(40000, rng=rng)
+    p = pf.Plan(th, ph, lmax=384, tol=1e-8)
+    srv = pf.Server(hbm_budget_gb=120, nslots=2)
+    pid = srv.add(p)
+    jobs = [(bool(k % 3), *_request(pf, O, p, bool(k % 3), rng)) for k in range(12)]
+    rids = [srv.submit(pid, fwd, inp, out) for fwd, inp, out in jobs]
+    for r in rids:
+        srv.wait(r)
+    for fwd, inp, out in jobs:
+        ref = np.zeros_like(out)
+        if fwd:
+            p.mul(ref, inp)
+            assert np.array_equal(out, ref)
+        else:
+            p.mul_adjoint(ref, inp)
+            assert O.alm_reldiff(out, ref, p.lmax) < 1e-13
+    assert srv.stats()["completed"] == 12
+    srv.close()
+
+
 def test_budget_refuses_plans(pf, O, cuda):
     rng = np.random.default_rng(71)
     th, ph = cap_points(20000, rng=rng)

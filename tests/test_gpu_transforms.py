@@ -226,6 +226,38 @@ def test_tma_transposes_equal_plain_ones(pf, O, cuda, precision, tol):
     assert n.value == 0
 
 
+@pytest.mark.parametrize("L,B", [(512, 1), (300, 2)])
+def test_async_host_applies_in_flight_together(pf, O, cuda, L, B):
+    # pfsht_forward_host_async / pfsht_adjoint_host_async: two rounds of a forward and an adjoint
+    # issued back to back on one plan before one wait; each result equals its device apply
+    import torch
+    rng = np.random.default_rng(44)
+    th, ph = cap_points(30000, rng=rng)
+    ps = pf.Plan(th, ph, lmax=L, tol=1e-8, ntrans=B)
+
+    def pinned(a):
+        t = torch.from_numpy(np.ascontiguousarray(np.asarray(a).T)).pin_memory()
+        return t.numpy().T
+
+    rounds = []
+    for _ in range(2):
+        alm = O.rand_alm(L, ntrans=B, rng=rng)
+        g = np.asfortranarray(cn(rng, len(th), B)) if B > 1 else cn(rng, len(th))
+        a_in = pinned(alm if B > 1 else alm[:, :, 0])
+        g_in = pinned(g)
+        f_out = pinned(np.zeros((len(th), B) if B > 1 else len(th), np.complex128))
+        a_out = pinned(np.full(alm.shape if B > 1 else alm.shape[:2], np.nan, np.complex128))
+        ps.mul_async(f_out, a_in)
+        ps.mul_adjoint_async(a_out, g_in)
+        rounds.append((alm, g, f_out, a_out))
+    ps.host_sync()
+    for alm, g, f_out, a_out in rounds:
+        assert np.array_equal(f_out, _fwd(ps, alm))
+        assert O.alm_reldiff(a_out, _adj(ps, g), L) < 1e-14
+        a3 = a_out if B > 1 else a_out[:, :, None]
+        assert np.all(a3[~O.valid_mask(L)] == 0)
+
+
 def test_forward_is_deterministic(pf, O, cuda):
     # the forward path has no atomics: two applies agree bit for bit
     rng = np.random.default_rng(41)
