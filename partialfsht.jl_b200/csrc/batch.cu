@@ -3,14 +3,16 @@
 //
 // One direction of a batch is one CUDA graph, captured on first use and replayed with a single
 // cudaGraphLaunch:
-//   forward : pointer table -> ring passes of all scalar plans (one launch per kernel shape,
-//             items of all plans heaviest first) -> per plan, on one of several streams: the
+//   forward : pointer table -> ring passes of all scalar plans (one persistent launch: warps
+//             pull the items of every plan and tile shape, heaviest first, from a counter) ->
+//             per plan, on one of several streams: the
 //             spin ring pass of a spin plan, FFT along Theta and NUFFT type 2 into the plan's
 //             own field buffer -> one copy kernel into the callers' fields
 //   adjoint : pointer table -> one copy kernel from the callers' fields -> per plan on the
 //             streams: NUFFT type 1, inverse FFT along Theta, zeroing of the caller's
 //             coefficient array (and a spin plan's own ring pass) -> ring passes of all scalar
-//             plans
+//             plans (one persistent launch; tiles of eight rings per lane, if a plan asks for
+//             them, run in launches of their own after it)
 // Callers' arrays are reached through a device pointer table that the graph's first node
 // copies from pinned host memory, so new arrays on each call need no new capture.
 #include <cuda_runtime.h>
@@ -49,7 +51,8 @@ struct pfsht_batch {
     int device = 0;
     int n = 0;
     std::vector<pfsht_plan*> plans;
-    std::vector<std::unique_ptr<pf::RingBatchGroup>> gf, ga;  // ring items per kernel shape
+    pf::RingMerged mf, ma;                                    // all ring items per direction
+    std::vector<std::unique_ptr<pf::RingBatchGroup>> gf, ga;  // shapes outside the merged launch
     pf::DevBuf slots;    // RingSlot[n]
     pf::DevBuf ptrs;     // void*[2n]: coefficient arrays, then fields
     void** ptrs_host = nullptr;  // pinned source of the table
@@ -93,7 +96,10 @@ int record(pfsht_batch* b, bool fwd) {
     double2* const* stf = b->stf.as<double2*>();
     PF_CUDA(cudaMemcpyAsync(b->ptrs.p, b->ptrs_host, sizeof(void*) * 2 * n,
                             cudaMemcpyHostToDevice, m));
-    if (fwd) PF_TRY(ring_forward_batch(slots, b->gf, ptrs, m));
+    if (fwd) {
+        PF_TRY(ring_merged_launch(slots, b->mf, false, ptrs, m));
+        PF_TRY(ring_forward_batch(slots, b->gf, ptrs, m));
+    }
     else {
         field_copy_kernel<<<b->nchunks, 256, 0, m>>>(b->chunks.as<FChunk>(), stf, ptrs, n, 0);
         PF_TRY(check_launch("field_copy_kernel"));
@@ -127,6 +133,7 @@ int record(pfsht_batch* b, bool fwd) {
         field_copy_kernel<<<b->nchunks, 256, 0, m>>>(b->chunks.as<FChunk>(), stf, ptrs, n, 1);
         PF_TRY(check_launch("field_copy_kernel"));
     } else {
+        PF_TRY(ring_merged_launch(slots, b->ma, true, ptrs, m));
         PF_TRY(ring_adjoint_batch(slots, b->ga, ptrs, m));
     }
     return 0;
@@ -233,8 +240,8 @@ int batch_create(pfsht_plan* const* plans, int n, int nstreams, pfsht_batch** ou
     PF_CUDA(cudaMemcpy(b->stf.p, stf.data(), sizeof(double2*) * n, cudaMemcpyHostToDevice));
     PF_CUDA(cudaMemcpy(b->chunks.p, chunks.data(), sizeof(FChunk) * chunks.size(),
                        cudaMemcpyHostToDevice));
-    PF_TRY(build_ring_batch(fw, false, b->gf, b->main));
-    PF_TRY(build_ring_batch(ad, true, b->ga, b->main));
+    PF_TRY(build_ring_merged(fw, false, b->mf, b->gf, b->main));
+    PF_TRY(build_ring_merged(ad, true, b->ma, b->ga, b->main));
     *out = b.release();
     return 0;
 }
@@ -269,8 +276,8 @@ pfsht_status pfsht_batch_info(const pfsht_batch* b, int32_t* ring_launches_fwd,
                               int32_t* ring_launches_adj, int64_t* graph_nodes_fwd,
                               int64_t* graph_nodes_adj) {
     if (!b) return (pfsht_status)fail(PFSHT_ERR_ARGUMENT, "NULL batch");
-    if (ring_launches_fwd) *ring_launches_fwd = (int32_t)b->gf.size();
-    if (ring_launches_adj) *ring_launches_adj = (int32_t)b->ga.size();
+    if (ring_launches_fwd) *ring_launches_fwd = (int32_t)b->gf.size() + (b->mf.nitems > 0 ? 1 : 0);
+    if (ring_launches_adj) *ring_launches_adj = (int32_t)b->ga.size() + (b->ma.nitems > 0 ? 1 : 0);
     if (graph_nodes_fwd) *graph_nodes_fwd = b->nodes[1];
     if (graph_nodes_adj) *graph_nodes_adj = b->nodes[0];
     return PFSHT_OK;

@@ -163,6 +163,13 @@ struct RingBatchPlan {
     const std::vector<RingItem>* items;
     int B, rmax, mix;
 };
+// all plans' items of one direction in one persistent launch (every tile shape, heaviest first)
+struct RingMerged {
+    DevBuf items;    // BatchItem[nitems], it.pad_ = shape code
+    DevBuf counter;  // next item to pull
+    int nitems = 0;
+    int grid = 1;    // resident blocks
+};
 // one group per kernel shape, items of all plans heaviest first
 int build_ring_batch(const std::vector<RingBatchPlan>& plans, bool adjoint,
                      std::vector<std::unique_ptr<RingBatchGroup>>& groups, cudaStream_t s);
@@ -171,6 +178,13 @@ int ring_forward_batch(const RingSlot* slots, const std::vector<std::unique_ptr<
                        void* const* ptrs, cudaStream_t s);
 int ring_adjoint_batch(const RingSlot* slots, const std::vector<std::unique_ptr<RingBatchGroup>>& groups,
                        void* const* ptrs, cudaStream_t s);
+// the merged list of one direction; shapes the persistent kernel does not take stay in `rest`
+// (launched per shape as above)
+int build_ring_merged(const std::vector<RingBatchPlan>& plans, bool adjoint, RingMerged& mg,
+                      std::vector<std::unique_ptr<RingBatchGroup>>& rest, cudaStream_t s);
+// zero the counter and launch the persistent pass (inside a capture: a memset node and a kernel)
+int ring_merged_launch(const RingSlot* slots, const RingMerged& mg, bool adjoint, void* const* ptrs,
+                       cudaStream_t s);
 // alm_prepare of one plan whose coefficient array is ptrs[ptr]
 int alm_prepare_ptr(void* const* ptrs, int ptr, int L, int B, const unsigned char* sole_m,
                     int allow_sole, cudaStream_t s);

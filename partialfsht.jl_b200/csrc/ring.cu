@@ -1232,6 +1232,147 @@ static int adj_batch_shape(const RingSlot* slots, const RingBatchGroup& g, void*
     return launch_adj_batch<2, 1, MIX>(slots, g, ptrs, s);
 }
 
+// ---------------------------------------------------------------------------------------
+// one persistent launch per direction for the ring passes of many plans: each warp pulls the next
+// item (any plan, any tile shape; all items heaviest first) from a counter in device memory until
+// none is left, and the item's shape code (RingItem::pad_) selects the pass it runs. A block
+// holds one staging area per warp, sized for the largest shape, so warps of one block may run
+// different shapes. No warp waits for another.
+// ---------------------------------------------------------------------------------------
+// forward shapes: (rings per lane, transforms per pass) = (1, 4), (2, 2), (4, 1), (2, 1); the
+// mixed form adds 4
+static int fwd_shape(int rmax, int nb, int mix) {
+    const int k = nb == 4 ? 0 : nb == 2 ? 1 : rmax >= 4 ? 2 : 3;
+    return k + 4 * (mix ? 1 : 0);
+}
+// adjoint shapes (one transform per pass): rings per lane 4 or 2; the mixed form adds 2
+static int adj_shape(int rmax, int mix) { return (rmax >= 4 ? 0 : 1) + 2 * (mix ? 1 : 0); }
+
+union FwdAnySmem {
+    FwdSmem<4, false> a;
+    FwdSmem<2, false> b;
+    FwdSmem<1, false> c;
+    FwdSmem<4, true> d;
+    FwdSmem<2, true> e;
+    FwdSmem<1, true> f;
+};
+union AdjAnySmem {
+    AdjSmem<false, true> a;
+    AdjSmem<true, true> b;
+};
+
+__device__ __forceinline__ int pull_item(int* counter, int lane) {
+    int it = 0;
+    if (lane == 0) it = atomicAdd(counter, 1);
+    return __shfl_sync(0xffffffffu, it, 0);
+}
+
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, 3)
+ring_fwd_persistent_kernel(const RingSlot* __restrict__ slots, const BatchItem* __restrict__ items,
+                           int nitems, void* const* __restrict__ ptrs, int* __restrict__ counter) {
+    __shared__ FwdAnySmem sm[kWarpsPerBlock];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int it = pull_item(counter, lane); it < nitems; it = pull_item(counter, lane)) {
+        const BatchItem bi = items[it];
+        const RingSlot& sl = slots[bi.slot];
+        const RingTables t = sl.tf;
+        const RingOut o = sl.o;
+        const double2* alm = static_cast<const double2*>(ptrs[sl.ptr]);
+        FwdAnySmem& w = sm[warp];
+        switch (bi.it.pad_) {
+            case 0: ring_fwd_body<1, 4, false>(t, o, bi.it, sl.jlo, sl.jhi, alm, sl.H, bi.b0, w.a, warp, lane); break;
+            case 1: ring_fwd_body<2, 2, false>(t, o, bi.it, sl.jlo, sl.jhi, alm, sl.H, bi.b0, w.b, warp, lane); break;
+            case 2: ring_fwd_body<4, 1, false>(t, o, bi.it, sl.jlo, sl.jhi, alm, sl.H, bi.b0, w.c, warp, lane); break;
+            case 3: ring_fwd_body<2, 1, false>(t, o, bi.it, sl.jlo, sl.jhi, alm, sl.H, bi.b0, w.c, warp, lane); break;
+            case 4: ring_fwd_body<1, 4, true>(t, o, bi.it, sl.jlo, sl.jhi, alm, sl.H, bi.b0, w.d, warp, lane); break;
+            case 5: ring_fwd_body<2, 2, true>(t, o, bi.it, sl.jlo, sl.jhi, alm, sl.H, bi.b0, w.e, warp, lane); break;
+            case 6: ring_fwd_body<4, 1, true>(t, o, bi.it, sl.jlo, sl.jhi, alm, sl.H, bi.b0, w.f, warp, lane); break;
+            default: ring_fwd_body<2, 1, true>(t, o, bi.it, sl.jlo, sl.jhi, alm, sl.H, bi.b0, w.f, warp, lane); break;
+        }
+        __syncwarp();
+    }
+}
+
+__global__ void __launch_bounds__(kAdjWarps * 32)
+ring_adj_persistent_kernel(const RingSlot* __restrict__ slots, const BatchItem* __restrict__ items,
+                           int nitems, void* const* __restrict__ ptrs, int* __restrict__ counter) {
+    __shared__ AdjAnySmem sm[kAdjWarps];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int it = pull_item(counter, lane); it < nitems; it = pull_item(counter, lane)) {
+        const BatchItem bi = items[it];
+        const RingSlot& sl = slots[bi.slot];
+        const RingTables t = sl.t;
+        const RingOut o = sl.o;
+        double* almd = static_cast<double*>(ptrs[sl.ptr]);
+        AdjAnySmem& w = sm[warp];
+        switch (bi.it.pad_) {
+            case 0: ring_adj_body<4, 1, false, true>(t, o, bi.it, sl.H, almd, bi.b0, sl.allow_sole, w.a, warp, lane); break;
+            case 1: ring_adj_body<2, 1, false, true>(t, o, bi.it, sl.H, almd, bi.b0, sl.allow_sole, w.a, warp, lane); break;
+            case 2: ring_adj_body<4, 1, true, true>(t, o, bi.it, sl.H, almd, bi.b0, sl.allow_sole, w.b, warp, lane); break;
+            default: ring_adj_body<2, 1, true, true>(t, o, bi.it, sl.H, almd, bi.b0, sl.allow_sole, w.b, warp, lane); break;
+        }
+        __syncwarp();
+    }
+}
+
+int build_ring_merged(const std::vector<RingBatchPlan>& plans, bool adjoint, RingMerged& mg,
+                      std::vector<std::unique_ptr<RingBatchGroup>>& rest, cudaStream_t s) {
+    std::vector<std::unique_ptr<RingBatchGroup>> groups;
+    PF_TRY(build_ring_batch(plans, adjoint, groups, s));
+    std::vector<std::pair<int64_t, BatchItem>> all;
+    rest.clear();
+    for (auto& g : groups) {
+        // the eight-rings-per-lane adjoint keeps its own launch (its register count would set
+        // every shape's occupancy)
+        if (adjoint && g->rmax >= 8) {
+            rest.push_back(std::move(g));
+            continue;
+        }
+        std::vector<BatchItem> v(g->nitems);
+        if (g->nitems)
+            PF_CUDA(cudaMemcpy(v.data(), g->items.p, sizeof(BatchItem) * v.size(), cudaMemcpyDeviceToHost));
+        const int code = adjoint ? adj_shape(g->rmax, g->mix) : fwd_shape(g->rmax, g->nb, g->mix);
+        for (BatchItem& b : v) {
+            b.it.pad_ = code;
+            const int64_t cost = (int64_t)((b.it.n + 31) / 32) * (b.it.lend - b.it.lbeg + 1) * g->nb;
+            all.push_back({cost, b});
+        }
+    }
+    std::stable_sort(all.begin(), all.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+    std::vector<BatchItem> items(all.size());
+    for (size_t i = 0; i < all.size(); ++i) items[i] = all[i].second;
+    mg.nitems = (int)items.size();
+    PF_TRY(mg.items.alloc(sizeof(BatchItem) * std::max<size_t>(items.size(), 1)));
+    PF_TRY(mg.counter.alloc(sizeof(int)));
+    if (!items.empty())
+        PF_CUDA(cudaMemcpy(mg.items.p, items.data(), sizeof(BatchItem) * items.size(), cudaMemcpyHostToDevice));
+    // one block per resident slot: the persistent grid
+    int dev = 0, sms = 148, per = 1;
+    PF_CUDA(cudaGetDevice(&dev));
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (adjoint)
+        PF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, ring_adj_persistent_kernel, kAdjWarps * 32, 0));
+    else
+        PF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, ring_fwd_persistent_kernel, kWarpsPerBlock * 32, 0));
+    const int wpb = adjoint ? kAdjWarps : kWarpsPerBlock;
+    mg.grid = std::max(1, std::min(sms * std::max(1, per), (mg.nitems + wpb - 1) / wpb));
+    return 0;
+}
+
+int ring_merged_launch(const RingSlot* slots, const RingMerged& mg, bool adjoint, void* const* ptrs,
+                       cudaStream_t s) {
+    if (mg.nitems == 0) return 0;
+    PF_CUDA(cudaMemsetAsync(mg.counter.p, 0, sizeof(int), s));
+    if (adjoint) {
+        ring_adj_persistent_kernel<<<mg.grid, kAdjWarps * 32, 0, s>>>(slots, mg.items.as<BatchItem>(),
+                                                                      mg.nitems, ptrs, mg.counter.as<int>());
+        return check_launch("ring_adj_persistent_kernel");
+    }
+    ring_fwd_persistent_kernel<<<mg.grid, kWarpsPerBlock * 32, 0, s>>>(slots, mg.items.as<BatchItem>(),
+                                                                       mg.nitems, ptrs, mg.counter.as<int>());
+    return check_launch("ring_fwd_persistent_kernel");
+}
+
 int ring_forward_batch(const RingSlot* slots, const std::vector<std::unique_ptr<RingBatchGroup>>& groups,
                        void* const* ptrs, cudaStream_t s) {
     for (const auto& g : groups) {
