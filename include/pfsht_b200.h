@@ -86,7 +86,10 @@ typedef struct pfsht_opts {
                                    FP64 whatever the precision mode */
     int32_t nufft_transpose;    /* NUFFT fine-row transposes: 0 = TMA-staged tiles where the grid
                                    layout allows (plain loads for the rest), 1 = plain loads only */
-    int32_t reserved[1];
+    int32_t deterministic;      /* 1: adjoints that are bitwise reproducible run to run (each order's
+                                   ring sums added in a fixed order by one warp, spreading bins
+                                   launched in colours whose tiles are disjoint); 0 (default): the
+                                   faster adjoint, whose atomic additions vary at round-off */
 } pfsht_opts;
 
 typedef struct pfsht_plan pfsht_plan;

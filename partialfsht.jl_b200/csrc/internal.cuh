@@ -292,9 +292,10 @@ struct NufftGrid {
     int fp32 = 0;              // fine grids, FFTs, spreading and interpolation in FP32
     int64_t M = 0;
     // spreading in bin colours: bins (br, bc) of one colour (br mod rcol, bc mod ccol) have
-    // disjoint tiles, so launching the colours one after the other lets every tile add its rows
-    // with plain loads and stores, in a fixed order (a deterministic type-1 NUFFT); 0 colours: the
-    // grid does not allow it and rows add atomically
+    // disjoint tiles, so launching the colours one after the other (deterministic != 0) lets
+    // every tile add its rows with plain loads and stores, in a fixed order (a deterministic
+    // type-1 NUFFT); 0 colours: the grid does not allow it and rows add atomically
+    int deterministic = 0;
     int ncolors = 0;
     std::vector<int> color_off;  // ncolors + 1 offsets into NufftDev::sorder
     // the fine columns that hold no mode column: one run [gap_lo, gap_hi) (gap_ok), which the

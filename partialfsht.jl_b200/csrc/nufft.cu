@@ -914,7 +914,7 @@ __global__ void __launch_bounds__(SpreadWarps<W>::N * 32)
 spread_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
               const int* __restrict__ binstart, const int* __restrict__ binorder, int nbusy,
               int nbc, int BR, int BC, int64_t M, const double2* __restrict__ fin, int b,
-              int nrows, int nf2, int row_wrap, cx<T>* __restrict__ U) {
+              int nrows, int nf2, int row_wrap, int plain, cx<T>* __restrict__ U) {
     constexpr int KP = SpreadStage<W, T>::KP;
     constexpr int NW = SpreadWarps<W>::N;
     __shared__ SpreadStage<W, T> stg[NW];
@@ -937,9 +937,17 @@ spread_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
         int gr = tg.tr0 + r;
         if (row_wrap) gr = wrap(gr, nrows);
         if (col_ok && gr >= 0 && gr < nrows && (v.x != 0.0 || v.y != 0.0)) {
-            T* qd = reinterpret_cast<T*>(ub + (int64_t)gr * nf2 + gcol);
-            atomicAdd(qd, v.x);
-            atomicAdd(qd + 1, v.y);
+            cx<T>* qd = ub + (int64_t)gr * nf2 + gcol;
+            if (plain) {
+                // no other tile of this launch reaches the cell (bins launched by colour)
+                cx<T> u = *qd;
+                u.x += v.x;
+                u.y += v.y;
+                *qd = u;
+            } else {
+                atomicAdd(reinterpret_cast<T*>(qd), v.x);
+                atomicAdd(reinterpret_cast<T*>(qd) + 1, v.y);
+            }
         }
     };
     if (lane == 0) {
@@ -1052,7 +1060,7 @@ __global__ void __launch_bounds__(128)
 spread16_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
                 const int* __restrict__ binstart, const int* __restrict__ binorder, int nbusy,
                 int nbc, int BR, int BC, int64_t M, const double2* __restrict__ fin, int b,
-                int nrows, int nf2, int row_wrap, cx<T>* __restrict__ U) {
+                int nrows, int nf2, int row_wrap, int plain, cx<T>* __restrict__ U) {
     constexpr int RH = Spread16Stage<W, T>::RH;
     constexpr int RP = Spread16Stage<W, T>::RP;
     __shared__ Spread16Stage<W, T> stg[4];
@@ -1075,9 +1083,17 @@ spread16_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
         int gr = tg.tr0 + r;
         if (row_wrap) gr = wrap(gr, nrows);
         if (col_ok && gr >= 0 && gr < nrows && (v.x != 0.0 || v.y != 0.0)) {
-            T* qd = reinterpret_cast<T*>(ub + (int64_t)gr * nf2 + gcol);
-            atomicAdd(qd, v.x);
-            atomicAdd(qd + 1, v.y);
+            cx<T>* qd = ub + (int64_t)gr * nf2 + gcol;
+            if (plain) {
+                // no other tile of this launch reaches the cell (bins launched by colour)
+                cx<T> u = *qd;
+                u.x += v.x;
+                u.y += v.y;
+                *qd = u;
+            } else {
+                atomicAdd(reinterpret_cast<T*>(qd), v.x);
+                atomicAdd(reinterpret_cast<T*>(qd) + 1, v.y);
+            }
         }
     };
     // add every row this half holds and clear the window
@@ -1165,344 +1181,8 @@ spread16_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
     if (rbase >= 0) flush_all();
 }
 
-// ---------------------------------------------------------------------------------------
-// Spreading and interpolation by pairs of points of one origin row (tiles of 16 columns,
-// w <= 10). One warp per bin; lane (h, c) = (lane / 16, lane % 16) owns tile column c. The
-// bin's points arrive sorted by origin row, and the warp takes them two at a time from one
-// origin row R: half 0 the first of the pair, half 1 the second (or none when the row has an
-// odd count left). Each lane keeps the W tile rows that points of origin row R reach, rows
-// [R, R + W), in registers, row r in slot r mod W; moving on to a later origin row frees
-// exactly the slots of the rows left behind, so no register ever moves. A point's row weights
-// are stored rotated to the slots (the weight of row r0 + a in slot (r0 + a) mod W), so its W
-// complex multiply-adds per lane use fixed registers. The slot of a finished row is picked by a
-// warp-uniform switch.
-// ---------------------------------------------------------------------------------------
-template <int W, class T>
-__device__ __forceinline__ cx<T> take_slot(cx<T> (&acc)[W], int sl) {
-    const cx<T> z = Cx<T>::make(0, 0);
-    cx<T> v = z;
-    switch (sl) {
-#define PF_SLOT(I)                  \
-    case I:                         \
-        if constexpr (I < W) {      \
-            v = acc[I < W ? I : 0]; \
-            acc[I < W ? I : 0] = z; \
-        }                           \
-        break;
-        PF_SLOT(0) PF_SLOT(1) PF_SLOT(2) PF_SLOT(3) PF_SLOT(4) PF_SLOT(5) PF_SLOT(6) PF_SLOT(7)
-        PF_SLOT(8) PF_SLOT(9) PF_SLOT(10) PF_SLOT(11) PF_SLOT(12) PF_SLOT(13) PF_SLOT(14)
-        PF_SLOT(15)
-#undef PF_SLOT
-        default: break;
-    }
-    return v;
-}
-
-template <int W, class T>
-__device__ __forceinline__ void put_slot(cx<T> (&win)[W], int sl, cx<T> v) {
-    switch (sl) {
-#define PF_SLOT(I)                                   \
-    case I:                                          \
-        if constexpr (I < W) win[I < W ? I : 0] = v; \
-        break;
-        PF_SLOT(0) PF_SLOT(1) PF_SLOT(2) PF_SLOT(3) PF_SLOT(4) PF_SLOT(5) PF_SLOT(6) PF_SLOT(7)
-        PF_SLOT(8) PF_SLOT(9) PF_SLOT(10) PF_SLOT(11) PF_SLOT(12) PF_SLOT(13) PF_SLOT(14)
-        PF_SLOT(15)
-#undef PF_SLOT
-        default: break;
-    }
-}
-
-template <class T>
-__device__ __forceinline__ cx<T> shfl_xor_cx(cx<T> v, int m) {
-    return Cx<T>::make(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m));
-}
-
-// the row weights of a point at offset v1, rotated to the slots of origin row r0 (>= 0)
-template <int W, class T>
-__device__ __forceinline__ void store_rotated_rows(T v1, int r0, T* __restrict__ k1s) {
-    T k1[W];
-    es_weights<W, T>(v1, k1);
-    const int rot = r0 % W;
-#pragma unroll
-    for (int a = 0; a < W; ++a) {
-        int sl = rot + a;
-        if (sl >= W) sl -= W;
-        k1s[sl] = k1[a];
-    }
-    if constexpr (W & 1) k1s[W] = (T)0;
-}
-
-template <int W, class T>
-struct SpreadPairStage {
-    static constexpr int KP = (W + 1) / 2;
-    cx<T> k1[32][KP];      // row weights by slot, as pairs (slots 2i, 2i + 1); odd tail 0
-    cx<T> vk[32][W + 1];   // value x column weight; slot W is 0 for lanes off the point
-    int2 org[32];          // origin row (or -1: skip) and column inside the tile
-};
-
-// Type-1 spreading. A finished tile row is added to U by half 0 after the halves' sums are
-// combined: with plain != 0 (the bins of one launch have disjoint tiles) by a plain load and
-// store, else atomically.
-template <int W, class T>
-__global__ void __launch_bounds__(128)
-spread_pair_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
-                   const int* __restrict__ binstart, const int* __restrict__ binorder, int nbusy,
-                   int nbc, int BR, int BC, int64_t M, const double2* __restrict__ fin, int b,
-                   int nrows, int nf2, int row_wrap, int plain, cx<T>* __restrict__ U) {
-    constexpr int KP = SpreadPairStage<W, T>::KP;
-    __shared__ SpreadPairStage<W, T> stg[4];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int h = lane >> 4, c = lane & 15;
-    const int slot = blockIdx.x * 4 + warp;
-    if (slot >= nbusy) return;
-    const int bin = binorder[slot];
-    const int s = binstart[bin], e = binstart[bin + 1];
-    const TileGeom tg = tile_geom<W>(bin, nbc, BR, BC);
-    SpreadPairStage<W, T>& st = stg[warp];
-    cx<T>* ub = U + (int64_t)nrows * nf2 * b;
-    const bool col_ok = c < tg.TC;
-    const int gcol = wrap(tg.tc0 + c, nf2);
-    cx<T> acc[W];
-#pragma unroll
-    for (int a = 0; a < W; ++a) acc[a] = Cx<T>::make(0, 0);
-    int R = -1;  // current origin row (tile-local); the window holds rows [R, R + W)
-    auto flush_row = [&](int rr) {
-        cx<T> v = take_slot<W, T>(acc, rr % W);
-        const cx<T> o = shfl_xor_cx<T>(v, 16);
-        v.x += o.x;
-        v.y += o.y;
-        int gr = tg.tr0 + rr;
-        if (row_wrap) gr = wrap(gr, nrows);
-        if (h == 0 && col_ok && gr >= 0 && gr < nrows && (v.x != (T)0 || v.y != (T)0)) {
-            cx<T>* qd = ub + (int64_t)gr * nf2 + gcol;
-            if (plain) {
-                // no other tile of this launch reaches the cell
-                cx<T> u = *qd;
-                u.x += v.x;
-                u.y += v.y;
-                *qd = u;
-            } else {
-                atomicAdd(reinterpret_cast<T*>(qd), v.x);
-                atomicAdd(reinterpret_cast<T*>(qd) + 1, v.y);
-            }
-        }
-    };
-    if (lane == 0) {
-#pragma unroll
-        for (int q = 0; q < 32; ++q) st.vk[q][W] = Cx<T>::make(0, 0);
-    }
-    for (int base = s; base < e; base += 32) {
-        const int nb = min(32, e - base);
-        __syncwarp();
-        if (lane < nb) {
-            const double2 g = pts[base + lane];
-            const double2 v = fin[perm[base + lane] + M * b];
-            int r0, c0;
-            double v1, v2;
-            local_origin<W>(g, tg, nrows, nf2, row_wrap, r0, c0, v1, v2);
-            const bool inside = r0 >= 0 && r0 + W <= tg.TR && c0 >= 0 && c0 + W <= tg.TC;
-            store_rotated_rows<W, T>((T)v1, inside ? r0 : 0, reinterpret_cast<T*>(st.k1[lane]));
-            T k2[W];
-            es_weights<W, T>((T)v2, k2);
-#pragma unroll
-            for (int a = 0; a < W; ++a) st.vk[lane][a] = Cx<T>::make((T)v.x * k2[a], (T)v.y * k2[a]);
-            st.org[lane] = make_int2(inside ? r0 : -1, c0);
-        }
-        __syncwarp();
-        int q = 0;
-        while (q < nb) {  // warp-uniform: every lane reads the same staged origins
-            const int r = st.org[q].x;
-            if (r < 0) {  // outside its bin's tile: cannot happen for binned points
-                ++q;
-                continue;
-            }
-            if (r != R) {
-                if (R >= 0) {
-                    const int n = min(r - R, W);
-                    for (int i = 0; i < n; ++i) flush_row(R + i);
-                }
-                R = r;
-            }
-            const bool two = q + 1 < nb && st.org[q + 1].x == r;
-            const bool mine = h == 0 || two;
-            const int qq = q + h * (two ? 1 : 0);
-            const unsigned dc = (unsigned)(c - st.org[qq].y);
-            const cx<T> vk = st.vk[qq][mine && dc < (unsigned)W ? dc : W];
-#pragma unroll
-            for (int p = 0; p < KP; ++p) {
-                const cx<T> kk = st.k1[qq][p];
-                acc[2 * p].x = fma(vk.x, kk.x, acc[2 * p].x);
-                acc[2 * p].y = fma(vk.y, kk.x, acc[2 * p].y);
-                if (2 * p + 1 < W) {
-                    constexpr int Z = 0;
-                    const int i1 = 2 * p + 1 < W ? 2 * p + 1 : Z;
-                    acc[i1].x = fma(vk.x, kk.y, acc[i1].x);
-                    acc[i1].y = fma(vk.y, kk.y, acc[i1].y);
-                }
-            }
-            q += two ? 2 : 1;
-        }
-    }
-    if (R >= 0) {
-        for (int i = 0; i < W; ++i) flush_row(R + i);
-    }
-}
-
-template <int W, class T>
-struct InterpPairStage {
-    static constexpr int KP = (W + 1) / 2;
-    cx<T> k1[32][KP];    // row weights by slot, as pairs; odd tail 0
-    T k2[32][W + 1];     // column weights; slot W is 0 for lanes off the point
-    int2 org[32];        // origin row (or -1: skip) and column inside the tile
-    int out[32];         // the point's index in the caller's order
-};
-
-// Type-2 interpolation: each lane holds the W tile rows of its column that points of the
-// current origin row reach (read from U as the origin row advances, the next row loaded ahead),
-// contracts them with a point's rotated row weights and multiplies by its column weight; the 16
-// lanes of a half then sum over the columns. Four steps (up to eight points) are summed at once
-// by a reduce-scatter through shuffles, after which lanes 4j of each half hold step j's value.
-template <int W, class T>
-__global__ void __launch_bounds__(128)
-interp_pair_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
-                   const int* __restrict__ binstart, const int* __restrict__ binorder, int nbusy,
-                   int nbc, int BR, int BC, int64_t M, const cx<T>* __restrict__ U, int nrows,
-                   int nf2, int row_wrap, int b, double2* __restrict__ f) {
-    constexpr int KP = InterpPairStage<W, T>::KP;
-    __shared__ InterpPairStage<W, T> stg[4];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int h = lane >> 4, c = lane & 15;
-    const int slot = blockIdx.x * 4 + warp;
-    if (slot >= nbusy) return;
-    const int bin = binorder[slot];
-    const int s = binstart[bin], e = binstart[bin + 1];
-    const TileGeom tg = tile_geom<W>(bin, nbc, BR, BC);
-    InterpPairStage<W, T>& st = stg[warp];
-    const cx<T>* ub = U + (int64_t)nrows * nf2 * b;
-    const bool col_ok = c < tg.TC;
-    const int gcol = wrap(tg.tc0 + c, nf2);
-    auto load_row = [&](int rr) -> cx<T> {
-        int gr = tg.tr0 + rr;
-        if (row_wrap) gr = wrap(gr, nrows);
-        if (col_ok && rr < tg.TR && gr >= 0 && gr < nrows) return ub[(int64_t)gr * nf2 + gcol];
-        return Cx<T>::make(0, 0);
-    };
-    cx<T> win[W];
-#pragma unroll
-    for (int a = 0; a < W; ++a) win[a] = Cx<T>::make(0, 0);
-    int R = -1;                     // current origin row; win holds rows [R, R + W)
-    cx<T> pre = Cx<T>::make(0, 0);  // row R + W, loaded ahead
-    if (lane == 0) {
-#pragma unroll
-        for (int q = 0; q < 32; ++q) st.k2[q][W] = (T)0;
-    }
-    for (int base = s; base < e; base += 32) {
-        const int nb = min(32, e - base);
-        __syncwarp();
-        if (lane < nb) {
-            const double2 g = pts[base + lane];
-            int r0, c0;
-            double v1, v2;
-            local_origin<W>(g, tg, nrows, nf2, row_wrap, r0, c0, v1, v2);
-            const bool inside = r0 >= 0 && r0 + W <= tg.TR && c0 >= 0 && c0 + W <= tg.TC;
-            store_rotated_rows<W, T>((T)v1, inside ? r0 : 0, reinterpret_cast<T*>(st.k1[lane]));
-            T k2[W];
-            es_weights<W, T>((T)v2, k2);
-#pragma unroll
-            for (int a = 0; a < W; ++a) st.k2[lane][a] = k2[a];
-            st.org[lane] = make_int2(inside ? r0 : -1, c0);
-            st.out[lane] = perm[base + lane];
-        }
-        __syncwarp();
-        int q = 0;
-        while (q < nb) {  // warp-uniform control throughout
-            cx<T> t[4];
-            int who[4];  // staged point of this half in step j, or -1
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                t[j] = Cx<T>::make(0, 0);
-                who[j] = -1;
-                // points outside their tile (cannot happen for binned points) interpolate 0
-                while (q < nb && st.org[q].x < 0) {
-                    f[st.out[q] + M * b] = make_double2(0.0, 0.0);
-                    ++q;
-                }
-                if (q < nb) {
-                    const int r = st.org[q].x;
-                    if (r != R) {
-                        if (R < 0 || r - R >= W) {
-#pragma unroll
-                            for (int a = 0; a < W; ++a) put_slot<W, T>(win, (r + a) % W, load_row(r + a));
-                        } else {
-                            put_slot<W, T>(win, (R + W) % W, pre);
-                            for (int rr = R + W + 1; rr < r + W; ++rr) put_slot<W, T>(win, rr % W, load_row(rr));
-                        }
-                        R = r;
-                        pre = load_row(R + W);
-                    }
-                    const bool two = q + 1 < nb && st.org[q + 1].x == r;
-                    const bool mine = h == 0 || two;
-                    const int qq = q + h * (two ? 1 : 0);
-                    const unsigned dc = (unsigned)(c - st.org[qq].y);
-                    const T kc = st.k2[qq][mine && dc < (unsigned)W ? dc : W];
-                    cx<T> sr = Cx<T>::make(0, 0);
-#pragma unroll
-                    for (int p = 0; p < KP; ++p) {
-                        const cx<T> kk = st.k1[qq][p];
-                        sr.x = fma(win[2 * p].x, kk.x, sr.x);
-                        sr.y = fma(win[2 * p].y, kk.x, sr.y);
-                        if (2 * p + 1 < W) {
-                            constexpr int Z = 0;
-                            const int i1 = 2 * p + 1 < W ? 2 * p + 1 : Z;
-                            sr.x = fma(win[i1].x, kk.y, sr.x);
-                            sr.y = fma(win[i1].y, kk.y, sr.y);
-                        }
-                    }
-                    t[j] = Cx<T>::make(sr.x * kc, sr.y * kc);
-                    who[j] = mine ? qq : -1;
-                    q += two ? 2 : 1;
-                }
-            }
-            // reduce-scatter over the 16 lanes of each half: lane c ends with step
-            // 2 (c >> 3 & 1) + (c >> 2 & 1) summed over all 16 columns
-            const bool b3 = (c & 8) != 0, b2 = (c & 4) != 0;
-            cx<T> u0 = b3 ? t[2] : t[0], u1 = b3 ? t[3] : t[1];
-            const cx<T> s0 = b3 ? t[0] : t[2], s1 = b3 ? t[1] : t[3];
-            const cx<T> r0v = shfl_xor_cx<T>(s0, 8), r1v = shfl_xor_cx<T>(s1, 8);
-            u0.x += r0v.x;
-            u0.y += r0v.y;
-            u1.x += r1v.x;
-            u1.y += r1v.y;
-            cx<T> w = b2 ? u1 : u0;
-            const cx<T> sw = shfl_xor_cx<T>(b2 ? u0 : u1, 4);
-            w.x += sw.x;
-            w.y += sw.y;
-            cx<T> o = shfl_xor_cx<T>(w, 2);
-            w.x += o.x;
-            w.y += o.y;
-            o = shfl_xor_cx<T>(w, 1);
-            w.x += o.x;
-            w.y += o.y;
-            const int j = (b3 ? 2 : 0) + (b2 ? 1 : 0);
-            const int pq = j == 0 ? who[0] : j == 1 ? who[1] : j == 2 ? who[2] : who[3];
-            if ((c & 3) == 0 && pq >= 0) f[st.out[pq] + M * b] = make_double2((double)w.x, (double)w.y);
-        }
-    }
-}
-
 template <int W, class T>
 static int launch_interp(const NufftGrid& g, NufftDev& d, double2* f, int B, cudaStream_t s) {
-    if (W <= 10 && g.bin_cols + W - 1 <= 16 && !getenv("PFSHT_NUFFT_OLD")) {
-        for (int b = 0; b < B; ++b) {
-            interp_pair_kernel<(W <= 10 ? W : 2), T><<<(g.nbusy + 3) / 4, 128, 0, s>>>(
-                d.pts.as<double2>(), d.perm.as<int>(), d.binstart.as<int>(), d.binorder.as<int>(),
-                g.nbusy, g.nbc, g.bin_rows, g.bin_cols, g.M, d.U.as<cx<T>>(), g.nrows, g.nf2,
-                g.row_wrap, b, f);
-            PF_TRY(check_launch("interp_pair_kernel"));
-        }
-        return 0;
-    }
     const size_t smem = sizeof(cx<T>) * (g.bin_rows + W - 1) * (g.igroup * g.bin_cols + W - 1);
     if (smem > 48 * 1024)
         PF_CUDA(cudaFuncSetAttribute(interp_kernel<W, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1515,46 +1195,29 @@ static int launch_interp(const NufftGrid& g, NufftDev& d, double2* f, int B, cud
 
 template <int W, class T>
 static int launch_spread(const NufftGrid& g, NufftDev& d, const double2* f, int B, cudaStream_t s) {
-    if (W <= 10 && g.bin_cols + W - 1 <= 16 && !getenv("PFSHT_NUFFT_OLD")) {
-        for (int b = 0; b < B; ++b) {
-            if (g.ncolors > 0) {
-                // one launch per colour, in a fixed order: plain adds, a deterministic sum
-                for (int k = 0; k < g.ncolors; ++k) {
-                    const int n = g.color_off[k + 1] - g.color_off[k];
-                    if (n == 0) continue;
-                    spread_pair_kernel<(W <= 10 ? W : 2), T><<<(n + 3) / 4, 128, 0, s>>>(
-                        d.pts.as<double2>(), d.perm.as<int>(), d.binstart.as<int>(),
-                        d.sorder.as<int>() + g.color_off[k], n, g.nbc, g.bin_rows, g.bin_cols,
-                        g.M, f, b, g.nrows, g.nf2, g.row_wrap, 1, d.U.as<cx<T>>());
-                    PF_TRY(check_launch("spread_pair_kernel"));
-                }
+    // with the deterministic option, one launch per bin colour in a fixed order and plain adds
+    const bool col = g.deterministic && g.ncolors > 0;
+    const int nl = col ? g.ncolors : 1;
+    for (int b = 0; b < B; ++b) {
+        for (int k = 0; k < nl; ++k) {
+            const int n = col ? g.color_off[k + 1] - g.color_off[k] : g.nbusy;
+            const int* order = col ? d.sorder.as<int>() + g.color_off[k] : d.binorder.as<int>();
+            if (n == 0) continue;
+            if (W <= 10 && g.bin_cols + W - 1 <= 16) {
+                spread16_kernel<(W <= 10 ? W : 2), T><<<(n + 3) / 4, 128, 0, s>>>(
+                    d.pts.as<double2>(), d.perm.as<int>(), d.binstart.as<int>(), order, n, g.nbc,
+                    g.bin_rows, g.bin_cols, g.M, f, b, g.nrows, g.nf2, g.row_wrap, col ? 1 : 0,
+                    d.U.as<cx<T>>());
+                PF_TRY(check_launch("spread16_kernel"));
             } else {
-                spread_pair_kernel<(W <= 10 ? W : 2), T><<<(g.nbusy + 3) / 4, 128, 0, s>>>(
-                    d.pts.as<double2>(), d.perm.as<int>(), d.binstart.as<int>(), d.binorder.as<int>(),
-                    g.nbusy, g.nbc, g.bin_rows, g.bin_cols, g.M, f, b, g.nrows, g.nf2, g.row_wrap,
-                    0, d.U.as<cx<T>>());
-                PF_TRY(check_launch("spread_pair_kernel"));
+                constexpr int NW = SpreadWarps<W>::N;
+                spread_kernel<W, T><<<(n + NW - 1) / NW, NW * 32, 0, s>>>(
+                    d.pts.as<double2>(), d.perm.as<int>(), d.binstart.as<int>(), order, n, g.nbc,
+                    g.bin_rows, g.bin_cols, g.M, f, b, g.nrows, g.nf2, g.row_wrap, col ? 1 : 0,
+                    d.U.as<cx<T>>());
+                PF_TRY(check_launch("spread_kernel"));
             }
         }
-        return 0;
-    }
-    if (W <= 10 && g.bin_cols + W - 1 <= 16) {
-        for (int b = 0; b < B; ++b) {
-            spread16_kernel<(W <= 10 ? W : 2), T><<<(g.nbusy + 3) / 4, 128, 0, s>>>(
-                d.pts.as<double2>(), d.perm.as<int>(), d.binstart.as<int>(), d.binorder.as<int>(),
-                g.nbusy, g.nbc, g.bin_rows, g.bin_cols, g.M, f, b, g.nrows, g.nf2, g.row_wrap,
-                d.U.as<cx<T>>());
-            PF_TRY(check_launch("spread16_kernel"));
-        }
-        return 0;
-    }
-    for (int b = 0; b < B; ++b) {
-        constexpr int NW = SpreadWarps<W>::N;
-        spread_kernel<W, T><<<(g.nbusy + NW - 1) / NW, NW * 32, 0, s>>>(
-            d.pts.as<double2>(), d.perm.as<int>(), d.binstart.as<int>(), d.binorder.as<int>(),
-            g.nbusy, g.nbc, g.bin_rows, g.bin_cols, g.M, f, b, g.nrows, g.nf2, g.row_wrap,
-            d.U.as<cx<T>>());
-        PF_TRY(check_launch("spread_kernel"));
     }
     return 0;
 }

@@ -222,10 +222,10 @@ void fill_info(pfsht_plan* p) {
     in.device_bytes = bytes;
 }
 
-// Adjoint items: all retained rings of an order in one item when no order retains more than
-// four tiles of 32 * R rings (the warp walks them tile after tile and adds each tile's sums to
-// the previous ones in order: a deterministic pass without atomics), else tiles of 32 * R rings
-// whose sums add atomically; each order split into degree segments of about seg_degrees when the
+// Adjoint items: tiles of 32 * R rings whose sums add atomically when an order spans several;
+// with the deterministic option, all retained rings of an order in one item when no order retains
+// more than four tiles (the warp walks them tile after tile and adds each tile's sums to the
+// previous ones in order: a pass without atomics, measured ~8% slower at lmax 2048); each order split into degree segments of about seg_degrees when the
 // unsplit items would give fewer than ~8 warps per resident warp slot (12 per SM at the
 // adjoint's register count). The saved recurrence state is bounded by 512 MiB; past that, or
 // with seg_degrees < 0, the items stay whole.
@@ -235,7 +235,7 @@ int build_adjoint_items(pfsht_plan* p, const std::vector<int>& jlo, const std::v
     const int rmax = p->R > 0 ? p->R : 4;
     int maxret = 0;
     for (int m = 0; m <= std::min(mmax, L); ++m) maxret = std::max(maxret, jhi[m] - jlo[m] + 1);
-    const int tile = maxret <= 4 * 32 * rmax ? std::max(maxret, 1) : 32 * rmax;
+    const int tile = p->deterministic && maxret <= 4 * 32 * rmax ? std::max(maxret, 1) : 32 * rmax;
     int seg = p->seg_degrees;
     if (seg == 0) {
         int sms = 148;
@@ -333,6 +333,7 @@ int build_stretch(pfsht_plan* p, const double* d_theta, const double* d_phi, con
                             o.nufft_nf2, s));
     PF_TRY(nufft_setpts(p->ng, p->nd, Th.as<double>(), ph.as<double>(), s));
     p->ng.plain_transpose = o.nufft_transpose == 1 ? 1 : 0;
+    p->ng.deterministic = p->deterministic;
     PF_TRY(nufft_alloc(p->ng, p->nd, B));
     return 0;
 }
@@ -590,6 +591,7 @@ int plan_create(const double* theta, const double* phi, int64_t npts, int lmax, 
     p->R = o.ring_rings_per_lane == 2 || o.ring_rings_per_lane == 4 || o.ring_rings_per_lane == 8
                ? o.ring_rings_per_lane : 0;
     p->seg_degrees = o.ring_segment_degrees;
+    p->deterministic = o.deterministic ? 1 : 0;
     p->spin = o.spin;
     PF_CUDA(cudaStreamCreateWithFlags(&p->st_stream, cudaStreamNonBlocking));
     PF_CUDA(cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking));

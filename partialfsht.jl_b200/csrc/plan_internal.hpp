@@ -19,6 +19,7 @@ struct pfsht_plan {
     int64_t M = 0;
     double tol = 0;
     int R = 0;  // ring tile rings-per-lane override (0 = defaults)
+    int deterministic = 0;  // fixed-order adjoint sums (pfsht_opts.deterministic)
     pf::Leaf leaf;
     int ncols = 0;
     int nrings = 0;

@@ -631,24 +631,17 @@ ring_fwd_batch_kernel(const RingSlot* __restrict__ slots, const BatchItem* __res
 template <bool MIX> using RedT = std::conditional_t<MIX, float, double>;
 template <bool MIX> using RingDataT = std::conditional_t<MIX, float2, double2>;
 
-// One warp's staging (a block holds one per warp). SHF (one transform per pass): each degree's
-// four partial sums go through two shuffle stages first (lanes l, l ^ 16, then l ^ 8), after
-// which lane l holds component l >> 3 summed over the four lanes that share l & 7, and only that
-// value is staged: red8[degree slot][(l & 7) 4 + (l >> 3)], rows of 36 so that both the staging
-// and the reduction's reads fill each bank once
-template <bool MIX, bool SHF>
-struct AdjSmem {
-    RedT<MIX> red[SHF ? 1 : 32][33];
-    RedT<MIX> red8[SHF ? 8 : 1][36];
+template <bool MIX>
+struct AdjSmem {  // one warp's staging (a block holds one per warp)
+    RedT<MIX> red[32][33];
     double2 bg[32];
 };
 
-template <int R, int NB, bool MIX, bool SHF>
+template <int R, int NB, bool MIX>
 __device__ __forceinline__ void ring_adj_item(const RingTables& t, const RingOut& o,
                                               const RingItem& item, const double2* __restrict__ in,
                                               double* __restrict__ almd, int b0, int wmode,
-                                              AdjSmem<MIX, SHF>& sm, int warp, int lane) {
-    static_assert(!SHF || NB == 1, "the shuffle staging serves one transform per pass");
+                                              AdjSmem<MIX>& sm, int warp, int lane) {
     constexpr int STRIDE = MIX ? 16 : 64;
     constexpr int NV = 4 * NB;   // (+m re, +m im, -m re, -m im) per transform
     constexpr int LB = 32 / NV;  // degrees per reduction block
@@ -763,20 +756,8 @@ __device__ __forceinline__ void ring_adj_item(const RingTables& t, const RingOut
                 }
             }
         }
-        if constexpr (SHF) {
-            const bool hi16 = (lane & 16) != 0, b8 = (lane & 8) != 0;
-            RT k0 = hi16 ? part[2] : part[0], k1 = hi16 ? part[3] : part[1];
-            const RT s0 = hi16 ? part[0] : part[2], s1 = hi16 ? part[1] : part[3];
-            k0 += __shfl_xor_sync(0xffffffffu, s0, 16);
-            k1 += __shfl_xor_sync(0xffffffffu, s1, 16);
-            RT kk = b8 ? k1 : k0;
-            const RT ss = b8 ? k0 : k1;
-            kk += __shfl_xor_sync(0xffffffffu, ss, 8);
-            sm.red8[slot][(lane & 7) * 4 + (lane >> 3)] = kk;
-        } else {
 #pragma unroll
-            for (int v = 0; v < NV; ++v) sm.red[slot * NV + v][lane] = part[v];
-        }
+        for (int v = 0; v < NV; ++v) sm.red[slot * NV + v][lane] = part[v];
     };
     // reduce the staged degrees [lfirst, lfirst + cnt) over the lanes and write alm; degree
     // lfirst + i carries the factor g of its chunk slot gslot0 + i (1 for the seed degrees)
@@ -784,25 +765,14 @@ __device__ __forceinline__ void ring_adj_item(const RingTables& t, const RingOut
         __syncwarp();
         if (lane < cnt * NV) {
             const int li = lane / NV, v = lane % NV;
+            // four independent partial sums: the chain of dependent adds is 8 long, not 32
             RT s0 = 0, s1 = 0, s2 = 0, s3 = 0;
-            if constexpr (SHF) {
-                // the eight lane groups' sums of component v of degree slot li
 #pragma unroll
-                for (int k = 0; k < 8; k += 4) {
-                    s0 += sm.red8[li][k * 4 + v];
-                    s1 += sm.red8[li][(k + 1) * 4 + v];
-                    s2 += sm.red8[li][(k + 2) * 4 + v];
-                    s3 += sm.red8[li][(k + 3) * 4 + v];
-                }
-            } else {
-                // four independent partial sums: the chain of dependent adds is 8 long, not 32
-#pragma unroll
-                for (int q = 0; q < 32; q += 4) {
-                    s0 += sm.red[lane][q];
-                    s1 += sm.red[lane][q + 1];
-                    s2 += sm.red[lane][q + 2];
-                    s3 += sm.red[lane][q + 3];
-                }
+            for (int q = 0; q < 32; q += 4) {
+                s0 += sm.red[lane][q];
+                s1 += sm.red[lane][q + 1];
+                s2 += sm.red[lane][q + 2];
+                s3 += sm.red[lane][q + 3];
             }
             double s = (double)((s0 + s1) + (s2 + s3));
             if (gslot0 >= 0) s *= sm.bg[gslot0 + li].y;
@@ -916,11 +886,11 @@ __device__ __forceinline__ void ring_adj_item(const RingTables& t, const RingOut
     }
 }
 
-template <int RMAX, int NB, bool MIX, bool SHF>
+template <int RMAX, int NB, bool MIX>
 __device__ __forceinline__ void ring_adj_body(const RingTables& t, const RingOut& o,
                                               const RingItem& item, const double2* __restrict__ in,
                                               double* __restrict__ almd, int b0, int allow_sole,
-                                              AdjSmem<MIX, SHF>& sm, int warp, int lane) {
+                                              AdjSmem<MIX>& sm, int warp, int lane) {
     // an item holding all retained rings of its order writes its degrees alone: its first ring
     // tile stores them and the later ones add in order (deterministic); an order split over
     // several items adds atomically into zeros
@@ -932,22 +902,22 @@ __device__ __forceinline__ void ring_adj_body(const RingTables& t, const RingOut
         sub.n = min(32 * RMAX, item.n - base);
         if (sub.ck >= 0) sub.ck += base;
         const int reff = (sub.n + 31) >> 5;
-        if (RMAX >= 8 && reff >= 5) ring_adj_item<(RMAX >= 8 ? 8 : 1), NB, MIX, SHF>(t, o, sub, in, almd, b0, wmode, sm, warp, lane);
-        else if (RMAX >= 4 && reff >= 3) ring_adj_item<(RMAX >= 4 ? 4 : 1), NB, MIX, SHF>(t, o, sub, in, almd, b0, wmode, sm, warp, lane);
-        else if (RMAX >= 2 && reff == 2) ring_adj_item<(RMAX >= 2 ? 2 : 1), NB, MIX, SHF>(t, o, sub, in, almd, b0, wmode, sm, warp, lane);
-        else ring_adj_item<1, NB, MIX, SHF>(t, o, sub, in, almd, b0, wmode, sm, warp, lane);
+        if (RMAX >= 8 && reff >= 5) ring_adj_item<(RMAX >= 8 ? 8 : 1), NB, MIX>(t, o, sub, in, almd, b0, wmode, sm, warp, lane);
+        else if (RMAX >= 4 && reff >= 3) ring_adj_item<(RMAX >= 4 ? 4 : 1), NB, MIX>(t, o, sub, in, almd, b0, wmode, sm, warp, lane);
+        else if (RMAX >= 2 && reff == 2) ring_adj_item<(RMAX >= 2 ? 2 : 1), NB, MIX>(t, o, sub, in, almd, b0, wmode, sm, warp, lane);
+        else ring_adj_item<1, NB, MIX>(t, o, sub, in, almd, b0, wmode, sm, warp, lane);
     }
 }
 
-template <int RMAX, int NB, bool MIX, bool SHF>
+template <int RMAX, int NB, bool MIX>
 __global__ void __launch_bounds__(kAdjWarps * 32)
 ring_adj_kernel(RingTables t, RingOut o, const RingItem* __restrict__ items, int nitems,
                 const double2* __restrict__ in, double* __restrict__ almd, int b0, int allow_sole) {
-    __shared__ AdjSmem<MIX, SHF> sm[kAdjWarps];
+    __shared__ AdjSmem<MIX> sm[kAdjWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int it = blockIdx.x * kAdjWarps + warp;
     if (it >= nitems) return;
-    ring_adj_body<RMAX, NB, MIX, SHF>(t, o, items[it], in, almd, b0, allow_sole, sm[warp], warp, lane);
+    ring_adj_body<RMAX, NB, MIX>(t, o, items[it], in, almd, b0, allow_sole, sm[warp], warp, lane);
 }
 
 // the adjoint ring passes of many plans: item i belongs to plan items[i].slot
@@ -955,8 +925,7 @@ template <int RMAX, int NB, bool MIX>
 __global__ void __launch_bounds__(kAdjWarps * 32)
 ring_adj_batch_kernel(const RingSlot* __restrict__ slots, const BatchItem* __restrict__ items,
                       int nitems, void* const* __restrict__ ptrs) {
-    constexpr bool SHF = NB == 1;
-    __shared__ AdjSmem<MIX, SHF> sm[kAdjWarps];
+    __shared__ AdjSmem<MIX> sm[kAdjWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int it = blockIdx.x * kAdjWarps + warp;
     if (it >= nitems) return;
@@ -964,7 +933,7 @@ ring_adj_batch_kernel(const RingSlot* __restrict__ slots, const BatchItem* __res
     const RingSlot& sl = slots[bi.slot];
     const RingTables t = sl.t;
     const RingOut o = sl.o;
-    ring_adj_body<RMAX, NB, MIX, SHF>(t, o, bi.it, sl.H, static_cast<double*>(ptrs[sl.ptr]), bi.b0,
+    ring_adj_body<RMAX, NB, MIX>(t, o, bi.it, sl.H, static_cast<double*>(ptrs[sl.ptr]), bi.b0,
                                       sl.allow_sole, sm[warp], warp, lane);
 }
 
@@ -997,12 +966,8 @@ template <int RMAX, int NB, bool MIX>
 static int launch_adj(const RingTables& t, const RingOut& o, const RingItem* items, int nitems,
                       const double2* in, double2* alm, int b0, int allow_sole, cudaStream_t s) {
     const int grid = (nitems + kAdjWarps - 1) / kAdjWarps;
-    if (NB == 1 && !getenv("PFSHT_ADJ_OLD"))
-        ring_adj_kernel<RMAX, NB, MIX, NB == 1><<<grid, kAdjWarps * 32, 0, s>>>(
-            t, o, items, nitems, in, reinterpret_cast<double*>(alm), b0, allow_sole);
-    else
-        ring_adj_kernel<RMAX, NB, MIX, false><<<grid, kAdjWarps * 32, 0, s>>>(
-            t, o, items, nitems, in, reinterpret_cast<double*>(alm), b0, allow_sole);
+    ring_adj_kernel<RMAX, NB, MIX><<<grid, kAdjWarps * 32, 0, s>>>(
+        t, o, items, nitems, in, reinterpret_cast<double*>(alm), b0, allow_sole);
     return check_launch("ring_adj_kernel");
 }
 
@@ -1257,8 +1222,8 @@ union FwdAnySmem {
     FwdSmem<1, true> f;
 };
 union AdjAnySmem {
-    AdjSmem<false, true> a;
-    AdjSmem<true, true> b;
+    AdjSmem<false> a;
+    AdjSmem<true> b;
 };
 
 __device__ __forceinline__ int pull_item(int* counter, int lane) {
@@ -1306,10 +1271,10 @@ ring_adj_persistent_kernel(const RingSlot* __restrict__ slots, const BatchItem* 
         double* almd = static_cast<double*>(ptrs[sl.ptr]);
         AdjAnySmem& w = sm[warp];
         switch (bi.it.pad_) {
-            case 0: ring_adj_body<4, 1, false, true>(t, o, bi.it, sl.H, almd, bi.b0, sl.allow_sole, w.a, warp, lane); break;
-            case 1: ring_adj_body<2, 1, false, true>(t, o, bi.it, sl.H, almd, bi.b0, sl.allow_sole, w.a, warp, lane); break;
-            case 2: ring_adj_body<4, 1, true, true>(t, o, bi.it, sl.H, almd, bi.b0, sl.allow_sole, w.b, warp, lane); break;
-            default: ring_adj_body<2, 1, true, true>(t, o, bi.it, sl.H, almd, bi.b0, sl.allow_sole, w.b, warp, lane); break;
+            case 0: ring_adj_body<4, 1, false>(t, o, bi.it, sl.H, almd, bi.b0, sl.allow_sole, w.a, warp, lane); break;
+            case 1: ring_adj_body<2, 1, false>(t, o, bi.it, sl.H, almd, bi.b0, sl.allow_sole, w.a, warp, lane); break;
+            case 2: ring_adj_body<4, 1, true>(t, o, bi.it, sl.H, almd, bi.b0, sl.allow_sole, w.b, warp, lane); break;
+            default: ring_adj_body<2, 1, true>(t, o, bi.it, sl.H, almd, bi.b0, sl.allow_sole, w.b, warp, lane); break;
         }
         __syncwarp();
     }

@@ -50,12 +50,13 @@ def test_stretch_apply_matches_oracle(pf, O, cuda, L):
 
 def test_ring_adjoint_is_deterministic(pf, O, cuda):
     # the reference's threaded adjoint ring pass equals its serial one bit for bit
-    # (test/test_backends.jl:202-259): here every order's retained rings sit in one item whose
-    # warp adds its ring tiles' sums in a fixed order, so two passes agree bit for bit
+    # (test/test_backends.jl:202-259): with the deterministic option every order's retained rings
+    # sit in one item whose warp adds its ring tiles' sums in a fixed order, so two passes agree
+    # bit for bit
     rng = np.random.default_rng(13)
     L = 1024
     th, ph = cap_points(100000, rng=rng)
-    plan = pf.Plan(th, ph, lmax=L, tol=1e-8)
+    plan = pf.Plan(th, ph, lmax=L, tol=1e-8, deterministic=True)
     n = plan.info["nrings"]
     Gr = to_dev(np.asfortranarray(cn(rng, n, 2 * L + 1, 1)))
     out = []

@@ -193,17 +193,20 @@ def test_host_buffers_equal_device_applies(pf, O, cuda, L, B):
 
 @pytest.mark.parametrize("precision,tol", [("fp64", 1e-8), ("mixed", 1e-6)])
 def test_adjoint_is_deterministic(pf, O, cuda, precision, tol):
-    # spreading runs its bins in colours whose tiles are disjoint (plain adds, fixed order) and
-    # the ring pass holds each order's rings in one warp: two adjoints agree bit for bit, as the
-    # reference's threaded and serial adjoints do (test/test_backends.jl:202-259)
+    # with the deterministic option, spreading runs its bins in colours whose tiles are disjoint
+    # (plain adds, fixed order) and the ring pass holds each order's rings in one warp: two
+    # adjoints agree bit for bit, as the reference's threaded and serial adjoints do
+    # (test/test_backends.jl:202-259); they equal the default plan's to round-off
     rng = np.random.default_rng(43)
     L = 512
     th, ph = cap_points(50000, rng=rng)
-    ps = pf.Plan(th, ph, lmax=L, tol=tol, precision=precision)
+    ps = pf.Plan(th, ph, lmax=L, tol=tol, precision=precision, deterministic=True)
     g = to_dev(cn(rng, len(th)))
     a1 = to_host(ps.H * g)
     a2 = to_host(ps.H * g)
     assert np.array_equal(a1, a2)
+    pd = pf.Plan(th, ph, lmax=L, tol=tol, precision=precision)
+    assert O.alm_reldiff(a1, to_host(pd.H * g), L) < (2e-6 if precision == "mixed" else 1e-13)
 
 
 @pytest.mark.parametrize("precision,tol", [("fp64", 1e-8), ("mixed", 1e-6)])
