@@ -294,7 +294,7 @@ struct NufftGrid {
     // spreading in bin colours: bins (br, bc) of one colour (br mod rcol, bc mod ccol) have
     // disjoint tiles, so launching the colours one after the other (deterministic != 0) lets
     // every tile add its rows with plain loads and stores, in a fixed order (a deterministic
-    // type-1 NUFFT); 0 colours: the grid does not allow it and rows add atomically
+    // type-1 NUFFT); bins whose tiles wrap around the grid have colour classes of their own
     int deterministic = 0;
     int ncolors = 0;
     std::vector<int> color_off;  // ncolors + 1 offsets into NufftDev::sorder

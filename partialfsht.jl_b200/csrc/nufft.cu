@@ -266,21 +266,27 @@ int nufft_setpts(NufftGrid& g, NufftDev& d, const double* x, const double* y, cu
         PF_CUDA(cudaMemcpyAsync(d.binorder.p, order.data(), sizeof(int) * order.size(),
                                 cudaMemcpyHostToDevice, s));
     // spreading colours: tiles of bins rcol rows or ccol columns of bins apart are disjoint when
-    // the kernel's reach w - 1 fits in (rcol - 1) bins; wrapped grids need whole colour periods
+    // the kernel's reach w - 1 fits in (rcol - 1) bins. Tiles that run past the grid's last column
+    // (or, when rows wrap, its last row) wrap onto its first ones, so those bins get colour
+    // classes of their own, one set for column wrap, one for row wrap and one for both; within
+    // such a set no two bins of one class both wrap, so their tiles stay disjoint as well.
     {
         const int rcol = 1 + (g.w - 1 + g.bin_rows - 1) / g.bin_rows;
         const int ccol = 1 + (g.w - 1 + g.bin_cols - 1) / g.bin_cols;
-        const bool ok = g.nbc % ccol == 0 && g.nbc >= ccol &&
-                        (!g.row_wrap || (g.nbr % rcol == 0 && g.nbr >= rcol));
-        g.ncolors = ok ? rcol * ccol : 0;
+        const int K = rcol * ccol;
+        g.ncolors = 4 * K;
         std::vector<int> sord;
         g.color_off.assign(1, 0);
-        if (ok) {
-            for (int k = 0; k < g.ncolors; ++k) {
-                for (int b : order)
-                    if ((b / g.nbc) % rcol * ccol + (b % g.nbc) % ccol == k) sord.push_back(b);
-                g.color_off.push_back((int)sord.size());
-            }
+        auto colour = [&](int b) {
+            const int br = b / g.nbc, bc = b % g.nbc;
+            const int cw = bc * g.bin_cols + g.bin_cols + g.w - 1 > g.nf2 ? 1 : 0;
+            const int rw = g.row_wrap && br * g.bin_rows + g.bin_rows + g.w - 1 > g.nrows ? 1 : 0;
+            return (br % rcol) * ccol + bc % ccol + K * (cw + 2 * rw);
+        };
+        for (int k = 0; k < g.ncolors; ++k) {
+            for (int b : order)
+                if (colour(b) == k) sord.push_back(b);
+            g.color_off.push_back((int)sord.size());
         }
         PF_TRY(d.sorder.alloc(sizeof(int) * std::max<size_t>(sord.size(), 1)));
         if (!sord.empty())
@@ -563,13 +569,13 @@ __global__ void rows_adj_kernel(const cx<T>* __restrict__ U, int nf1, int ncols,
 constexpr int kTmaWaitLimit = 1 << 20;
 
 // U[r, p2] = pad[(row0 + r) mod nf1, p2col[p2]]; blocks past the tiles zero the fine columns
-// [gap_lo, gap_hi) that hold no mode column (the only such columns)
+// [gap_lo, gap_hi) that hold no mode column (the only such columns), 32 rows x 256 columns each
 template <class T>
 __global__ void __launch_bounds__(256)
 rows_fwd_tma_kernel(const __grid_constant__ CUtensorMap pmap, const cx<T>* __restrict__ pad,
                     int nf1, int ncols, int row0, int nrows, int nf2,
                     const int* __restrict__ colp2, int gap_lo, int gap_hi, int ntc, int ntr,
-                    cx<T>* __restrict__ U) {
+                    int nzc, cx<T>* __restrict__ U) {
     constexpr int E = sizeof(cx<T>);  // 16 (FP64) or 8 (FP32) bytes
     constexpr int SUB = 128 / E;       // fine rows per 128-byte line
     constexpr int NSUB = 32 / SUB;     // line blocks per 32-row tile
@@ -579,10 +585,12 @@ rows_fwd_tma_kernel(const __grid_constant__ CUtensorMap pmap, const cx<T>* __res
     cx<T>* ub = U + (int64_t)nrows * nf2 * b;
     const int ntiles = ntc * ntr;
     if ((int)blockIdx.x >= ntiles) {
-        const int zr = ((int)blockIdx.x - ntiles) * 32;
+        const int zb = (int)blockIdx.x - ntiles;
+        const int zr = (zb / nzc) * 32, z0 = gap_lo + (zb % nzc) * 256;
+        const int z1 = min(z0 + 256, gap_hi);
         const cx<T> z = Cx<T>::make(0, 0);
         for (int r = zr + ty; r < min(zr + 32, nrows); r += 8)
-            for (int p2 = gap_lo + tx; p2 < gap_hi; p2 += 32) ub[(int64_t)r * nf2 + p2] = z;
+            for (int p2 = z0 + tx; p2 < z1; p2 += 32) ub[(int64_t)r * nf2 + p2] = z;
         return;
     }
     const int c0 = ((int)blockIdx.x % ntc) * 32, r0 = ((int)blockIdx.x / ntc) * 32;
@@ -1271,11 +1279,11 @@ static int type2_impl(const NufftGrid& g, NufftDev& d, const double2* modes, dou
     clock_mark(clk, kStFft1Fwd, s);
     if (d.have_maps) {
         const int ntc = (g.ncols + 31) / 32, ntr = (g.nrows + 31) / 32;
-        const int nz = g.gap_hi > g.gap_lo ? ntr : 0;
-        dim3 grid(ntc * ntr + nz, 1, B);
+        const int nzc = (g.gap_hi - g.gap_lo + 255) / 256;
+        dim3 grid(ntc * ntr + ntr * nzc, 1, B);
         rows_fwd_tma_kernel<T><<<grid, dim3(32, 8), 0, s>>>(
             d.pad_map, d.pad.as<cx<T>>(), g.nf1, g.ncols, g.row0, g.nrows, g.nf2,
-            d.colp2.as<int>(), g.gap_lo, g.gap_hi, ntc, ntr, d.U.as<cx<T>>());
+            d.colp2.as<int>(), g.gap_lo, g.gap_hi, ntc, ntr, nzc, d.U.as<cx<T>>());
         PF_TRY(check_launch("rows_fwd_tma_kernel"));
     } else {
         dim3 grid((g.nf2 + 31) / 32, (g.nrows + 31) / 32, B);

@@ -212,7 +212,8 @@ def test_adjoint_is_deterministic(pf, O, cuda, precision, tol):
 @pytest.mark.parametrize("precision,tol", [("fp64", 1e-8), ("mixed", 1e-6)])
 def test_tma_transposes_equal_plain_ones(pf, O, cuda, precision, tol):
     # the NUFFT's fine-row transposes with TMA-staged tiles move the same values as the plain-load
-    # kernels: both applies agree bit for bit; every bounded tile wait ended
+    # kernels: forwards agree bit for bit, adjoints to the order of their atomic additions; every
+    # bounded tile wait ended
     import ctypes as C
     rng = np.random.default_rng(45)
     L = 700
@@ -223,7 +224,7 @@ def test_tma_transposes_equal_plain_ones(pf, O, cuda, precision, tol):
     alm = O.rand_alm(L, rng=rng)
     g = cn(rng, len(th))
     assert np.array_equal(_fwd(pt, alm), _fwd(pp, alm))
-    assert np.array_equal(_adj(pt, g), _adj(pp, g))
+    assert O.alm_reldiff(_adj(pt, g), _adj(pp, g), L) < (2e-6 if precision == "mixed" else 1e-14)
     n = C.c_int32(-1)
     assert pf._lib.load().pfsht_wait_timeouts(C.byref(n)) == 0
     assert n.value == 0
