@@ -311,6 +311,8 @@ struct NufftDev {
     DevBuf binorder;  // int32 nbusy: non-empty bins, most points first
     DevBuf iorder;    // int32 nisb: non-empty interpolation groups, most points first
     DevBuf sorder;    // int32 nbusy: non-empty bins by spreading colour, most points first in each
+    DevBuf ipts;      // double2: pts in the interpolation's order (each group's points dealt over
+    DevBuf iperm;     // int32    their shared-memory bank class), and their original indices
     DevBuf colp2;     // int32 ncols: fine column of each mode column
     DevBuf p2col;     // int32 nf2: mode column of each fine column or -1
     DevBuf mult1;     // double2 n1: per-mode complex factor along dim 1 (deconv incl.)

@@ -202,6 +202,68 @@ __global__ void gather_points_kernel(const double2* __restrict__ g, const int* _
     }
 }
 
+// bin offsets on the host (nbins + 1)
+static std::vector<int> binstart_host(const NufftGrid& g, const NufftDev& d, cudaStream_t s) {
+    std::vector<int> bs((size_t)g.nbr * g.nbc + 1, 0);
+    if (cudaMemcpyAsync(bs.data(), d.binstart.p, sizeof(int) * bs.size(), cudaMemcpyDeviceToHost, s) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        bs.clear();
+    return bs;
+}
+
+// The interpolation's order of the points (ipts / iperm): within each interpolation group, the
+// points dealt round-robin over the shared-memory bank class of their tile origin (element
+// offset (r0 TC + c0) mod KM, KM elements per 128 bytes), so that the KM lanes that read the
+// tile together in one shared-memory phase start at different banks and each tap's loads need
+// no replay. The group's point range is unchanged.
+int interp_point_order(const NufftGrid& g, NufftDev& d, const std::vector<int>& bs, cudaStream_t s) {
+    const int64_t M = g.M;
+    if (bs.empty()) {
+        set_error("copying the NUFFT bin offsets failed");
+        return 4;
+    }
+    std::vector<double2> pts(M);
+    std::vector<int> perm(M);
+    PF_CUDA(cudaMemcpyAsync(pts.data(), d.pts.p, sizeof(double2) * M, cudaMemcpyDeviceToHost, s));
+    PF_CUDA(cudaMemcpyAsync(perm.data(), d.perm.p, sizeof(int) * M, cudaMemcpyDeviceToHost, s));
+    PF_CUDA(cudaStreamSynchronize(s));
+    const int W = g.w, KM = g.fp32 ? 16 : 8;
+    const int G = g.igroup, TC = G * g.bin_cols + W - 1;
+    std::vector<double2> opts(M);
+    std::vector<int> operm(M);
+    std::vector<std::vector<int>> bucket(KM);
+#pragma omp parallel for schedule(dynamic, 16) num_threads(16) firstprivate(bucket) if (M > 100000)
+    for (int q = 0; q < g.nbr * g.nsbc; ++q) {
+        const int br = q / g.nsbc, sg = q % g.nsbc;
+        const int a = bs[br * g.nbc + sg * G], e = bs[br * g.nbc + std::min(g.nbc, sg * G + G)];
+        const int tr0 = br * g.bin_rows, tc0 = sg * G * g.bin_cols;
+        for (auto& v : bucket) v.clear();
+        for (int i = a; i < e; ++i) {
+            int r = (int)std::ceil(pts[i].x - 0.5 * W);
+            if (g.row_wrap) r = ((r % g.nrows) + g.nrows) % g.nrows;
+            int c = (int)std::ceil(pts[i].y - 0.5 * W);
+            c = ((c % g.nf2) + g.nf2) % g.nf2;
+            const int64_t off = (int64_t)(r - tr0) * TC + (c - tc0);
+            bucket[(int)(((off % KM) + KM) % KM)].push_back(i);
+        }
+        int o = a;
+        for (size_t j = 0; o < e; ++j)
+            for (int k = 0; k < KM; ++k)
+                if (j < bucket[k].size()) {
+                    opts[o] = pts[bucket[k][j]];
+                    operm[o] = perm[bucket[k][j]];
+                    ++o;
+                }
+    }
+    PF_TRY(d.ipts.alloc(sizeof(double2) * std::max<int64_t>(M, 1)));
+    PF_TRY(d.iperm.alloc(sizeof(int) * std::max<int64_t>(M, 1)));
+    PF_CUDA(cudaMemcpyAsync(d.ipts.p, opts.data(), sizeof(double2) * M, cudaMemcpyHostToDevice, s));
+    PF_CUDA(cudaMemcpyAsync(d.iperm.p, operm.data(), sizeof(int) * M, cudaMemcpyHostToDevice, s));
+    PF_CUDA(cudaStreamSynchronize(s));
+    return 0;
+}
+
 int nufft_setpts(NufftGrid& g, NufftDev& d, const double* x, const double* y, cudaStream_t s) {
     const int64_t M = g.M;
     if (M > INT32_MAX) {
@@ -309,7 +371,7 @@ int nufft_setpts(NufftGrid& g, NufftDev& d, const double* x, const double* y, cu
         PF_CUDA(cudaMemcpyAsync(d.iorder.p, gorder.data(), sizeof(int) * gorder.size(),
                                 cudaMemcpyHostToDevice, s));
     PF_CUDA(cudaStreamSynchronize(s));
-    return 0;
+    return interp_point_order(g, d, binstart_host(g, d, s), s);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -1195,7 +1257,7 @@ static int launch_interp(const NufftGrid& g, NufftDev& d, double2* f, int B, cud
     if (smem > 48 * 1024)
         PF_CUDA(cudaFuncSetAttribute(interp_kernel<W, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     interp_kernel<W, T><<<g.nisb, 128, smem, s>>>(
-        d.pts.as<double2>(), d.perm.as<int>(), d.binstart.as<int>(), d.iorder.as<int>(), g.nbc,
+        d.ipts.as<double2>(), d.iperm.as<int>(), d.binstart.as<int>(), d.iorder.as<int>(), g.nbc,
         g.igroup, g.nsbc, g.bin_rows, g.bin_cols, g.M, d.U.as<cx<T>>(), g.nrows, g.nf2,
         g.row_wrap, B, f);
     return check_launch("interp_kernel");
