@@ -90,6 +90,9 @@ typedef struct pfsht_opts {
                                    ring sums added in a fixed order by one warp, spreading bins
                                    launched in colours whose tiles are disjoint); 0 (default): the
                                    faster adjoint, whose atomic additions vary at round-off */
+    int32_t nufft_spread;       /* NUFFT spreading: 0 = each bin's whole tile held in registers
+                                   where the tile fits (16 columns, 32 rows), 1 = a sliding window
+                                   of the kernel's rows (same values, in the same order) */
 } pfsht_opts;
 
 typedef struct pfsht_plan pfsht_plan;

@@ -164,7 +164,10 @@ class Plan:
     lengths, deterministic) or a pair (nf1, nf2) of lengths at or above the minimum;
     ``info["nf1"]``, ``info["nf2"]`` give the lengths in use. ``transpose`` is "tma" (the NUFFT's
     fine-row transposes load their tiles with TMA tensor copies where the layout allows, the
-    default) or "plain" (plain loads only; the results are the same bit for bit).
+    default) or "plain" (plain loads only; the results are the same bit for bit). ``spread`` is
+    "registers" (the spreading holds each bin's whole tile in registers where it fits, the
+    default) or "window" (a sliding window of the kernel's rows); both add the same values in
+    the same order.
     ``deterministic=True`` makes adjoints bitwise reproducible run to run (fixed-order sums in
     the ring pass and the spreading) at some cost in speed; by default floating-point atomic
     additions let two adjoints differ at round-off.
@@ -176,7 +179,8 @@ class Plan:
     def __init__(self, theta, phi, *, lmax, tol=1e-10, ntrans=1, method="auto",
                  precision="fp64", oversample_theta=1.0, oversample_phi=1.0, eps_apo_max=1.0,
                  device=None, rings_per_lane=0, bin_rows=0, bin_cols=0, segment_degrees=0,
-                 fft_lengths="timed", maxboxes=8, spin=0, transpose="tma", deterministic=False):
+                 fft_lengths="timed", maxboxes=8, spin=0, transpose="tma", deterministic=False,
+                 spread="registers"):
         self._h = None
         if len(theta) != len(phi):
             raise DimensionMismatch("θ and φ must have the same length")
@@ -207,6 +211,9 @@ class Plan:
             raise ValueError(f"unknown transpose {transpose!r}")
         o.nufft_transpose = 0 if transpose == "tma" else 1
         o.deterministic = 1 if deterministic else 0
+        if spread not in ("registers", "window"):
+            raise ValueError(f"unknown spread {spread!r}")
+        o.nufft_spread = 0 if spread == "registers" else 1
         if isinstance(fft_lengths, (tuple, list)) and len(fft_lengths) == 2:
             o.nufft_fft_lengths = 2
             o.nufft_nf1, o.nufft_nf2 = int(fft_lengths[0]), int(fft_lengths[1])

@@ -25,7 +25,8 @@ class Opts(C.Structure):
                 ("oversample_phi", C.c_double), ("eps_apo_max", C.c_double),
                 ("ring_segment_degrees", C.c_int32), ("nufft_fft_lengths", C.c_int32),
                 ("nufft_nf1", C.c_int32), ("nufft_nf2", C.c_int32), ("maxboxes", C.c_int32),
-                ("spin", C.c_int32), ("nufft_transpose", C.c_int32), ("deterministic", C.c_int32)]
+                ("spin", C.c_int32), ("nufft_transpose", C.c_int32), ("deterministic", C.c_int32),
+                ("nufft_spread", C.c_int32)]
 
 
 class Box(C.Structure):

@@ -302,6 +302,7 @@ struct NufftGrid {
     // TMA row transposes zero directly
     int gap_lo = 0, gap_hi = 0, gap_ok = 0;
     int plain_transpose = 0;   // 1: the plain-load transposes only
+    int spread_reg = 1;        // spreading holds each bin's tile in registers where it fits
 };
 
 struct NufftDev {

@@ -882,14 +882,29 @@ interp_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
     const int s = binstart[br * nbc + sg * G];
     const int e = binstart[br * nbc + min(nbc, sg * G + G)];
     const TileGeom tg{br * BR, sg * G * BC, BR + W - 1, G * BC + W - 1};
+    // the tile is at most 32 columns wide (G BC <= 33 - W): lane = column, warps stride the rows
+    const int wid = threadIdx.x >> 5, ln = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int gcol = wrap(tg.tc0 + ln, nf2);
     for (int b = 0; b < B; ++b) {
         const cx<T>* ub = U + (int64_t)nrows * nf2 * b;
-        for (int t = threadIdx.x; t < tg.TR * tg.TC; t += blockDim.x) {
-            int r = tg.tr0 + t / tg.TC;
-            if (row_wrap) r = wrap(r, nrows);
-            cx<T> v = Cx<T>::make(0, 0);
-            if (r >= 0 && r < nrows) v = ub[(int64_t)r * nf2 + wrap(tg.tc0 + t % tg.TC, nf2)];
-            tile[t] = v;
+        if (tg.TC <= 32) {
+            if (ln < tg.TC) {
+                for (int rr = wid; rr < tg.TR; rr += nw) {
+                    int r = tg.tr0 + rr;
+                    if (row_wrap) r = wrap(r, nrows);
+                    cx<T> v = Cx<T>::make(0, 0);
+                    if (r >= 0 && r < nrows) v = ub[(int64_t)r * nf2 + gcol];
+                    tile[rr * tg.TC + ln] = v;
+                }
+            }
+        } else {
+            for (int t = threadIdx.x; t < tg.TR * tg.TC; t += blockDim.x) {
+                int r = tg.tr0 + t / tg.TC;
+                if (row_wrap) r = wrap(r, nrows);
+                cx<T> v = Cx<T>::make(0, 0);
+                if (r >= 0 && r < nrows) v = ub[(int64_t)r * nf2 + wrap(tg.tc0 + t % tg.TC, nf2)];
+                tile[t] = v;
+            }
         }
         // FP32 grids: the first point's coordinates load while the tile copy completes and
         // each later point's load is issued one iteration ahead (in FP64 the extra registers
@@ -1251,6 +1266,282 @@ spread16_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
     if (rbase >= 0) flush_all();
 }
 
+// Type-1 spreading with the bin's whole tile in registers: one warp per bin, lane (h, c) owns
+// tile column c (the tile is at most 16 columns wide) and every row of parity h, 2 NRH rows
+// at most (row 2 k + h in acc[k]). A point of origin row r0 = 2 j + p reaches, in each half,
+// registers j .. j + RW - 1 (RW = W / 2 + 1): register j + i of half h holds row offset
+// 2 i + h - p. Per batch of 32 points each lane stages one point's row weights and its value
+// times its column weights; the bin's points are sorted by origin row, so the batch splits
+// into runs of one row pair j, and each run is added by a warp-uniform switch on j that names
+// the registers statically: per point and lane, RW row weights, one column value and 2 RW
+// FMAs. Nothing is added to U until the bin ends, when each lane adds its rows once: no window
+// slides, no row is flushed twice, and a cell's sum runs over the bin's points in the same
+// order as in spread16_kernel, so the two give the same values.
+//
+// Two staging layouts, each the faster one measured for its precision:
+// - FP64 (SpreadPickStage): the row weights zero-padded, [0, 0, k_0 .. k_{W-1}, 0 ..], which a
+//   lane reads at stride 2 from 2 + h - p; the W column values and a 0, of which a lane picks
+//   its own by its offset from the point's first column; runs found point by point.
+// - FP32 (SpreadRowStage): each half's RW row weights in 16-byte vectors, and the value at
+//   every tile column (0 off the point), one load per lane; runs found by a ballot.
+template <int W, class T>
+struct SpreadPickStage {
+    static constexpr int RW = W / 2 + 1;       // registers a point reaches in one half
+    static constexpr int NK = 2 * RW + 2;      // [0, 0, k_0 .. k_{W-1}, 0 ..]
+    T k1[32][NK];              // row weights, zero-padded
+    cx<T> vk[32][W + 1];       // value x column weight; slot W is 0 for lanes off the point
+    int2 org[32];              // origin row (or -1: skip) and column inside the tile
+    long long roff[32];        // element offset of local row r in U (or -1: outside the grid)
+};
+
+template <int W, class T>
+struct SpreadRowStage {
+    static constexpr int RW = W / 2 + 1;
+    static constexpr int VPL = 16 / (int)sizeof(T);        // T per 16-byte load
+    static constexpr int KP = (RW + VPL - 1) / VPL * VPL;  // row weights per half
+    // rows padded to odd multiples of 16 bytes: the lanes' 16-byte stores of their points'
+    // rows fall in distinct banks
+    static constexpr int KS = 2 * KP + VPL;
+    static constexpr int NV = 16 + 16 / (int)sizeof(cx<T>);
+    alignas(16) T kw[32][KS];  // [point][half KP + i]: weight of register j + i (0-padded)
+    cx<T> vc[32][NV];          // [point][column]: value x column weight (0 off the point)
+    long long roff[32];
+};
+
+template <int W, class T> struct SpreadRegLayout {
+    using type = std::conditional_t<sizeof(T) == 8, SpreadPickStage<W, T>, SpreadRowStage<W, T>>;
+};
+
+// FP64: the points q, q + 1, .. < nb of origin row pair J; each point's operands are read
+// before its run test, so the test does not hold up the loads. Returns the first point after
+// the run.
+template <int J, int W, int NRH, class T>
+__device__ __forceinline__ int add_run(const SpreadPickStage<W, T>& st, int q, int nb, int h,
+                                       int c, cx<T> (&acc)[NRH]) {
+    constexpr int RW = SpreadPickStage<W, T>::RW;
+    if constexpr (J + RW <= NRH) {
+        do {
+            const int2 o = st.org[q];
+            const T* kr = st.k1[q] + 2 + h - (o.x & 1);
+            T kw[RW];
+#pragma unroll
+            for (int i = 0; i < RW; ++i) kw[i] = kr[2 * i];
+            const unsigned dc = (unsigned)(c - o.y);
+            const cx<T> vk = st.vk[q][dc < (unsigned)W ? dc : W];
+            if ((o.x >> 1) != J) break;  // the next pair (or a point outside the tile: -1)
+#pragma unroll
+            for (int i = 0; i < RW; ++i) {
+                acc[J + i].x = fma(vk.x, kw[i], acc[J + i].x);
+                acc[J + i].y = fma(vk.y, kw[i], acc[J + i].y);
+            }
+        } while (++q < nb);
+        return q;
+    } else {
+        return q + 1;  // no point of a fitting grid reaches this pair
+    }
+}
+
+// FP32: the points q0 .. q1 - 1, all of origin row pair J
+template <int J, int W, int NRH, class T>
+__device__ __forceinline__ void add_run(const SpreadRowStage<W, T>& st, int q0, int q1, int h,
+                                        int c, cx<T> (&acc)[NRH]) {
+    using S = SpreadRowStage<W, T>;
+    constexpr int RW = S::RW, KP = S::KP, KS = S::KS, NV = S::NV;
+    if constexpr (J + RW <= NRH) {
+        const T* kp = st.kw[q0] + h * KP;
+        const cx<T>* vp = &st.vc[q0][c];
+        for (int q = q0; q < q1; ++q, kp += KS, vp += NV) {
+            T kw[KP];
+            if constexpr (sizeof(T) == 8) {
+#pragma unroll
+                for (int u = 0; u < KP / 2; ++u) {
+                    const double2 t2 = reinterpret_cast<const double2*>(kp)[u];
+                    kw[2 * u] = t2.x;
+                    kw[2 * u + 1] = t2.y;
+                }
+            } else {
+#pragma unroll
+                for (int u = 0; u < KP / 4; ++u) {
+                    const float4 t4 = reinterpret_cast<const float4*>(kp)[u];
+                    kw[4 * u] = t4.x;
+                    kw[4 * u + 1] = t4.y;
+                    kw[4 * u + 2] = t4.z;
+                    kw[4 * u + 3] = t4.w;
+                }
+            }
+            const cx<T> vk = *vp;
+#pragma unroll
+            for (int i = 0; i < RW; ++i) {
+                acc[J + i].x = fma(vk.x, kw[i], acc[J + i].x);
+                acc[J + i].y = fma(vk.y, kw[i], acc[J + i].y);
+            }
+        }
+    }
+}
+
+// register pairs of rows each lane holds: the tile may be 2 NRH rows high
+constexpr int kSpreadRegRows = 16;
+
+// whether spread_reg_kernel covers a grid's bins: tiles at most 16 columns wide and origin
+// rows r0 <= bin_rows - 1 whose window ends inside the held rows
+__host__ __device__ constexpr bool spread_reg_fits(int w, int bin_rows, int bin_cols) {
+    return w <= 10 && bin_cols + w - 1 <= 16 && bin_rows >= 1 &&
+           (bin_rows - 1) / 2 <= kSpreadRegRows - (w / 2 + 1);
+}
+
+#define PF_ROW_PAIR_CASES(CASE)                                                               \
+    CASE(0) CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8) CASE(9) CASE(10) \
+    CASE(11) CASE(12) CASE(13) CASE(14) CASE(15)
+
+template <int W, class T>
+__global__ void __launch_bounds__(128, 4)
+spread_reg_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
+                  const int* __restrict__ binstart, const int* __restrict__ binorder, int nbusy,
+                  int nbc, int BR, int BC, int64_t M, const double2* __restrict__ fin, int b,
+                  int nrows, int nf2, int row_wrap, int plain, cx<T>* __restrict__ U) {
+    using S = typename SpreadRegLayout<W, T>::type;
+    constexpr bool kPick = std::is_same_v<S, SpreadPickStage<W, T>>;
+    constexpr int RW = S::RW;
+    constexpr int NRH = kSpreadRegRows;
+    static_assert(NRH <= 16, "the row switch names 16 cases");
+    static_assert(W <= 16, "a point's columns fit the 16-column tile");
+    extern __shared__ __align__(16) unsigned char spread_reg_smem[];  // 4 stages
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int h = lane >> 4, c = lane & 15;
+    const int slot = blockIdx.x * 4 + warp;
+    if (slot >= nbusy) return;
+    const int bin = binorder[slot];
+    const int s = binstart[bin], e = binstart[bin + 1];
+    const TileGeom tg = tile_geom<W>(bin, nbc, BR, BC);
+    S& st = reinterpret_cast<S*>(spread_reg_smem)[warp];
+    cx<T>* ub = U + (int64_t)nrows * nf2 * b;
+    {
+        // lane r: where local row r lands in U
+        int gr = tg.tr0 + lane;
+        if (row_wrap) gr = wrap(gr, nrows);
+        st.roff[lane] = (lane < tg.TR && gr >= 0 && gr < nrows) ? (long long)gr * nf2 : -1;
+        if constexpr (kPick) st.vk[lane][W] = Cx<T>::make(0, 0);
+    }
+    cx<T> acc[NRH];
+#pragma unroll
+    for (int i = 0; i < NRH; ++i) acc[i] = Cx<T>::make(0, 0);
+    for (int base = s; base < e; base += 32) {
+        const int nb = min(32, e - base);
+        __syncwarp();
+        int jl = -1;  // this lane's point's origin row pair (-1: none, or outside the tile)
+        if (lane < nb) {
+            const double2 g = pts[base + lane];
+            const double2 v = fin[perm[base + lane] + M * b];
+            int r0, c0;
+            double v1, v2;
+            local_origin<W>(g, tg, nrows, nf2, row_wrap, r0, c0, v1, v2);
+            const bool inside = r0 >= 0 && r0 + W <= tg.TR && c0 >= 0 && c0 + W <= tg.TC;
+            {
+                T k1[W];
+                es_weights<W, T>((T)v1, k1);
+                auto at = [&](int a) -> T { return (a >= 0 && a < W) ? k1[(a >= 0 && a < W) ? a : 0] : (T)0; };
+                if constexpr (kPick) {
+#pragma unroll
+                    for (int n = 0; n < S::NK; ++n) st.k1[lane][n] = at(n - 2);
+                } else {
+                    // even offsets for the half of parity p, odd ones for the other
+                    constexpr int KP = S::KP;
+                    T* w0 = st.kw[lane];
+                    T* w1 = st.kw[lane] + KP;
+                    if (r0 & 1) {
+#pragma unroll
+                        for (int i = 0; i < KP; ++i) {
+                            w0[i] = i < RW ? at(2 * i - 1) : (T)0;
+                            w1[i] = i < RW ? at(2 * i) : (T)0;
+                        }
+                    } else {
+#pragma unroll
+                        for (int i = 0; i < KP; ++i) {
+                            w0[i] = i < RW ? at(2 * i) : (T)0;
+                            w1[i] = i < RW ? at(2 * i + 1) : (T)0;
+                        }
+                    }
+                }
+            }
+            {
+                T k2[W];
+                es_weights<W, T>((T)v2, k2);
+                if constexpr (kPick) {
+#pragma unroll
+                    for (int d = 0; d < W; ++d)
+                        st.vk[lane][d] = Cx<T>::make((T)v.x * k2[d], (T)v.y * k2[d]);
+                    st.org[lane] = make_int2(inside ? r0 : -1, c0);
+                } else {
+                    cx<T>* vr = st.vc[lane];
+#pragma unroll
+                    for (int cc = 0; cc < 16; ++cc) vr[cc] = Cx<T>::make(0, 0);
+                    // (a point outside the tile writes somewhere in its row and is skipped)
+                    vr += min(max(c0, 0), 16 - W);
+#pragma unroll
+                    for (int d = 0; d < W; ++d) vr[d] = Cx<T>::make((T)v.x * k2[d], (T)v.y * k2[d]);
+                }
+            }
+            // a point outside its bin's tile (cannot happen for binned points) is skipped
+            jl = inside ? (r0 >> 1) : -1;
+        }
+        __syncwarp();
+        if constexpr (kPick) {
+            // one switch per run of points of one origin row pair
+            for (int q = 0; q < nb;) {
+                const int r0 = st.org[q].x;
+                if (r0 < 0) {
+                    ++q;
+                    continue;
+                }
+                switch (r0 >> 1) {
+#define PF_RUN_CASE(J) case J: q = add_run<J, W, NRH, T>(st, q, nb, h, c, acc); break;
+                    PF_ROW_PAIR_CASES(PF_RUN_CASE)
+#undef PF_RUN_CASE
+                    default: ++q; break;
+                }
+            }
+        } else {
+            // runs found by a ballot, one switch per run
+            const int jprev = __shfl_up_sync(0xffffffffu, jl, 1);
+            unsigned starts = __ballot_sync(0xffffffffu, lane < nb && (lane == 0 || jl != jprev));
+            while (starts) {
+                const int q0 = __ffs(starts) - 1;
+                starts &= starts - 1;
+                const int q1 = starts ? __ffs(starts) - 1 : nb;
+                switch (__shfl_sync(0xffffffffu, jl, q0)) {
+#define PF_RUN_CASE(J) case J: add_run<J, W, NRH, T>(st, q0, q1, h, c, acc); break;
+                    PF_ROW_PAIR_CASES(PF_RUN_CASE)
+#undef PF_RUN_CASE
+                    default: break;
+                }
+            }
+        }
+    }
+    __syncwarp();
+    if (c < tg.TC) {
+        const int gcol = wrap(tg.tc0 + c, nf2);
+#pragma unroll
+        for (int k = 0; k < NRH; ++k) {
+            const cx<T> v = acc[k];
+            const long long off = st.roff[2 * k + h];
+            if (off >= 0 && (v.x != 0.0 || v.y != 0.0)) {
+                cx<T>* qd = ub + off + gcol;
+                if (plain) {
+                    // no other tile of this launch reaches the cell (bins launched by colour)
+                    cx<T> u = *qd;
+                    u.x += v.x;
+                    u.y += v.y;
+                    *qd = u;
+                } else {
+                    atomicAdd(reinterpret_cast<T*>(qd), v.x);
+                    atomicAdd(reinterpret_cast<T*>(qd) + 1, v.y);
+                }
+            }
+        }
+    }
+}
+#undef PF_ROW_PAIR_CASES
+
 template <int W, class T>
 static int launch_interp(const NufftGrid& g, NufftDev& d, double2* f, int B, cudaStream_t s) {
     const size_t smem = sizeof(cx<T>) * (g.bin_rows + W - 1) * (g.igroup * g.bin_cols + W - 1);
@@ -1273,7 +1564,18 @@ static int launch_spread(const NufftGrid& g, NufftDev& d, const double2* f, int 
             const int n = col ? g.color_off[k + 1] - g.color_off[k] : g.nbusy;
             const int* order = col ? d.sorder.as<int>() + g.color_off[k] : d.binorder.as<int>();
             if (n == 0) continue;
-            if (W <= 10 && g.bin_cols + W - 1 <= 16) {
+            if (g.spread_reg && spread_reg_fits(W, g.bin_rows, g.bin_cols)) {
+                constexpr int WR = W <= 10 ? W : 2;
+                const size_t smem = 4 * sizeof(typename SpreadRegLayout<WR, T>::type);
+                if (smem > 48 * 1024)
+                    PF_CUDA(cudaFuncSetAttribute(spread_reg_kernel<WR, T>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                spread_reg_kernel<WR, T><<<(n + 3) / 4, 128, smem, s>>>(
+                    d.pts.as<double2>(), d.perm.as<int>(), d.binstart.as<int>(), order, n, g.nbc,
+                    g.bin_rows, g.bin_cols, g.M, f, b, g.nrows, g.nf2, g.row_wrap, col ? 1 : 0,
+                    d.U.as<cx<T>>());
+                PF_TRY(check_launch("spread_reg_kernel"));
+            } else if (W <= 10 && g.bin_cols + W - 1 <= 16) {
                 spread16_kernel<(W <= 10 ? W : 2), T><<<(n + 3) / 4, 128, 0, s>>>(
                     d.pts.as<double2>(), d.perm.as<int>(), d.binstart.as<int>(), order, n, g.nbc,
                     g.bin_rows, g.bin_cols, g.M, f, b, g.nrows, g.nf2, g.row_wrap, col ? 1 : 0,

@@ -333,6 +333,7 @@ int build_stretch(pfsht_plan* p, const double* d_theta, const double* d_phi, con
                             o.nufft_nf2, s));
     PF_TRY(nufft_setpts(p->ng, p->nd, Th.as<double>(), ph.as<double>(), s));
     p->ng.plain_transpose = o.nufft_transpose == 1 ? 1 : 0;
+    p->ng.spread_reg = o.nufft_spread == 1 ? 0 : 1;
     p->ng.deterministic = p->deterministic;
     PF_TRY(nufft_alloc(p->ng, p->nd, B));
     return 0;

@@ -230,6 +230,24 @@ def test_tma_transposes_equal_plain_ones(pf, O, cuda, precision, tol):
     assert n.value == 0
 
 
+@pytest.mark.parametrize("precision,tol,B", [("fp64", 1e-8, 1), ("mixed", 1e-6, 1), ("fp64", 1e-8, 2)])
+def test_register_spreading_equals_window_spreading(pf, O, cuda, precision, tol, B):
+    # spreading with each bin's tile held in registers adds the same products in the same order
+    # per cell as the sliding-window kernel: with the deterministic option (plain adds, colour
+    # order) the adjoints agree bit for bit, by default to the order of the atomic additions
+    rng = np.random.default_rng(46)
+    L = 600
+    th, ph = cap_points(70000, rng=rng)
+    kw = dict(lmax=L, tol=tol, precision=precision, ntrans=B, fft_lengths="minimal")
+    g = to_dev(np.asfortranarray(cn(rng, len(th), B)) if B > 1 else cn(rng, len(th)))
+    pr = pf.Plan(th, ph, deterministic=True, **kw)
+    pw = pf.Plan(th, ph, deterministic=True, spread="window", **kw)
+    assert np.array_equal(to_host(pr.H * g), to_host(pw.H * g))
+    ar = to_host(pf.Plan(th, ph, **kw).H * g)
+    aw = to_host(pf.Plan(th, ph, spread="window", **kw).H * g)
+    assert O.alm_reldiff(ar, aw, L) < (2e-6 if precision == "mixed" else 1e-13)
+
+
 @pytest.mark.parametrize("L,B", [(512, 1), (300, 2)])
 def test_async_host_applies_in_flight_together(pf, O, cuda, L, B):
     # pfsht_forward_host_async / pfsht_adjoint_host_async: two rounds of a forward and an adjoint
