@@ -1054,8 +1054,12 @@ static int host_adjoint_pipelined(pfsht_plan* p, const void* in, void* out, cuda
     return 0;
 }
 
+void plan_host_wait(pfsht_plan* p) {
+    if (p->host_zero.valid()) p->host_zero.get();
+}
+
 int plan_host_enqueue(pfsht_plan* p, const void* in, void* out, bool fwd, cudaStream_t s,
-                      bool order_on_s) {
+                      bool order_on_s, bool zero_async) {
     PF_TRY(plan_host_staging(p));
     const size_t nf = sizeof(double2) * (size_t)p->M * p->B;
     if (p->host_pipeline) {
@@ -1063,7 +1067,13 @@ int plan_host_enqueue(pfsht_plan* p, const void* in, void* out, bool fwd, cudaSt
             PF_TRY(host_forward_pipelined(p, in, out, s));
         } else {
             PF_TRY(host_adjoint_pipelined(p, in, out, s));
-            alm_zero_host_padding(p, out);
+            // the padding rows (tens of MB at large lmax) are zeroed while the device works,
+            // so the caller can issue its next apply at once
+            plan_host_wait(p);
+            if (zero_async)
+                p->host_zero = std::async(std::launch::async, [p, out] { alm_zero_host_padding(p, out); });
+            else
+                alm_zero_host_padding(p, out);
         }
     } else {
         // whole copies around the apply on the compute stream
@@ -1096,8 +1106,9 @@ extern "C" {
 static int host_apply(pfsht_plan* p, const void* in, void* out, bool fwd) {
     DeviceGuard dg(p->device);
     cudaStream_t s = p->st_stream;
-    PF_TRY(plan_host_enqueue(p, in, out, fwd, s));
+    PF_TRY(plan_host_enqueue(p, in, out, fwd, s, true, true));
     PF_CUDA(cudaStreamSynchronize(s));
+    plan_host_wait(p);
     return 0;
 }
 
@@ -1126,7 +1137,7 @@ pfsht_status pfsht_adjoint_host(pfsht_plan* p, const void* f, void* alm) {
 static int host_apply_async(pfsht_plan* p, const void* in, void* out, bool fwd, void* stream) {
     DeviceGuard dg(p->device);
     cudaStream_t s = stream ? (cudaStream_t)stream : p->st_stream;
-    return plan_host_enqueue(p, in, out, fwd, s, false);
+    return plan_host_enqueue(p, in, out, fwd, s, false, true);
 }
 
 pfsht_status pfsht_forward_host_async(pfsht_plan* p, const void* alm, void* f, void* stream) {
@@ -1143,6 +1154,7 @@ static int host_sync(pfsht_plan* p) {
     if (!p->d2h) return 0;  // no host apply was issued
     DeviceGuard dg(p->device);
     PF_CUDA(cudaStreamSynchronize(p->d2h));
+    plan_host_wait(p);
     return 0;
 }
 

@@ -3,6 +3,7 @@
 #pragma once
 #include <cufft.h>
 
+#include <future>
 #include <memory>
 #include <vector>
 
@@ -76,7 +77,10 @@ struct pfsht_plan {
     DevBuf gidx, fg, acc;
     pfsht_plan_info info{};
     StageClock clk;
+    // an asynchronous host adjoint's zeroing of its output's padding rows, on a host thread
+    std::future<void> host_zero;
     ~pfsht_plan() {
+        if (host_zero.valid()) host_zero.wait();
         if (have_fth) cufftDestroy(fth);
         if (st_stream) cudaStreamDestroy(st_stream);
         if (side) cudaStreamDestroy(side);
@@ -116,9 +120,12 @@ int plan_adjoint_before_ring(pfsht_plan* p, const double2* f, cudaStream_t s);
 // runs on `s`, the copies on the plan's h2d / d2h streams; with order_on_s the end of the output
 // copy is ordered before whatever is enqueued on `s` afterwards, otherwise only the plan's d2h
 // stream (pfsht_host_sync) marks it. For the adjoint it also zeroes the host array's padding rows
-// on host threads before it returns. The host arrays must stay valid until the copies end.
+// on host threads: before it returns, or with zero_async on a host thread of its own that
+// plan_host_wait joins. The host arrays must stay valid until the copies end.
 int plan_host_enqueue(pfsht_plan* p, const void* in, void* out, bool fwd, cudaStream_t s,
-                      bool order_on_s = true);
+                      bool order_on_s = true, bool zero_async = false);
+// wait for the plan's asynchronous padding zeroing, if one is running
+void plan_host_wait(pfsht_plan* p);
 // allocate the plan's staging buffers for host-buffer applies
 int plan_host_staging(pfsht_plan* p);
 
