@@ -1287,9 +1287,12 @@ spread16_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
 template <int W, class T>
 struct SpreadPickStage {
     static constexpr int RW = W / 2 + 1;       // registers a point reaches in one half
-    static constexpr int NK = 2 * RW + 2;      // [0, 0, k_0 .. k_{W-1}, 0 ..]
+    // [0, 0, k_0 .. k_{W-1}, 0 ..]; both rows an odd number of elements long, so that the lanes'
+    // stores of their points' rows fall in distinct banks
+    static constexpr int NK = 2 * RW + 3;
+    static constexpr int NV = (W + 1) % 2 ? W + 1 : W + 2;
     T k1[32][NK];              // row weights, zero-padded
-    cx<T> vk[32][W + 1];       // value x column weight; slot W is 0 for lanes off the point
+    cx<T> vk[32][NV];          // value x column weight; slot W is 0 for lanes off the point
     int2 org[32];              // origin row (or -1: skip) and column inside the tile
     long long roff[32];        // element offset of local row r in U (or -1: outside the grid)
 };
@@ -1302,7 +1305,7 @@ struct SpreadRowStage {
     // rows padded to odd multiples of 16 bytes: the lanes' 16-byte stores of their points'
     // rows fall in distinct banks
     static constexpr int KS = 2 * KP + VPL;
-    static constexpr int NV = 16 + 16 / (int)sizeof(cx<T>);
+    static constexpr int NV = 17;  // an odd number of values, for the same reason
     alignas(16) T kw[32][KS];  // [point][half KP + i]: weight of register j + i (0-padded)
     cx<T> vc[32][NV];          // [point][column]: value x column weight (0 off the point)
     long long roff[32];
@@ -1444,22 +1447,32 @@ spread_reg_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
 #pragma unroll
                     for (int n = 0; n < S::NK; ++n) st.k1[lane][n] = at(n - 2);
                 } else {
-                    // even offsets for the half of parity p, odd ones for the other
+                    // even offsets for the half of parity p, odd ones for the other, stored
+                    // as 16-byte vectors
                     constexpr int KP = S::KP;
-                    T* w0 = st.kw[lane];
-                    T* w1 = st.kw[lane] + KP;
+                    T w[2 * KP];
                     if (r0 & 1) {
 #pragma unroll
                         for (int i = 0; i < KP; ++i) {
-                            w0[i] = i < RW ? at(2 * i - 1) : (T)0;
-                            w1[i] = i < RW ? at(2 * i) : (T)0;
+                            w[i] = i < RW ? at(2 * i - 1) : (T)0;
+                            w[KP + i] = i < RW ? at(2 * i) : (T)0;
                         }
                     } else {
 #pragma unroll
                         for (int i = 0; i < KP; ++i) {
-                            w0[i] = i < RW ? at(2 * i) : (T)0;
-                            w1[i] = i < RW ? at(2 * i + 1) : (T)0;
+                            w[i] = i < RW ? at(2 * i) : (T)0;
+                            w[KP + i] = i < RW ? at(2 * i + 1) : (T)0;
                         }
+                    }
+                    if constexpr (sizeof(T) == 8) {
+#pragma unroll
+                        for (int u = 0; u < KP; ++u)
+                            reinterpret_cast<double2*>(st.kw[lane])[u] = make_double2(w[2 * u], w[2 * u + 1]);
+                    } else {
+#pragma unroll
+                        for (int u = 0; u < KP / 2; ++u)
+                            reinterpret_cast<float4*>(st.kw[lane])[u] =
+                                make_float4(w[4 * u], w[4 * u + 1], w[4 * u + 2], w[4 * u + 3]);
                     }
                 }
             }
