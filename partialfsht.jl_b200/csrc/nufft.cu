@@ -229,7 +229,7 @@ int interp_point_order(const NufftGrid& g, NufftDev& d, const std::vector<int>& 
     PF_CUDA(cudaMemcpyAsync(perm.data(), d.perm.p, sizeof(int) * M, cudaMemcpyDeviceToHost, s));
     PF_CUDA(cudaStreamSynchronize(s));
     const int W = g.w, KM = g.fp32 ? 16 : 8;
-    const int G = g.igroup, TC = G * g.bin_cols + W - 1;
+    const int G = g.igroup, TS = (G * g.bin_cols + W - 1) | 1;  // the kernel's tile row stride
     std::vector<double2> opts(M);
     std::vector<int> operm(M);
     std::vector<std::vector<int>> bucket(KM);
@@ -244,7 +244,7 @@ int interp_point_order(const NufftGrid& g, NufftDev& d, const std::vector<int>& 
             if (g.row_wrap) r = ((r % g.nrows) + g.nrows) % g.nrows;
             int c = (int)std::ceil(pts[i].y - 0.5 * W);
             c = ((c % g.nf2) + g.nf2) % g.nf2;
-            const int64_t off = (int64_t)(r - tr0) * TC + (c - tc0);
+            const int64_t off = (int64_t)(r - tr0) * TS + (c - tc0);
             bucket[(int)(((off % KM) + KM) % KM)].push_back(i);
         }
         int o = a;
@@ -885,6 +885,9 @@ interp_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
     // the tile is at most 32 columns wide (G BC <= 33 - W): lane = column, warps stride the rows
     const int wid = threadIdx.x >> 5, ln = threadIdx.x & 31, nw = blockDim.x >> 5;
     const int gcol = wrap(tg.tc0 + ln, nf2);
+    // tile rows an odd number of elements apart: a tap's bank class then depends on its row as
+    // well as its column, which evens out the classes the points are dealt over
+    const int TS = tg.TC | 1;
     for (int b = 0; b < B; ++b) {
         const cx<T>* ub = U + (int64_t)nrows * nf2 * b;
         if (tg.TC <= 32) {
@@ -894,7 +897,7 @@ interp_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
                     if (row_wrap) r = wrap(r, nrows);
                     cx<T> v = Cx<T>::make(0, 0);
                     if (r >= 0 && r < nrows) v = ub[(int64_t)r * nf2 + gcol];
-                    tile[rr * tg.TC + ln] = v;
+                    tile[rr * TS + ln] = v;
                 }
             }
         } else {
@@ -903,7 +906,7 @@ interp_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
                 if (row_wrap) r = wrap(r, nrows);
                 cx<T> v = Cx<T>::make(0, 0);
                 if (r >= 0 && r < nrows) v = ub[(int64_t)r * nf2 + wrap(tg.tc0 + t % tg.TC, nf2)];
-                tile[t] = v;
+                tile[(t / tg.TC) * TS + t % tg.TC] = v;
             }
         }
         // FP32 grids: the first point's coordinates load while the tile copy completes and
@@ -941,7 +944,7 @@ interp_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
             if (r0 >= 0 && r0 + W <= tg.TR && c0 >= 0 && c0 + W <= tg.TC) {
                 const T w1 = (T)v1, u1 = w1 * w1;
                 auto row_sum = [&](int a) {
-                    const cx<T>* row = tile + (r0 + a) * tg.TC + c0;
+                    const cx<T>* row = tile + (r0 + a) * TS + c0;
                     cx<T> sr = Cx<T>::make(0, 0);
 #pragma unroll
                     for (int c = 0; c < W; ++c) {
@@ -1557,7 +1560,7 @@ spread_reg_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
 
 template <int W, class T>
 static int launch_interp(const NufftGrid& g, NufftDev& d, double2* f, int B, cudaStream_t s) {
-    const size_t smem = sizeof(cx<T>) * (g.bin_rows + W - 1) * (g.igroup * g.bin_cols + W - 1);
+    const size_t smem = sizeof(cx<T>) * (g.bin_rows + W - 1) * ((g.igroup * g.bin_cols + W - 1) | 1);
     if (smem > 48 * 1024)
         PF_CUDA(cudaFuncSetAttribute(interp_kernel<W, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     interp_kernel<W, T><<<g.nisb, 128, smem, s>>>(
