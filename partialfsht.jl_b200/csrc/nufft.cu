@@ -909,19 +909,19 @@ interp_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
                 tile[(t / tg.TC) * TS + t % tg.TC] = v;
             }
         }
-        // FP32 grids: the first point's coordinates load while the tile copy completes and
-        // each later point's load is issued one iteration ahead (in FP64 the extra registers
-        // cost more occupancy than the hidden latency gains)
+        // each thread's first point loads while the tile copy completes; FP32 grids also issue
+        // each later point's load one iteration ahead (in FP64 the extra registers would cost
+        // more occupancy than the hidden latency gains)
         constexpr bool kAhead = sizeof(T) == 4;
         int p = s + threadIdx.x;
         double2 gn = make_double2(0.0, 0.0);
         int jn = 0;
-        if (kAhead && p < e) {
+        if (p < e) {
             gn = pts[p];
             jn = perm[p];
         }
         __syncthreads();
-        for (; p < e; p += blockDim.x) {
+        for (bool first = true; p < e; p += blockDim.x, first = false) {
             double2 g;
             int j;
             if constexpr (kAhead) {
@@ -932,8 +932,14 @@ interp_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
                     jn = perm[p + blockDim.x];
                 }
             } else {
-                g = pts[p];
-                j = perm[p];
+                // FP64: only each thread's first point is loaded under the tile copy
+                if (first) {
+                    g = gn;
+                    j = jn;
+                } else {
+                    g = pts[p];
+                    j = perm[p];
+                }
             }
             int r0, c0;
             double v1, v2;
