@@ -248,6 +248,24 @@ def test_register_spreading_equals_window_spreading(pf, O, cuda, precision, tol,
     assert O.alm_reldiff(ar, aw, L) < (2e-6 if precision == "mixed" else 1e-13)
 
 
+@pytest.mark.parametrize("bin_rows,bin_cols", [(32, 0), (9, 4), (1, 1)])
+def test_spreading_bin_shapes(pf, O, cuda, bin_rows, bin_cols):
+    # bins taller than the register tile holds (32 rows at w = 9) fall back to the sliding
+    # window; short and narrow bins use the register tile with few row pairs: every shape gives
+    # the default plan's adjoint to the order of the atomic additions, and its forward
+    rng = np.random.default_rng(47)
+    L = 400
+    th, ph = cap_points(40000, rng=rng)
+    kw = dict(lmax=L, tol=1e-8, fft_lengths="minimal")
+    g = to_dev(cn(rng, len(th)))
+    alm = O.rand_alm(L, rng=rng)
+    pd = pf.Plan(th, ph, **kw)
+    ps = pf.Plan(th, ph, bin_rows=bin_rows, bin_cols=bin_cols, **kw)
+    assert O.alm_reldiff(to_host(ps.H * g), to_host(pd.H * g), L) < 1e-13
+    fd, fs = _fwd(pd, alm), _fwd(ps, alm)
+    assert np.max(np.abs(fs - fd)) <= 1e-13 * np.max(np.abs(fd))
+
+
 @pytest.mark.parametrize("L,B", [(512, 1), (300, 2)])
 def test_async_host_applies_in_flight_together(pf, O, cuda, L, B):
     # pfsht_forward_host_async / pfsht_adjoint_host_async: two rounds of a forward and an adjoint
