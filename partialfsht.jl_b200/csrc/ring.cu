@@ -39,7 +39,7 @@
 namespace pf {
 
 static constexpr int kWarpsPerBlock = 4;  // forward
-static constexpr int kAdjWarps = 2;       // adjoint
+static constexpr int kAdjWarps = 1;       // adjoint (one-warp blocks: a finer tail)
 
 // ---------------------------------------------------------------------------------------
 // recurrence coefficient table (beta_l, g_l), from the exact expressions of
