@@ -700,6 +700,47 @@ __device__ __forceinline__ void ring_adj_item(const RingTables& t, const RingOut
         }
     };
     const bool seeded = item.ck < 0;
+    // every global load of the item's start is issued before any of them is used: the first
+    // chunk's recurrence coefficients, the ring data, then the seeds or checkpoints
+    const int lfirst = seeded ? m + 2 : item.lbeg;
+    double2 bg_first = make_double2(0.0, 0.0);
+    if (lfirst <= item.lend && lane <= item.lend - lfirst) bg_first = abm[lfirst + lane - m - 2];
+    double2 rp[R][NB], rm[R][NB];
+    double wr[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int k = lane + 32 * r;
+        wr[r] = 1.0;
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            rp[r][b] = make_double2(0.0, 0.0);
+            rm[r][b] = make_double2(0.0, 0.0);
+        }
+        if (k < item.n) {
+            const int j = item.j0 + k;
+            if (t.w) wr[r] = t.w[j];
+#pragma unroll
+            for (int b = 0; b < NB; ++b) {
+                const double2* ib = in + o.bstride * (b0 + b);
+                double2 v = ib[j + o.ld * (o.col_off + m)];
+                if (o.reflect) {
+                    const double2 u = ib[(o.nrows - 1 - j) + o.ld * (o.col_off + m)];
+                    v.x += smir * u.x;
+                    v.y += smir * u.y;
+                }
+                rp[r][b] = v;
+                if (m > 0) {
+                    double2 u = ib[j + o.ld * (o.col_off - m)];
+                    if (o.reflect) {
+                        const double2 q = ib[(o.nrows - 1 - j) + o.ld * (o.col_off - m)];
+                        u.x += smir * q.x;
+                        u.y += smir * q.y;
+                    }
+                    rm[r][b] = u;
+                }
+            }
+        }
+    }
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int k = lane + 32 * r;
@@ -718,7 +759,17 @@ __device__ __forceinline__ void ring_adj_item(const RingTables& t, const RingOut
                 E[r] = t.ck_E[item.ck + k];
             }
         }
-        load_g(r);
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int k = lane + 32 * r;
+        const bool live = k < item.n && E[r] >= kZeroE;
+        const double sc = live ? scalbn(wr[r], E[r]) : 0.0;
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            gp[r][b] = live ? put(rp[r][b].x * sc, rp[r][b].y * sc) : put(0.0, 0.0);
+            gm[r][b] = live ? put(rm[r][b].x * sc * sgn, rm[r][b].y * sc * sgn) : put(0.0, 0.0);
+        }
     }
     // partial sums over this lane's rings for degree slot `slot`
     auto stage = [&](const double (&P)[R], int slot) {
@@ -821,8 +872,7 @@ __device__ __forceinline__ void ring_adj_item(const RingTables& t, const RingOut
         }
     };
     // the coefficients of the next 32 degrees are loaded while this chunk runs
-    double2 bg_next = make_double2(0.0, 0.0);
-    if (lstart <= item.lend && lane <= item.lend - lstart) bg_next = abm[lstart + lane - m - 2];
+    double2 bg_next = bg_first;  // lstart == lfirst here
     // segments start on the renormalisation schedule, so the count restarts at 0
     int steps = 0;
     for (int l0 = lstart; l0 <= item.lend; l0 += 32) {
