@@ -303,6 +303,7 @@ struct NufftGrid {
     int gap_lo = 0, gap_hi = 0, gap_ok = 0;
     int plain_transpose = 0;   // 1: the plain-load transposes only
     int spread_reg = 1;        // spreading holds each bin's tile in registers where it fits
+    int interp_pipe = 1;       // one-transform interpolation copies the next group's tile ahead
 };
 
 struct NufftDev {
@@ -320,6 +321,7 @@ struct NufftDev {
     DevBuf dec2;      // double ncols: deconvolution along dim 2
     DevBuf pad;       // double2 nf1 x ncols x B
     DevBuf U;         // double2 nrows x nf2 x B
+    DevBuf counter;   // int: the next interpolation group to pull
     cufftHandle f1 = 0, f2 = 0;
     bool have_f1 = false, have_f2 = false;
     // 2-D tensor maps of pad (nf1 x ncols B) and U (nf2 x nrows B) for the TMA row transposes

@@ -469,6 +469,7 @@ int nufft_alloc(NufftGrid& g, NufftDev& d, int B) {
     const cufftType ty = g.fp32 ? CUFFT_C2C : CUFFT_Z2Z;
     PF_TRY(d.pad.alloc(el * (size_t)g.nf1 * g.ncols * B));
     PF_TRY(d.U.alloc(el * (size_t)g.nrows * g.nf2 * B));
+    PF_TRY(d.counter.alloc(sizeof(int)));
     int n1[1] = {g.nf1};
     PF_CUFFT(cufftPlanMany(&d.f1, 1, n1, n1, 1, g.nf1, n1, 1, g.nf1, ty, g.ncols * B));
     d.have_f1 = true;
@@ -864,6 +865,52 @@ __device__ __forceinline__ void es_weights(T v, T (&k)[W]) {
     }
 }
 
+// one point's interpolation from its group's tile (rows TS elements apart): the w x w taps,
+// rows in mirrored pairs with the column weights held in registers; 0 for a point outside the
+// tile (which binning excludes)
+template <int W, class T>
+__device__ __forceinline__ cx<T> interp_point(double2 g, const TileGeom& tg, int TS,
+                                              const cx<T>* tile, int nrows, int nf2, int row_wrap) {
+    int r0, c0;
+    double v1, v2;
+    local_origin<W>(g, tg, nrows, nf2, row_wrap, r0, c0, v1, v2);
+    T k2[W];
+    es_weights<W, T>((T)v2, k2);
+    cx<T> acc = Cx<T>::make(0, 0);
+    if (r0 >= 0 && r0 + W <= tg.TR && c0 >= 0 && c0 + W <= tg.TC) {
+        const T w1 = (T)v1, u1 = w1 * w1;
+        auto row_sum = [&](int a) {
+            const cx<T>* row = tile + (r0 + a) * TS + c0;
+            cx<T> sr = Cx<T>::make(0, 0);
+#pragma unroll
+            for (int c = 0; c < W; ++c) {
+                const cx<T> u = row[c];
+                sr.x = fma(u.x, k2[c], sr.x);
+                sr.y = fma(u.y, k2[c], sr.y);
+            }
+            return sr;
+        };
+        // rows in mirrored pairs (a, W - 1 - a): one pair of row weights at a time
+#pragma unroll
+        for (int a = 0; a < W / 2; ++a) {
+            T ka, kb;
+            es_pair<W, T>(a, w1, u1, ka, kb);
+            const cx<T> sa = row_sum(a), sb = row_sum(W - 1 - a);
+            acc.x = fma(sa.x, ka, acc.x);
+            acc.y = fma(sa.y, ka, acc.y);
+            acc.x = fma(sb.x, kb, acc.x);
+            acc.y = fma(sb.y, kb, acc.y);
+        }
+        if constexpr (W & 1) {
+            const T km = es_mid<W, T>(u1);
+            const cx<T> sm = row_sum(W / 2);
+            acc.x = fma(sm.x, km, acc.x);
+            acc.y = fma(sm.y, km, acc.y);
+        }
+    }
+    return acc;
+}
+
 // Type-2 interpolation: one CTA per group of consecutive bins of a bin row copies the group's
 // tile of U (at most 32 columns) into shared memory, then each thread interpolates points of
 // the group from it. The row weights are evaluated row by
@@ -941,47 +988,95 @@ interp_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
                     j = perm[p];
                 }
             }
-            int r0, c0;
-            double v1, v2;
-            local_origin<W>(g, tg, nrows, nf2, row_wrap, r0, c0, v1, v2);
-            T k2[W];
-            es_weights<W, T>((T)v2, k2);
-            cx<T> acc = Cx<T>::make(0, 0);
-            if (r0 >= 0 && r0 + W <= tg.TR && c0 >= 0 && c0 + W <= tg.TC) {
-                const T w1 = (T)v1, u1 = w1 * w1;
-                auto row_sum = [&](int a) {
-                    const cx<T>* row = tile + (r0 + a) * TS + c0;
-                    cx<T> sr = Cx<T>::make(0, 0);
-#pragma unroll
-                    for (int c = 0; c < W; ++c) {
-                        const cx<T> u = row[c];
-                        sr.x = fma(u.x, k2[c], sr.x);
-                        sr.y = fma(u.y, k2[c], sr.y);
-                    }
-                    return sr;
-                };
-                // rows in mirrored pairs (a, W - 1 - a): one pair of row weights at a time
-#pragma unroll
-                for (int a = 0; a < W / 2; ++a) {
-                    T ka, kb;
-                    es_pair<W, T>(a, w1, u1, ka, kb);
-                    const cx<T> sa = row_sum(a), sb = row_sum(W - 1 - a);
-                    acc.x = fma(sa.x, ka, acc.x);
-                    acc.y = fma(sa.y, ka, acc.y);
-                    acc.x = fma(sb.x, kb, acc.x);
-                    acc.y = fma(sb.y, kb, acc.y);
-                }
-                if constexpr (W & 1) {
-                    const T km = es_mid<W, T>(u1);
-                    const cx<T> sm = row_sum(W / 2);
-                    acc.x = fma(sm.x, km, acc.x);
-                    acc.y = fma(sm.y, km, acc.y);
-                }
-            }
+            const cx<T> acc = interp_point<W, T>(g, tg, TS, tile, nrows, nf2, row_wrap);
             f[j + M * b] = make_double2((double)acc.x, (double)acc.y);
         }
         __syncthreads();
     }
+}
+
+// asynchronous global -> shared copy of one grid value, or zeros (src_bytes = 0); each thread
+// later waits for its own copies
+template <class T>
+__device__ __forceinline__ void cp_async_value(cx<T>* dst, const cx<T>* src, bool valid) {
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+    const int n = valid ? (int)sizeof(cx<T>) : 0;
+    if constexpr (sizeof(cx<T>) == 16)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(n)
+                     : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(n)
+                     : "memory");
+}
+
+// Type-2 interpolation, pipelined (one transform): a resident grid of blocks pulls groups of
+// bins from a counter, heaviest first; while a block interpolates the points of one group from
+// its tile, the next group's tile is copied into the other half of its shared memory with
+// cp.async, so the copy's latency is not exposed between groups. Points and results as in
+// interp_kernel.
+template <int W, class T>
+__global__ void __launch_bounds__(128, sizeof(T) == 8 ? 5 : 4)
+interp_pipe_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
+                   const int* __restrict__ binstart, const int* __restrict__ iorder, int ngroups,
+                   int nbc, int G, int nsbc, int BR, int BC, const cx<T>* __restrict__ U, int nrows,
+                   int nf2, int row_wrap, int tile_elems, double2* __restrict__ f,
+                   int* __restrict__ counter) {
+    extern __shared__ __align__(16) unsigned char interp_smem[];
+    cx<T>* tiles = reinterpret_cast<cx<T>*>(interp_smem);  // two tiles of tile_elems values
+    __shared__ int s_next;
+    const int wid = threadIdx.x >> 5, ln = threadIdx.x & 31, nw = blockDim.x >> 5;
+    auto geom = [&](int q) {
+        const int sb = iorder[q];
+        const int br = sb / nsbc, sg = sb % nsbc;
+        return TileGeom{br * BR, sg * G * BC, BR + W - 1, G * BC + W - 1};
+    };
+    // the tile is at most 32 columns wide (G BC <= 33 - W): lane = column, warps stride the rows
+    auto copy_tile = [&](int q, cx<T>* tile) {
+        const TileGeom tg = geom(q);
+        const int TS = tg.TC | 1;
+        if (ln < tg.TC) {
+            const int gcol = wrap(tg.tc0 + ln, nf2);
+            for (int rr = wid; rr < tg.TR; rr += nw) {
+                int r = tg.tr0 + rr;
+                if (row_wrap) r = wrap(r, nrows);
+                const bool ok = r >= 0 && r < nrows;
+                cp_async_value<T>(tile + rr * TS + ln, U + (ok ? (int64_t)r * nf2 + gcol : 0), ok);
+            }
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    };
+    if (threadIdx.x == 0) s_next = atomicAdd(counter, 1);
+    __syncthreads();
+    int cur = s_next;
+    if (cur >= ngroups) return;
+    copy_tile(cur, tiles);
+    for (int buf = 0;; buf ^= 1) {
+        __syncthreads();  // every thread has read s_next
+        if (threadIdx.x == 0) s_next = atomicAdd(counter, 1);
+        __syncthreads();
+        const int nxt = s_next;
+        if (nxt < ngroups) copy_tile(nxt, tiles + (buf ^ 1) * tile_elems);
+        else asm volatile("cp.async.commit_group;\n" ::: "memory");
+        // this thread's copies of the current tile are done; the barrier makes everyone's visible
+        asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+        __syncthreads();
+        const TileGeom tg = geom(cur);
+        const int sb = iorder[cur];
+        const int br = sb / nsbc, sg = sb % nsbc;
+        const int s = binstart[br * nbc + sg * G];
+        const int e = binstart[br * nbc + min(nbc, sg * G + G)];
+        const cx<T>* tile = tiles + buf * tile_elems;
+        for (int p = s + threadIdx.x; p < e; p += blockDim.x) {
+            const double2 g = pts[p];
+            const int j = perm[p];
+            const cx<T> acc = interp_point<W, T>(g, tg, tg.TC | 1, tile, nrows, nf2, row_wrap);
+            f[j] = make_double2((double)acc.x, (double)acc.y);
+        }
+        __syncthreads();  // the tile is read before it is refilled
+        if (nxt >= ngroups) break;
+        cur = nxt;
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
 // Type-1 spreading, output stationary: one warp per bin, lane l owns tile column l (the
@@ -1564,9 +1659,34 @@ spread_reg_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
 }
 #undef PF_ROW_PAIR_CASES
 
+// groups per resident block from which the one-transform interpolation is pipelined
+constexpr int kInterpPipeGroups = 4;
+
 template <int W, class T>
 static int launch_interp(const NufftGrid& g, NufftDev& d, double2* f, int B, cudaStream_t s) {
-    const size_t smem = sizeof(cx<T>) * (g.bin_rows + W - 1) * ((g.igroup * g.bin_cols + W - 1) | 1);
+    const int tile_elems = (g.bin_rows + W - 1) * ((g.igroup * g.bin_cols + W - 1) | 1);
+    if (B == 1 && g.interp_pipe && g.igroup * g.bin_cols + W - 1 <= 32 && g.nisb > 0) {
+        const size_t smem2 = 2 * sizeof(cx<T>) * (size_t)tile_elems;
+        if (smem2 > 48 * 1024)
+            PF_CUDA(cudaFuncSetAttribute(interp_pipe_kernel<W, T>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
+        int per = 0, dev = 0, nsm = 0;
+        PF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, interp_pipe_kernel<W, T>, 128, smem2));
+        PF_CUDA(cudaGetDevice(&dev));
+        PF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        const int grid = std::max(1, std::min(g.nisb, std::max(1, per) * nsm));
+        // the copy ahead pays once each resident block takes several groups (measured: 3-4%
+        // faster at lmax 2048, 4 to 8 groups per block; 32% slower at lmax 1024, under 2)
+        if (g.nisb >= kInterpPipeGroups * grid) {
+            PF_CUDA(cudaMemsetAsync(d.counter.p, 0, sizeof(int), s));
+            interp_pipe_kernel<W, T><<<grid, 128, smem2, s>>>(
+                d.ipts.as<double2>(), d.iperm.as<int>(), d.binstart.as<int>(), d.iorder.as<int>(),
+                g.nisb, g.nbc, g.igroup, g.nsbc, g.bin_rows, g.bin_cols, d.U.as<cx<T>>(), g.nrows,
+                g.nf2, g.row_wrap, tile_elems, f, d.counter.as<int>());
+            return check_launch("interp_pipe_kernel");
+        }
+    }
+    const size_t smem = sizeof(cx<T>) * (size_t)tile_elems;
     if (smem > 48 * 1024)
         PF_CUDA(cudaFuncSetAttribute(interp_kernel<W, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     interp_kernel<W, T><<<g.nisb, 128, smem, s>>>(
