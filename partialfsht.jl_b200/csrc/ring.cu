@@ -40,6 +40,7 @@ namespace pf {
 
 static constexpr int kWarpsPerBlock = 4;  // forward
 static constexpr int kAdjWarps = 1;       // adjoint (one-warp blocks: a finer tail)
+static constexpr int kAdjWarpsPersistent = 2;  // the batches' persistent adjoint (measured faster)
 
 // ---------------------------------------------------------------------------------------
 // recurrence coefficient table (beta_l, g_l), from the exact expressions of
@@ -1308,10 +1309,10 @@ ring_fwd_persistent_kernel(const RingSlot* __restrict__ slots, const BatchItem* 
     }
 }
 
-__global__ void __launch_bounds__(kAdjWarps * 32)
+__global__ void __launch_bounds__(kAdjWarpsPersistent * 32)
 ring_adj_persistent_kernel(const RingSlot* __restrict__ slots, const BatchItem* __restrict__ items,
                            int nitems, void* const* __restrict__ ptrs, int* __restrict__ counter) {
-    __shared__ AdjAnySmem sm[kAdjWarps];
+    __shared__ AdjAnySmem sm[kAdjWarpsPersistent];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int it = pull_item(counter, lane); it < nitems; it = pull_item(counter, lane)) {
         const BatchItem bi = items[it];
@@ -1366,10 +1367,10 @@ int build_ring_merged(const std::vector<RingBatchPlan>& plans, bool adjoint, Rin
     PF_CUDA(cudaGetDevice(&dev));
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (adjoint)
-        PF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, ring_adj_persistent_kernel, kAdjWarps * 32, 0));
+        PF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, ring_adj_persistent_kernel, kAdjWarpsPersistent * 32, 0));
     else
         PF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, ring_fwd_persistent_kernel, kWarpsPerBlock * 32, 0));
-    const int wpb = adjoint ? kAdjWarps : kWarpsPerBlock;
+    const int wpb = adjoint ? kAdjWarpsPersistent : kWarpsPerBlock;
     mg.grid = std::max(1, std::min(sms * std::max(1, per), (mg.nitems + wpb - 1) / wpb));
     return 0;
 }
@@ -1379,7 +1380,7 @@ int ring_merged_launch(const RingSlot* slots, const RingMerged& mg, bool adjoint
     if (mg.nitems == 0) return 0;
     PF_CUDA(cudaMemsetAsync(mg.counter.p, 0, sizeof(int), s));
     if (adjoint) {
-        ring_adj_persistent_kernel<<<mg.grid, kAdjWarps * 32, 0, s>>>(slots, mg.items.as<BatchItem>(),
+        ring_adj_persistent_kernel<<<mg.grid, kAdjWarpsPersistent * 32, 0, s>>>(slots, mg.items.as<BatchItem>(),
                                                                       mg.nitems, ptrs, mg.counter.as<int>());
         return check_launch("ring_adj_persistent_kernel");
     }
