@@ -313,6 +313,8 @@ struct NufftDev {
     DevBuf binorder;  // int32 nbusy: non-empty bins, most points first
     DevBuf iorder;    // int32 nisb: non-empty interpolation groups, most points first
     DevBuf sorder;    // int32 nbusy: non-empty bins by spreading colour, most points first in each
+    DevBuf bslot;     // int4 nbusy: (bin, first point, end, 0) in binorder's order
+    DevBuf sslot;     // int4 nbusy: the same in sorder's order
     DevBuf ipts;      // double2: pts in the interpolation's order (each group's points dealt over
     DevBuf iperm;     // int32    their shared-memory bank class), and their original indices
     DevBuf colp2;     // int32 ncols: fine column of each mode column

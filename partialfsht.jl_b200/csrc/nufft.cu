@@ -354,6 +354,20 @@ int nufft_setpts(NufftGrid& g, NufftDev& d, const double* x, const double* y, cu
         if (!sord.empty())
             PF_CUDA(cudaMemcpyAsync(d.sorder.p, sord.data(), sizeof(int) * sord.size(),
                                     cudaMemcpyHostToDevice, s));
+        // the register-tile spreading reads a bin's number and point range in one load
+        std::vector<int> first(nbins + 1, 0);
+        for (int b = 0; b < nbins; ++b) first[b + 1] = first[b] + cnt[b];
+        auto slots = [&](const std::vector<int>& ord, DevBuf& out) -> int {
+            std::vector<int4> v(std::max<size_t>(ord.size(), 1), make_int4(0, 0, 0, 0));
+            for (size_t i = 0; i < ord.size(); ++i)
+                v[i] = make_int4(ord[i], first[ord[i]], first[ord[i] + 1], 0);
+            PF_TRY(out.alloc(sizeof(int4) * v.size()));
+            PF_CUDA(cudaMemcpyAsync(out.p, v.data(), sizeof(int4) * v.size(), cudaMemcpyHostToDevice, s));
+            PF_CUDA(cudaStreamSynchronize(s));
+            return 0;
+        };
+        PF_TRY(slots(order, d.bslot));
+        PF_TRY(slots(sord, d.sslot));
     }
     // interpolation groups igroup consecutive bins of a bin row; non-empty groups, most
     // points first
@@ -1503,9 +1517,9 @@ __host__ __device__ constexpr bool spread_reg_fits(int w, int bin_rows, int bin_
 template <int W, class T>
 __global__ void __launch_bounds__(128, 4)
 spread_reg_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
-                  const int* __restrict__ binstart, const int* __restrict__ binorder, int nbusy,
-                  int nbc, int BR, int BC, int64_t M, const double2* __restrict__ fin, int b,
-                  int nrows, int nf2, int row_wrap, int plain, cx<T>* __restrict__ U) {
+                  const int4* __restrict__ slots, int nbusy, int nbc, int BR, int BC, int64_t M,
+                  const double2* __restrict__ fin, int b, int nrows, int nf2, int row_wrap,
+                  int plain, cx<T>* __restrict__ U) {
     using S = typename SpreadRegLayout<W, T>::type;
     constexpr bool kPick = std::is_same_v<S, SpreadPickStage<W, T>>;
     constexpr int RW = S::RW;
@@ -1517,8 +1531,8 @@ spread_reg_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
     const int h = lane >> 4, c = lane & 15;
     const int slot = blockIdx.x * 4 + warp;
     if (slot >= nbusy) return;
-    const int bin = binorder[slot];
-    const int s = binstart[bin], e = binstart[bin + 1];
+    const int4 sl = slots[slot];  // bin, first point, end
+    const int bin = sl.x, s = sl.y, e = sl.z;
     const TileGeom tg = tile_geom<W>(bin, nbc, BR, BC);
     S& st = reinterpret_cast<S*>(spread_reg_smem)[warp];
     cx<T>* ub = U + (int64_t)nrows * nf2 * b;
@@ -1712,10 +1726,10 @@ static int launch_spread(const NufftGrid& g, NufftDev& d, const double2* f, int 
                 if (smem > 48 * 1024)
                     PF_CUDA(cudaFuncSetAttribute(spread_reg_kernel<WR, T>,
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                const int4* sl = col ? d.sslot.as<int4>() + g.color_off[k] : d.bslot.as<int4>();
                 spread_reg_kernel<WR, T><<<(n + 3) / 4, 128, smem, s>>>(
-                    d.pts.as<double2>(), d.perm.as<int>(), d.binstart.as<int>(), order, n, g.nbc,
-                    g.bin_rows, g.bin_cols, g.M, f, b, g.nrows, g.nf2, g.row_wrap, col ? 1 : 0,
-                    d.U.as<cx<T>>());
+                    d.pts.as<double2>(), d.perm.as<int>(), sl, n, g.nbc, g.bin_rows, g.bin_cols,
+                    g.M, f, b, g.nrows, g.nf2, g.row_wrap, col ? 1 : 0, d.U.as<cx<T>>());
                 PF_TRY(check_launch("spread_reg_kernel"));
             } else if (W <= 10 && g.bin_cols + W - 1 <= 16) {
                 spread16_kernel<(W <= 10 ? W : 2), T><<<(n + 3) / 4, 128, 0, s>>>(

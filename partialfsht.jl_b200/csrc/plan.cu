@@ -215,6 +215,8 @@ void fill_info(pfsht_plan* p) {
     for (const DevBuf* b : {&p->cos_t, &p->log2sin, &p->log2c, &p->w, &p->ab, &p->aboff, &p->fwd_items.items, &p->adj_items.items,
                             &p->adj_seg.ck_p, &p->adj_seg.ck_E,
                             &p->H, &p->phi_pts, &p->nd.pts, &p->nd.perm, &p->nd.binstart,
+                            &p->nd.binorder, &p->nd.sorder, &p->nd.bslot, &p->nd.sslot,
+                            &p->nd.iorder, &p->nd.ipts, &p->nd.iperm, &p->nd.counter,
                             &p->nd.colp2, &p->nd.p2col, &p->nd.mult1, &p->nd.dec2, &p->nd.pad,
                             &p->nd.U, &p->st_alm, &p->st_f, &p->ab_fwd, &p->st_alm2,
                             &p->st_f2, &p->blk_fwd_items, &p->blk_adj_items})
