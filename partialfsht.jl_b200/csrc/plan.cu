@@ -17,7 +17,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <memory>
+#include <queue>
 #include <string>
 #include <vector>
 
@@ -231,6 +233,56 @@ void fill_info(pfsht_plan* p) {
 // unsplit items would give fewer than ~8 warps per resident warp slot (12 per SM at the
 // adjoint's register count). The saved recurrence state is bounded by 512 MiB; past that, or
 // with seg_degrees < 0, the items stay whole.
+// Degree-segment length of the adjoint's items, from a model of the ring pass: an item of d
+// degrees whose lanes hold R rings costs d (6 R + 4) (the recurrence and the four sums per ring,
+// the transpose-reduce per degree) plus 400 for its start (seed or saved state, ring data, first
+// coefficients: about 60 degrees' work); items are dealt heaviest first to the resident warp
+// slots, and the segment length of 64 q degrees (q = 2..8) with the shortest schedule wins.
+// Measured against fixed lengths at lmax 256 / 1024 / 2048, the adjoint's best lengths were
+// 128 / 128 / 448 degrees (0.021 / 0.066 / 0.263 ms against 0.031 / 0.074 / 0.270 ms at 256),
+// which the model picks.
+static int choose_segment_degrees(const std::vector<int>& jlo, const std::vector<int>& jhi, int L,
+                                  int mmax, int tile, int rmax, int slots) {
+    std::vector<double> cost;
+    double best = 0.0;
+    int best_q = 0;
+    for (int q = 2; q <= 8; ++q) {
+        cost.clear();
+        for (int m = 0; m <= std::min(mmax, L); ++m) {
+            if (jhi[m] < jlo[m]) continue;
+            const int nb = L >= m + 2 ? (L - m - 1 + 63) / 64 : 0;
+            const int K = std::max(1, std::min(nb, (nb + q / 2) / q));
+            for (int j0 = jlo[m]; j0 <= jhi[m]; j0 += tile) {
+                const int n = std::min(tile, jhi[m] - j0 + 1);
+                for (int base = 0; base < n; base += 32 * rmax) {
+                    const int reff = (std::min(32 * rmax, n - base) + 31) / 32;
+                    const int R = reff >= 3 ? 4 : reff;
+                    for (int k = 0; k < K; ++k) {
+                        const int first = k == 0 ? m : m + 2 + 64 * (int)(((int64_t)k * nb) / K);
+                        const int last = k + 1 < K ? m + 1 + 64 * (int)(((int64_t)(k + 1) * nb) / K) : L;
+                        cost.push_back((double)(last - first + 1) * (6.0 * R + 4.0) + 400.0);
+                    }
+                }
+            }
+        }
+        std::sort(cost.begin(), cost.end(), std::greater<double>());
+        std::priority_queue<double, std::vector<double>, std::greater<double>> busy;
+        for (int w = 0; w < slots; ++w) busy.push(0.0);
+        double span = 0.0;
+        for (double c : cost) {
+            const double t = busy.top() + c;
+            busy.pop();
+            busy.push(t);
+            span = std::max(span, t);
+        }
+        if (best_q == 0 || span < best) {
+            best = span;
+            best_q = q;
+        }
+    }
+    return 64 * best_q;
+}
+
 int build_adjoint_items(pfsht_plan* p, const std::vector<int>& jlo, const std::vector<int>& jhi,
                         int mmax, cudaStream_t s) {
     const int L = p->L;
@@ -243,7 +295,8 @@ int build_adjoint_items(pfsht_plan* p, const std::vector<int>& jlo, const std::v
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device);
         const size_t whole = make_ring_items(jlo, jhi, L, mmax, tile).size();
-        seg = whole >= (size_t)sms * 12 * 8 ? -1 : 256;
+        seg = whole >= (size_t)sms * 12 * 8 ? -1
+                                            : choose_segment_degrees(jlo, jhi, L, mmax, tile, rmax, sms * 11);
     }
     if (seg > 0) {
         PF_TRY(build_ring_segments(p->rt, jlo, jhi, L, mmax, seg, (int64_t)512 << 20, p->adj_seg, s));
