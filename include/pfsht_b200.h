@@ -145,7 +145,9 @@ pfsht_status pfsht_adjoint_host(pfsht_plan* plan, const void* f, void* alm);
  * the copies to overlap. One plan's host applies run in the order issued. */
 pfsht_status pfsht_forward_host_async(pfsht_plan* plan, const void* alm, void* f, void* stream);
 pfsht_status pfsht_adjoint_host_async(pfsht_plan* plan, const void* f, void* alm, void* stream);
-/* Waits for every host-buffer apply of the plan issued so far. */
+/* Waits for every host-buffer apply of the plan issued so far, including an asynchronous
+ * adjoint's zeroing of the padding and unretained orders of its host output, which runs on a
+ * host thread of its own. */
 pfsht_status pfsht_host_sync(pfsht_plan* plan);
 
 /* Bytes the two host-buffer applies move across PCIe per call (no reference counterpart):
