@@ -1416,7 +1416,7 @@ struct SpreadPickStage {
 };
 
 template <int W, class T>
-struct SpreadRowStage {
+struct SpreadRowStage {  // T = float (the FP64 grids use SpreadPickStage)
     static constexpr int RW = W / 2 + 1;
     static constexpr int VPL = 16 / (int)sizeof(T);        // T per 16-byte load
     static constexpr int KP = (RW + VPL - 1) / VPL * VPL;  // row weights per half
@@ -1462,7 +1462,7 @@ __device__ __forceinline__ int add_run(const SpreadPickStage<W, T>& st, int q, i
     }
 }
 
-// FP32: the points q0 .. q1 - 1, all of origin row pair J
+// FP32: the points q0 .. q1 - 1, all of origin row pair J (row weights read as float4)
 template <int J, int W, int NRH, class T>
 __device__ __forceinline__ void add_run(const SpreadRowStage<W, T>& st, int q0, int q1, int h,
                                         int c, cx<T> (&acc)[NRH]) {
@@ -1473,22 +1473,13 @@ __device__ __forceinline__ void add_run(const SpreadRowStage<W, T>& st, int q0, 
         const cx<T>* vp = &st.vc[q0][c];
         for (int q = q0; q < q1; ++q, kp += KS, vp += NV) {
             T kw[KP];
-            if constexpr (sizeof(T) == 8) {
 #pragma unroll
-                for (int u = 0; u < KP / 2; ++u) {
-                    const double2 t2 = reinterpret_cast<const double2*>(kp)[u];
-                    kw[2 * u] = t2.x;
-                    kw[2 * u + 1] = t2.y;
-                }
-            } else {
-#pragma unroll
-                for (int u = 0; u < KP / 4; ++u) {
-                    const float4 t4 = reinterpret_cast<const float4*>(kp)[u];
-                    kw[4 * u] = t4.x;
-                    kw[4 * u + 1] = t4.y;
-                    kw[4 * u + 2] = t4.z;
-                    kw[4 * u + 3] = t4.w;
-                }
+            for (int u = 0; u < KP / 4; ++u) {
+                const float4 t4 = reinterpret_cast<const float4*>(kp)[u];
+                kw[4 * u] = t4.x;
+                kw[4 * u + 1] = t4.y;
+                kw[4 * u + 2] = t4.z;
+                kw[4 * u + 3] = t4.w;
             }
             const cx<T> vk = *vp;
 #pragma unroll
@@ -1582,16 +1573,10 @@ spread_reg_kernel(const double2* __restrict__ pts, const int* __restrict__ perm,
                             w[KP + i] = i < RW ? at(2 * i + 1) : (T)0;
                         }
                     }
-                    if constexpr (sizeof(T) == 8) {
 #pragma unroll
-                        for (int u = 0; u < KP; ++u)
-                            reinterpret_cast<double2*>(st.kw[lane])[u] = make_double2(w[2 * u], w[2 * u + 1]);
-                    } else {
-#pragma unroll
-                        for (int u = 0; u < KP / 2; ++u)
-                            reinterpret_cast<float4*>(st.kw[lane])[u] =
-                                make_float4(w[4 * u], w[4 * u + 1], w[4 * u + 2], w[4 * u + 3]);
-                    }
+                    for (int u = 0; u < KP / 2; ++u)
+                        reinterpret_cast<float4*>(st.kw[lane])[u] =
+                            make_float4(w[4 * u], w[4 * u + 1], w[4 * u + 2], w[4 * u + 3]);
                 }
             }
             {
